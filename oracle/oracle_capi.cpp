@@ -1,0 +1,517 @@
+// oracle_capi.cpp — C entry points over the CPU restatement, for ctypes.
+//
+// TEST INFRASTRUCTURE: loaded only by tests/, __graft_entry__.smoke() and the cpu_baseline
+// leg of bench.py, as the checker. Nothing in the product links this library.
+//
+// Two ways in:
+//  * scene runs: DEM + walls + Manning + boundary segments (+ a fine-resolution edit) are
+//    built into a terrain here, at f32 or f64, exactly as crates/itr-hydro/src/terrain.rs
+//    does, then run with the oracle or the fused kernel (crates/itr-hydro/src/kernel.rs).
+//  * flat runs (f32): the same packed arrays the GPU C ABI takes (per-design face jumps,
+//    wet/gn2, boundary codes), so a GPU result can be compared to the CPU result on
+//    identical inputs.
+// The 8 validation cases of crates/itr-hydro/src/validation.rs are restated at the end.
+#include "itr_oracle.hpp"
+#include <thread>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+
+using namespace orc;
+
+// ------------------------------------------------------------------ small helpers ----
+extern "C" float orc_rcbrt32(float x) { return rcbrt(x); }
+extern "C" double orc_rcbrt64(double x) { return rcbrt(x); }
+extern "C" double orc_exp(double x) { return itr_math::exp_ref(x); }
+extern "C" double orc_log1p(double x) { return itr_math::log1p_ref(x); }
+extern "C" double orc_softplus(double x) { return itr_math::softplus(x); }
+extern "C" double orc_hyeto_integral(const double* t, const double* r, int n, double a, double b) {
+  Hyetograph h; h.t.assign(t, t + n); h.r.assign(r, r + n); return h.integral(a, b);
+}
+extern "C" double orc_hyeto_rate(const double* t, const double* r, int n, double x) {
+  Hyetograph h; h.t.assign(t, t + n); h.r.assign(r, r + n); return h.rate(x);
+}
+extern "C" float orc_fixedsum32(const float* v, int n) { FixedSum<float> s; s.add_slice(v, (size_t)n); return s.total(); }
+extern "C" double orc_fixedsum64(const double* v, int n) { FixedSum<double> s; s.add_slice(v, (size_t)n); return s.total(); }
+
+// Primitive::profile and DesignSpace::materialize. prims: n x 7 doubles
+// (kind, cx, cy, length, width, angle_deg, height). Writes the edit bbox and dz into
+// out_dz (capacity nx*ny); returns the number of dz values, or 0 for an empty edit.
+extern "C" double orc_profile(const double* prim, double x, double y) {
+  Primitive p; p.kind = (int)prim[0]; p.cx = prim[1]; p.cy = prim[2]; p.length = prim[3];
+  p.width = prim[4]; p.angle_deg = prim[5]; p.height = prim[6];
+  return prim_profile(p, x, y);
+}
+extern "C" int64_t orc_materialize(const double* prims, int n, double ox, double oy, double dx, double dy,
+                        int64_t nx, int64_t ny, const uint8_t* editable, double max_abs_dz,
+                        int64_t* bbox /*c0,r0,w,h*/, double* vol /*cut,fill*/, double* out_dz) {
+  std::vector<Primitive> v;
+  for (int i = 0; i < n; ++i) {
+    const double* q = prims + 7 * i;
+    Primitive p; p.kind = (int)q[0]; p.cx = q[1]; p.cy = q[2]; p.length = q[3]; p.width = q[4];
+    p.angle_deg = q[5]; p.height = q[6];
+    v.push_back(p);
+  }
+  TerrainEdit e = materialize(v, ox, oy, dx, dy, (size_t)nx, (size_t)ny, editable, max_abs_dz);
+  bbox[0] = (int64_t)e.c0; bbox[1] = (int64_t)e.r0; bbox[2] = (int64_t)e.w; bbox[3] = (int64_t)e.h;
+  vol[0] = e.cut_m3; vol[1] = e.fill_m3;
+  for (size_t i = 0; i < e.dz.size(); ++i) out_dz[i] = e.dz[i];
+  return (int64_t)e.dz.size();
+}
+
+// ------------------------------------------------------------------ scenes ----------
+struct Scene {
+  FineTerrain fine;
+  std::vector<Segment> segs;
+  size_t level = 1;
+  TerrainBase<float> b32;
+  TerrainBase<double> b64;
+};
+
+// seg_f: per segment 5 doubles (kind, side, has_range, r0, r1) + stage; hydrographs in
+// seg_ht/seg_hq with offsets seg_off (n_seg+1).
+extern "C" void* orc_scene_new(int64_t nx, int64_t ny, double ox, double oy, double dx, double dy,
+                    const double* dem, const uint8_t* walls, const double* manning, int64_t level,
+                    int n_seg, const double* seg_f, const double* seg_stage, const int64_t* seg_off,
+                    const double* seg_ht, const double* seg_hq) {
+  Scene* s = new Scene();
+  s->fine = fine_terrain((size_t)nx, (size_t)ny, ox, oy, dx, dy, dem, walls, manning);
+  for (int i = 0; i < n_seg; ++i) {
+    Segment g;
+    g.kind = (int)seg_f[5 * i + 0]; g.side = (int)seg_f[5 * i + 1];
+    g.has_range = seg_f[5 * i + 2] != 0.0; g.r0 = seg_f[5 * i + 3]; g.r1 = seg_f[5 * i + 4];
+    g.stage_m = seg_stage[i];
+    for (int64_t k = seg_off[i]; k < seg_off[i + 1]; ++k) { g.ht.push_back(seg_ht[k]); g.hq.push_back(seg_hq[k]); }
+    s->segs.push_back(g);
+  }
+  s->level = (size_t)level;
+  terrain_build(s->b32, s->fine, s->level, s->segs);
+  terrain_build(s->b64, s->fine, s->level, s->segs);
+  return s;
+}
+extern "C" void orc_scene_free(void* h) { delete (Scene*)h; }
+
+extern "C" void orc_scene_info(void* h, int64_t* out /*nx,ny,mode,wet_count*/, double* outd /*dx,dy,z_ref,z_wall*/) {
+  Scene* s = (Scene*)h;
+  out[0] = (int64_t)s->b32.layout.nx; out[1] = (int64_t)s->b32.layout.ny;
+  out[2] = (int64_t)s->b32.mode; out[3] = (int64_t)s->b32.wet_count;
+  outd[0] = s->b32.dx; outd[1] = s->b32.dy; outd[2] = s->fine.z_ref; outd[3] = s->fine.z_wall;
+}
+
+static TerrainEdit make_edit(const int64_t* bbox, const double* dz, double cut, double fill) {
+  TerrainEdit e;
+  if (bbox) {
+    e.c0 = (size_t)bbox[0]; e.r0 = (size_t)bbox[1]; e.w = (size_t)bbox[2]; e.h = (size_t)bbox[3];
+    e.dz.assign(dz, dz + e.w * e.h);
+  }
+  e.cut_m3 = cut; e.fill_m3 = fill;
+  return e;
+}
+
+// Packed f32 face arrays of the prepared (edited) terrain, in the GPU ABI layout:
+// dzx[r*(nx+1)+f] = fx0.row(r+1)[f], dzy[f*nx+c] = fy0.row(f)[c+1]; crest second jumps too.
+// Also wet/gn2 (nx*ny) and z_level (f64, nx*ny).
+extern "C" void orc_scene_pack32(void* h, const int64_t* bbox, const double* dz, float* dzx, float* dzy,
+                      float* dzx2, float* dzy2, float* wet, float* gn2, double* zlev) {
+  Scene* s = (Scene*)h;
+  PreparedTerrain<float> pt; pt.base = &s->b32; pt.reset(s->b32);
+  TerrainEdit e = make_edit(bbox, dz, 0, 0);
+  if (bbox) pt.apply_edit(e);
+  const Layout& L = s->b32.layout;
+  size_t nx = L.nx, ny = L.ny;
+  for (size_t r = 0; r < ny; ++r)
+    for (size_t f = 0; f <= nx; ++f) {
+      dzx[r * (nx + 1) + f] = pt.fx0[L.at(f, r + 1)];
+      if (dzx2) dzx2[r * (nx + 1) + f] = pt.fx1[L.at(f, r + 1)];
+    }
+  for (size_t f = 0; f <= ny; ++f)
+    for (size_t c = 0; c < nx; ++c) {
+      dzy[f * nx + c] = pt.fy0[L.at(c + 1, f)];
+      if (dzy2) dzy2[f * nx + c] = pt.fy1[L.at(c + 1, f)];
+    }
+  for (size_t r = 0; r < ny; ++r)
+    for (size_t c = 0; c < nx; ++c) {
+      wet[r * nx + c] = s->b32.wet[L.at(c + 1, r + 1)];
+      gn2[r * nx + c] = s->b32.gn2[L.at(c + 1, r + 1)];
+    }
+  std::vector<double> z = pt.z_level();
+  for (size_t k = 0; k < nx * ny; ++k) zlev[k] = z[k];
+}
+
+// Boundary codes per side cell: north[nx], south[nx], west[ny], east[ny] (0 wall,
+// 1 transmissive, 2 stage, 3 inflow).
+extern "C" void orc_scene_bc(void* h, uint8_t* codes) {
+  Scene* s = (Scene*)h;
+  const Boundaries& b = s->b32.bnd;
+  size_t k = 0;
+  for (auto* v : {&b.north, &b.south, &b.west, &b.east})
+    for (const Ghost& g : *v) codes[k++] = (uint8_t)g.kind;
+}
+
+struct ParamsIn {  // mirrors the 16-double params vector built by the Python side
+  double duration, sync, cfl, dt_max, h_dry, h_eps, infil, initial_depth, has_stage, stage, skip_dry, inflow_scale;
+};
+
+static Params make_params(const double* pv, const double* rain_t, const double* rain_r, int n_rain) {
+  Params p;
+  p.duration = pv[0]; p.sync = pv[1]; p.cfl = pv[2]; p.dt_max = pv[3]; p.h_dry = pv[4]; p.h_eps = pv[5];
+  p.infil_capacity = pv[6]; p.initial_depth = pv[7]; p.has_stage = pv[8] != 0.0; p.initial_stage = pv[9];
+  p.skip_dry = pv[10] != 0.0; p.inflow_scale = pv[11];
+  p.rain.t.assign(rain_t, rain_t + n_rain); p.rain.r.assign(rain_r, rain_r + n_rain);
+  return p;
+}
+
+// Observer / objective description. obj_f: tol, tau, cut_cost, fill_cost, earth_weight,
+// require(0/1), has_incumbent(0/1), incumbent, cut, fill.
+struct ObjIn {
+  Objective obj; ObserverCfg cfg; std::vector<double> baseline;
+};
+static void make_obj(ObjIn& o, int n_mon, const uint32_t* mon, int n_guard, const int64_t* guard_pos,
+                     const double* baseline, int n_assets, const int64_t* asset_off, const int64_t* asset_pos,
+                     const double* asset_thr, const double* asset_w, const double* obj_f) {
+  o.obj.mon_cells.assign(mon, mon + n_mon);
+  for (int i = 0; i < n_guard; ++i) o.obj.guard_pos.push_back((size_t)guard_pos[i]);
+  for (int a = 0; a < n_assets; ++a) {
+    Asset as; as.threshold = asset_thr[a]; as.weight = asset_w[a];
+    for (int64_t k = asset_off[a]; k < asset_off[a + 1]; ++k) as.pos.push_back((size_t)asset_pos[k]);
+    o.obj.assets.push_back(as);
+  }
+  o.obj.guard_tol = obj_f[0]; o.obj.tau = obj_f[1]; o.obj.cut_cost = obj_f[2]; o.obj.fill_cost = obj_f[3];
+  o.obj.earth_weight = obj_f[4]; o.obj.require_no_worsening = obj_f[5] != 0.0;
+  o.cfg.obj = &o.obj;
+  if (baseline) { o.baseline.assign(baseline, baseline + n_mon); o.cfg.baseline = o.baseline.data(); }
+  o.cfg.has_incumbent = obj_f[6] != 0.0; o.cfg.incumbent = obj_f[7];
+  o.cfg.cut = obj_f[8]; o.cfg.fill = obj_f[9];
+}
+
+// out_s (16): t_end, steps, sync_count, abort, abort_cell, abort_exceed, abort_sync, abort_lb,
+// v0, rel_residual, dt_min, dt_max, dt_mean, cell_updates, rows_skipped, n_rows.
+template <class T>
+static void write_result(const RunResult& R, const Solver<T>& S, double* out_s, double* mon_max, double* mon_tmax,
+                         double* ledger, int max_rows, double* h_out, double* qx_out, double* qy_out,
+                         double* peak, double* peak_step) {
+  out_s[0] = R.t_end; out_s[1] = (double)R.steps; out_s[2] = R.sync_count; out_s[3] = R.abort;
+  out_s[4] = R.abort_cell; out_s[5] = R.abort_exceed; out_s[6] = R.abort_sync; out_s[7] = R.abort_lb;
+  out_s[8] = R.v0; out_s[9] = R.rel_residual; out_s[10] = R.dt_min; out_s[11] = R.dt_max; out_s[12] = R.dt_mean;
+  out_s[13] = (double)R.cell_updates; out_s[14] = (double)R.rows_skipped; out_s[15] = (double)R.rows.size();
+  for (size_t k = 0; k < R.mon_max.size(); ++k) { if (mon_max) mon_max[k] = R.mon_max[k]; if (mon_tmax) mon_tmax[k] = R.mon_tmax[k]; }
+  if (ledger)
+    for (size_t r = 0; r < R.rows.size() && (int)r < max_rows; ++r) {
+      const LedgerRow& q = R.rows[r];
+      double* o = ledger + 8 * r;
+      o[0] = q.t; o[1] = q.volume; o[2] = q.rain; o[3] = q.inflow; o[4] = q.outflow; o[5] = q.infil; o[6] = q.fix; o[7] = q.residual;
+    }
+  const Layout& L = S.L;
+  for (size_t r = 0; r < L.ny; ++r)
+    for (size_t c = 0; c < L.nx; ++c) {
+      size_t k = L.at(c + 1, r + 1), o = r * L.nx + c;
+      if (h_out) h_out[o] = (double)S.h[k];
+      if (qx_out) qx_out[o] = (double)S.qx[k];
+      if (qy_out) qy_out[o] = (double)S.qy[k];
+      if (peak && !R.peak.empty()) peak[o] = R.peak[o];
+      if (peak_step && !R.peak_step.empty()) peak_step[o] = (double)R.peak_step[o];
+    }
+}
+
+template <class T>
+static void scene_run_t(Scene* s, TerrainBase<T>& tb, int kernel, const int64_t* bbox, const double* dz,
+                        double cut, double fill, const double* pv, const double* rain_t, const double* rain_r, int n_rain,
+                        int n_mon, const uint32_t* mon, ObjIn* oi, const double* h0d, int want_peak,
+                        double* out_s, double* mon_max, double* mon_tmax, double* ledger, int max_rows,
+                        double* h_out, double* qx_out, double* qy_out, double* peak, double* peak_step) {
+  (void)s;
+  PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+  TerrainEdit e = make_edit(bbox, dz, cut, fill);
+  if (bbox) pt.apply_edit(e);
+  Solver<T> S; S.p = make_params(pv, rain_t, rain_r, n_rain);
+  std::vector<uint32_t> mcells(mon, mon + n_mon);
+  std::vector<T> h0;
+  if (h0d) { h0.resize(tb.layout.nx * tb.layout.ny); for (size_t k = 0; k < h0.size(); ++k) h0[k] = (T)h0d[k]; }
+  RunResult R = S.run(pt, mcells, kernel == 0 ? K_ORACLE : K_FUSED, oi ? &oi->cfg : nullptr,
+                      h0d ? h0.data() : nullptr, want_peak != 0);
+  write_result(R, S, out_s, mon_max, mon_tmax, ledger, max_rows, h_out, qx_out, qy_out, peak, peak_step);
+}
+
+// prec 0 = f32, 1 = f64; kernel 0 = step_oracle, 1 = step_fused.
+extern "C" void orc_scene_run(void* h, int prec, int kernel, const int64_t* bbox, const double* dz, double cut, double fill,
+                   const double* pv, const double* rain_t, const double* rain_r, int n_rain,
+                   int n_mon, const uint32_t* mon, int n_guard, const int64_t* guard_pos, const double* baseline,
+                   int n_assets, const int64_t* asset_off, const int64_t* asset_pos, const double* asset_thr,
+                   const double* asset_w, const double* obj_f, const double* h0, int want_peak,
+                   double* out_s, double* mon_max, double* mon_tmax, double* ledger, int max_rows,
+                   double* h_out, double* qx_out, double* qy_out, double* peak, double* peak_step) {
+  Scene* s = (Scene*)h;
+  ObjIn oi; ObjIn* op = nullptr;
+  if (obj_f) { make_obj(oi, n_mon, mon, n_guard, guard_pos, baseline, n_assets, asset_off, asset_pos, asset_thr, asset_w, obj_f); op = &oi; }
+  if (prec == 0)
+    scene_run_t<float>(s, s->b32, kernel, bbox, dz, cut, fill, pv, rain_t, rain_r, n_rain, n_mon, mon, op, h0, want_peak,
+                       out_s, mon_max, mon_tmax, ledger, max_rows, h_out, qx_out, qy_out, peak, peak_step);
+  else
+    scene_run_t<double>(s, s->b64, kernel, bbox, dz, cut, fill, pv, rain_t, rain_r, n_rain, n_mon, mon, op, h0, want_peak,
+                        out_s, mon_max, mon_tmax, ledger, max_rows, h_out, qx_out, qy_out, peak, peak_step);
+}
+
+// ------------------------------------------------------------------ flat (f32) -----
+// A terrain described only by the packed arrays of the GPU ABI. Stage/inflow ghosts are
+// not representable here (walls and transmissive only), matching the GPU path's scope.
+struct Flat {
+  FineTerrain fine;  // only z_ref (0) and nothing else is read
+  TerrainBase<float> tb;
+  PreparedTerrain<float> pt;
+};
+
+static void flat_build(Flat& F, int64_t nx, int64_t ny, double dx, double dy, int mode, const float* wet,
+                       const float* gn2, const uint8_t* bc, const float* dzx, const float* dzy,
+                       const float* dzx2, const float* dzy2) {
+  TerrainBase<float>& tb = F.tb;
+  tb.fine = &F.fine; tb.level = 1; tb.dx = dx; tb.dy = dy; tb.g = G_ACC;
+  tb.layout = Layout((size_t)nx, (size_t)ny);
+  tb.mode = mode == 1 ? CREST : SIGNED;
+  const Layout& L = tb.layout;
+  size_t len = L.len();
+  tb.fx0.assign(len, 0.f); tb.fx1.assign(len, 0.f); tb.fy0.assign(len, 0.f); tb.fy1.assign(len, 0.f);
+  tb.wet.assign(len, 0.f); tb.gn2.assign(len, 0.f);
+  tb.z.assign((size_t)(nx * ny), 0.0); tb.wall.assign((size_t)(nx * ny), 0);
+  tb.wet_count = 0;
+  for (int64_t r = 0; r < ny; ++r)
+    for (int64_t c = 0; c < nx; ++c) {
+      size_t k = (size_t)(r * nx + c);
+      tb.wet[L.at(c + 1, r + 1)] = wet[k]; tb.gn2[L.at(c + 1, r + 1)] = gn2[k];
+      tb.wall[k] = !(wet[k] != 0.0f);
+      tb.wet_count += wet[k] != 0.0f;
+    }
+  tb.bnd.north.assign(nx, Ghost{}); tb.bnd.south.assign(nx, Ghost{});
+  tb.bnd.west.assign(ny, Ghost{}); tb.bnd.east.assign(ny, Ghost{});
+  size_t q = 0;
+  for (auto* v : {&tb.bnd.north, &tb.bnd.south, &tb.bnd.west, &tb.bnd.east})
+    for (Ghost& g : *v) g.kind = bc[q++];
+  F.pt.base = &tb;
+  F.pt.fx0 = tb.fx0; F.pt.fx1 = tb.fx1; F.pt.fy0 = tb.fy0; F.pt.fy1 = tb.fy1;
+  for (int64_t r = 0; r < ny; ++r)
+    for (int64_t f = 0; f <= nx; ++f) {
+      F.pt.fx0[L.at(f, r + 1)] = dzx[r * (nx + 1) + f];
+      if (dzx2) F.pt.fx1[L.at(f, r + 1)] = dzx2[r * (nx + 1) + f];
+    }
+  for (int64_t f = 0; f <= ny; ++f)
+    for (int64_t c = 0; c < nx; ++c) {
+      F.pt.fy0[L.at(c + 1, f)] = dzy[f * nx + c];
+      if (dzy2) F.pt.fy1[L.at(c + 1, f)] = dzy2[f * nx + c];
+    }
+}
+
+extern "C" void orc_flat_run(int kernel, int64_t nx, int64_t ny, double dx, double dy, int mode, const float* wet, const float* gn2,
+                  const uint8_t* bc, const float* dzx, const float* dzy, const float* dzx2, const float* dzy2,
+                  const float* h0, const double* pv, const double* rain_t, const double* rain_r, int n_rain,
+                  int n_mon, const uint32_t* mon, int n_guard, const int64_t* guard_pos, const double* baseline,
+                  int n_assets, const int64_t* asset_off, const int64_t* asset_pos, const double* asset_thr,
+                  const double* asset_w, const double* obj_f, int want_peak,
+                  double* out_s, double* mon_max, double* mon_tmax, double* ledger, int max_rows,
+                  double* h_out, double* qx_out, double* qy_out, double* peak, double* peak_step) {
+  Flat F;
+  flat_build(F, nx, ny, dx, dy, mode, wet, gn2, bc, dzx, dzy, dzx2, dzy2);
+  ObjIn oi; ObjIn* op = nullptr;
+  if (obj_f) { make_obj(oi, n_mon, mon, n_guard, guard_pos, baseline, n_assets, asset_off, asset_pos, asset_thr, asset_w, obj_f); op = &oi; }
+  Solver<float> S; S.p = make_params(pv, rain_t, rain_r, n_rain);
+  std::vector<uint32_t> mcells(mon, mon + n_mon);
+  RunResult R = S.run(F.pt, mcells, kernel == 0 ? K_ORACLE : K_FUSED, op ? &op->cfg : nullptr, h0, want_peak != 0);
+  write_result(R, S, out_s, mon_max, mon_tmax, ledger, max_rows, h_out, qx_out, qy_out, peak, peak_step);
+}
+
+// Candidate-parallel f32 fused runs (one design per thread, the reference's default search
+// mode, crates/itr-opt/src/evaluator.rs:337-352), for the timed CPU baseline. Face arrays are
+// per design (n_designs * ny*(nx+1) and n_designs * (ny+1)*nx). Returns wall seconds; steps
+// per design go to out_steps, monitor maxima to out_mon (n_designs * n_mon).
+extern "C" double orc_flat_batch(int threads, int n_designs, int64_t nx, int64_t ny, double dx, double dy,
+                      const float* wet, const float* gn2, const uint8_t* bc, const float* dzx, const float* dzy,
+                      const float* h0, const double* pv, const double* rain_t, const double* rain_r, int n_rain,
+                      int n_mon, const uint32_t* mon, double* out_steps, double* out_mon) {
+  std::atomic<int> next(0);
+  auto t0 = std::chrono::steady_clock::now();
+  auto worker = [&]() {
+    for (;;) {
+      int d = next.fetch_add(1);
+      if (d >= n_designs) break;
+      Flat F;
+      flat_build(F, nx, ny, dx, dy, 0, wet, gn2, bc, dzx + (size_t)d * ny * (nx + 1), dzy + (size_t)d * (ny + 1) * nx, nullptr, nullptr);
+      Solver<float> S; S.p = make_params(pv, rain_t, rain_r, n_rain);
+      std::vector<uint32_t> mcells(mon, mon + n_mon);
+      RunResult R = S.run(F.pt, mcells, K_FUSED, nullptr, h0 ? h0 + (size_t)d * nx * ny : nullptr, false);
+      out_steps[d] = (double)R.steps;
+      for (int k = 0; k < n_mon; ++k) out_mon[(size_t)d * n_mon + k] = R.mon_max[k];
+    }
+  };
+  std::vector<std::thread> ts;
+  int nt = threads < 1 ? 1 : threads;
+  for (int i = 0; i < nt; ++i) ts.emplace_back(worker);
+  for (auto& t : ts) t.join();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// -------------------------------------------------------- validation.rs (8 cases) ----
+// Each returns {value, threshold, passed, extra}. prec 0 = f32, 1 = f64.
+struct CaseOut { double value, threshold, passed, extra; };
+
+static FineTerrain* make_fine(size_t nx, size_t ny, double dx, double (*zf)(double, double, const double*),
+                              const double* zp, bool (*wf)(size_t, size_t), double n) {
+  std::vector<double> dem(nx * ny); std::vector<uint8_t> w(nx * ny); std::vector<double> man(nx * ny, n);
+  double oy = (double)ny * dx;
+  for (size_t r = 0; r < ny; ++r)
+    for (size_t c = 0; c < nx; ++c) {
+      double x = 0.0 + ((double)c + 0.5) * dx, y = oy - ((double)r + 0.5) * dx;
+      dem[r * nx + c] = zf(x, y, zp);
+      w[r * nx + c] = wf ? wf(c, r) : 0;
+    }
+  FineTerrain* f = new FineTerrain(fine_terrain(nx, ny, 0.0, oy, dx, dx, dem.data(), w.data(), man.data()));
+  return f;
+}
+
+static Params vparams(double dur, double sync) {
+  Params p; p.duration = dur; p.sync = sync; p.cfl = 0.35; p.dt_max = 5.0; p.h_dry = 1e-6; p.h_eps = 1e-5;
+  p.infil_capacity = 0; p.initial_depth = 0; p.has_stage = false; p.skip_dry = true; p.inflow_scale = 1.0;
+  return p;
+}
+static Hyetograph mm_h(std::initializer_list<std::pair<double, double>> pts) {
+  Hyetograph h; for (auto& q : pts) { h.t.push_back(q.first); h.r.push_back(q.second / 1000.0 / 3600.0); } return h;
+}
+
+template <class T> static CaseOut case_run(int id) {
+  bool f64 = sizeof(T) == 8;
+  CaseOut o{0, 0, 0, 0};
+  if (id == 0) {  // lake_at_rest (validation.rs:79-97)
+    auto zf = [](double x, double y, const double*) { return 0.3 * std::sin(x / 7.0) * std::cos(y / 5.0) + (x > 30.0 ? 0.4 : 0.0); };
+    FineTerrain* f = make_fine(64, 48, 1.0, zf, nullptr, nullptr, 0.03);
+    TerrainBase<T> tb; terrain_build(tb, *f, 1, {});
+    Params p = vparams(60.0, 10.0); p.has_stage = true; p.initial_stage = 1.5;
+    PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+    Solver<T> S; S.p = p; RunResult R = S.run(pt, {}, K_FUSED, nullptr);
+    double err = 0;
+    for (size_t j = 1; j <= 48; ++j)
+      for (size_t i = 1; i <= 64; ++i) {
+        size_t k = S.L.at(i, j);
+        double eta = (double)S.h[k] + tb.z[(j - 1) * 64 + i - 1] + f->z_ref;
+        err = fmax_num(fmax_num(fmax_num(err, std::fabs(eta - 1.5)), std::fabs((double)S.qx[k])), std::fabs((double)S.qy[k]));
+      }
+    o.value = err; o.threshold = f64 ? 1e-12 : 1e-4; o.extra = (double)R.steps;
+    delete f;
+  } else if (id == 1) {  // rain_closed_plain (:99-107)
+    auto zf = [](double, double, const double*) { return 10.0; };
+    FineTerrain* f = make_fine(40, 30, 2.0, zf, nullptr, nullptr, 0.04);
+    TerrainBase<T> tb; terrain_build(tb, *f, 1, {});
+    Params p = vparams(600.0, 60.0); p.rain = mm_h({{0, 0}, {100, 50}, {400, 10}, {500, 0}});
+    PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+    Solver<T> S; S.p = p; RunResult R = S.run(pt, {}, K_FUSED, nullptr);
+    o.value = R.rel_residual; o.threshold = f64 ? 1e-12 : 1e-6; o.extra = R.rows.empty() ? 0 : R.rows.back().rain;
+    delete f;
+  } else if (id == 2) {  // dam_break_ritter (:109-171)
+    size_t nx = 800; double dx = 0.25, h0 = 1.0, x0 = 100.0;
+    auto zf = [](double, double, const double*) { return 0.0; };
+    FineTerrain* f = make_fine(nx, 3, dx, zf, nullptr, nullptr, 0.0);
+    TerrainBase<T> tb; terrain_build(tb, *f, 1, {});
+    Params p = vparams(10.0, 10.0); p.cfl = 0.4;
+    PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+    Solver<T> S; S.p = p;
+    typename Solver<T>::Start st;
+    Layout L = tb.layout;
+    st.h.assign(L.len(), T(0));
+    for (size_t j = 1; j <= L.ny; ++j)
+      for (size_t i = 1; i <= L.nx; ++i) { double x = ((double)i - 0.5) * dx; if (x < x0) st.h[L.at(i, j)] = (T)h0; }
+    st.dt_next = 0.4 * dx / std::sqrt(9.81 * h0);
+    double v0 = 0; for (size_t j = 0; j < L.ny; ++j) v0 += (x0 / dx) * h0;
+    st.v0 = v0 * dx * dx;
+    RunResult R = S.run(pt, {}, K_FUSED, nullptr, nullptr, false, &st);
+    double t = R.t_end, c0 = std::sqrt(9.81 * h0), l1 = 0;
+    size_t j = 2;
+    for (size_t i = 1; i <= nx; ++i) {
+      double x = ((double)i - 0.5) * dx - x0, exact;
+      if (x <= -c0 * t) exact = h0; else if (x >= 2.0 * c0 * t) exact = 0.0;
+      else { double a = 2.0 * c0 - x / t; exact = a * a / (9.0 * 9.81); }
+      l1 += std::fabs((double)S.h[L.at(i, j)] - exact) * dx;
+    }
+    o.value = l1 / (h0 * 3.0 * c0 * t); o.threshold = 0.03; o.extra = (double)R.steps;
+    delete f;
+  } else if (id == 3) {  // wet_dry_step (:173-185)
+    auto zf = [](double x, double, const double*) { return (x > 40.0 ? 0.8 : 0.0) + 0.01 * x; };
+    FineTerrain* f = make_fine(80, 20, 1.0, zf, nullptr, nullptr, 0.02);
+    TerrainBase<T> tb; terrain_build(tb, *f, 1, {});
+    Params p = vparams(120.0, 20.0); p.has_stage = true; p.initial_stage = 1.0;
+    PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+    Solver<T> S; S.p = p; RunResult R = S.run(pt, {}, K_FUSED, nullptr);
+    double min_h = std::numeric_limits<double>::max();
+    for (T v : S.h) min_h = fmin_num(min_h, (double)v);
+    o.value = R.rel_residual; o.threshold = f64 ? 1e-12 : 1e-6; o.extra = min_h;
+    if (!(min_h >= 0.0 && R.abort == AB_NONE)) o.threshold = -1;  // forces failure
+    delete f;
+  } else if (id == 4) {  // tilted_plane (:187-203)
+    size_t nx = 100, ny = 4; double dx = 2.0, slope = 0.01, n = 0.03;
+    std::vector<Segment> segs(1); segs[0].kind = 2; segs[0].side = 3;
+    static double s_slope; s_slope = slope;
+    auto zf = [](double x, double, const double*) { return 5.0 - s_slope * x; };
+    FineTerrain* f = make_fine(nx, ny, dx, zf, nullptr, nullptr, n);
+    TerrainBase<T> tb; terrain_build(tb, *f, 1, segs);
+    double rate = 100.0;
+    Params p = vparams(3600.0, 300.0); p.rain = mm_h({{0.0, rate}, {1e9, rate}});
+    PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+    Solver<T> S; S.p = p; RunResult R = S.run(pt, {}, K_FUSED, nullptr);
+    size_t k = R.rows.size();
+    double q_out = (R.rows[k - 1].outflow - R.rows[k - 2].outflow) / (R.rows[k - 1].t - R.rows[k - 2].t);
+    double q_in = rate / 1000.0 / 3600.0 * (double)(nx * ny) * dx * dx;
+    o.value = std::fabs(q_out / q_in - 1.0); o.threshold = 0.02; o.extra = q_out;
+    delete f;
+  } else if (id == 5) {  // gauge_invariance (:205-222)
+    auto run = [](double off, std::vector<T>& hout) {
+      static double s_off; s_off = off;
+      auto zf = [](double x, double y, const double*) {
+        double v = 0.2 * std::sin(x / 6.0) + 0.01 * y;
+        return s_off + std::round(v * 1024.0) / 1024.0;
+      };
+      FineTerrain* f = make_fine(40, 30, 1.0, zf, nullptr, nullptr, 0.03);
+      TerrainBase<T> tb; terrain_build(tb, *f, 1, {});
+      Params p = vparams(60.0, 30.0); p.has_stage = true; p.initial_stage = off + 0.5;
+      p.rain = mm_h({{0.0, 40.0}, {60.0, 0.0}});
+      PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+      Solver<T> S; S.p = p; S.run(pt, {}, K_FUSED, nullptr);
+      hout = S.h;
+      delete f;
+    };
+    std::vector<T> a, b; run(0.0, a); run(1000.0, b);
+    size_t diff = 0;
+    for (size_t i = 0; i < a.size(); ++i) if (std::memcmp(&a[i], &b[i], sizeof(T)) != 0) ++diff;
+    o.value = (double)diff; o.threshold = 0.0;
+  } else if (id == 6) {  // walls_under_rain (:224-241)
+    auto zf = [](double x, double, const double*) { return 0.01 * x; };
+    auto wf = [](size_t c, size_t r) { return (c >= 10 && c < 20) && (r >= 10 && r < 20); };
+    FineTerrain* f = make_fine(30, 30, 1.0, zf, nullptr, wf, 0.03);
+    TerrainBase<T> tb; terrain_build(tb, *f, 1, {});
+    Params p = vparams(300.0, 60.0); p.rain = mm_h({{0.0, 80.0}, {300.0, 80.0}});
+    PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+    Solver<T> S; S.p = p; RunResult R = S.run(pt, {}, K_FUSED, nullptr);
+    double wall_h = 0;
+    for (size_t r = 10; r < 20; ++r) for (size_t c = 10; c < 20; ++c) wall_h = fmax_num(wall_h, (double)S.h[S.L.at(c + 1, r + 1)]);
+    o.value = R.rel_residual; o.threshold = f64 ? 1e-12 : 1e-6; o.extra = wall_h;
+    if (wall_h != 0.0) o.threshold = -1;
+    delete f;
+  } else if (id == 7) {  // inflow_ledger (:243-258)
+    std::vector<Segment> segs(1);
+    segs[0].kind = 1; segs[0].side = 2; segs[0].has_range = true; segs[0].r0 = 10.0; segs[0].r1 = 20.0;
+    segs[0].ht = {0.0, 100.0, 300.0}; segs[0].hq = {0.0, 2.0, 0.0};
+    auto zf = [](double x, double, const double*) { return 1.0 - 0.005 * x; };
+    FineTerrain* f = make_fine(60, 30, 1.0, zf, nullptr, nullptr, 0.03);
+    TerrainBase<T> tb; terrain_build(tb, *f, 1, segs);
+    Params p = vparams(400.0, 50.0);
+    PreparedTerrain<T> pt; pt.base = &tb; pt.reset(tb);
+    Solver<T> S; S.p = p; RunResult R = S.run(pt, {}, K_FUSED, nullptr);
+    const LedgerRow& last = R.rows.back();
+    double net = last.inflow - last.outflow;
+    o.value = R.rel_residual; o.threshold = f64 ? 1e-12 : 1e-6; o.extra = net;
+    if (!(std::fabs(net / 300.0 - 1.0) < 0.02)) o.threshold = -1;
+    delete f;
+  }
+  o.passed = (std::isfinite(o.value) && o.value <= o.threshold) ? 1.0 : 0.0;
+  return o;
+}
+
+extern "C" void orc_validation(int prec, int id, double* out4) {
+  CaseOut o = prec == 0 ? case_run<float>(id) : case_run<double>(id);
+  out4[0] = o.value; out4[1] = o.threshold; out4[2] = o.passed; out4[3] = o.extra;
+}
+
