@@ -1,0 +1,185 @@
+/* itr_gpu.h — C ABI of the B200 batched forward operator (and its adjoint) for itr.
+ *
+ * This is the drop-in boundary for the reference's batch evaluator path:
+ *   trait BatchBackend<f32>::run(&SolverParams, &[&PreparedTerrain<f32>], &MonitorSet)
+ *       crates/itr-opt/src/evaluator.rs:131-135
+ *   GpuSolver::{new, run_batch, adapter_info}      crates/itr-gpu/src/lib.rs:85,149,126
+ *   CLI wiring Gpu(GpuSolver) -> BatchRun          crates/itr-cli/src/backend.rs:44-63
+ * Plain pointers and sizes only. A context owns its device memory and one CUDA stream; a
+ * context is not thread-safe (the reference backend is `&mut self`), several contexts may
+ * coexist. Every entry point returns an itr_status; itr_gpu_last_error() has the text.
+ *
+ * Units and layouts follow the reference: depths in m, rates in m/s, row-major grids with
+ * row 0 the northern row, linear cell id = row * nx + col (MonitorSet, model.rs:6-24).
+ */
+#ifndef ITR_GPU_H
+#define ITR_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ITR_GPU_ABI_VERSION 1
+
+typedef struct itr_ctx itr_ctx;
+
+/* Status codes. ITR_UNSUPPORTED plays the role of the reference's Err(String) from
+ * run_batch: "unsupported here", the evaluator then falls back to the CPU for that level
+ * (evaluator.rs:231-238). */
+enum itr_status {
+  ITR_OK = 0,
+  ITR_UNSUPPORTED = 1,
+  ITR_INVALID_ARG = 2,
+  ITR_DEVICE_ERROR = 3,
+  ITR_DEVICE_TIMEOUT = 4
+};
+
+/* Ghost-cell kinds per boundary side cell (terrain.rs:121-129, boundary.rs:12-87). */
+enum itr_bc { ITR_BC_WALL = 0, ITR_BC_TRANSMISSIVE = 1, ITR_BC_STAGE = 2, ITR_BC_INFLOW = 3 };
+
+/* Face modes (terrain.rs:12-18): one signed jump per face (fidelity level 1) or two
+ * non-negative jumps to a face crest (coarse levels). */
+enum itr_face_mode { ITR_FACE_SIGNED = 0, ITR_FACE_CREST = 1 };
+
+/* Per-design outcome (evaluator.rs:20-28 Status, reduced to what a batch run can yield). */
+enum itr_run_status {
+  ITR_RUN_OK = 0,
+  ITR_RUN_GUARD_ABORT = 1,     /* AbortReason::GuardViolation (objective.rs:130-145) */
+  ITR_RUN_INCUMBENT_ABORT = 2, /* AbortReason::Incumbent (evaluator.rs:100-104)       */
+  ITR_RUN_UNHEALTHY = 3        /* negative depth beyond h_dry or NaN (numerics.rs:163) */
+};
+
+/* SolverParams (crates/itr-hydro/src/solver.rs:27-49). locked_dt and cfl_hard have no
+ * counterpart here (baseline-locked dt is not part of the batch path); inflow_scale must
+ * be 1, as the reference GPU backend requires (backend.rs:53-55). */
+typedef struct itr_params {
+  double duration_s;
+  double sync_interval_s;
+  double cfl;
+  double dt_max_s;
+  double h_dry;
+  double h_eps;
+  const double* rain_t;     /* Hyetograph points: time [s]            (scenario.rs:526) */
+  const double* rain_rate;  /*                    rate [m/s]                             */
+  int32_t n_rain;
+  double infil_capacity;    /* constant infiltration capacity [m/s]                      */
+  double initial_depth;     /* used for designs whose h0 is NULL (init_state, solver.rs:287) */
+  int32_t skip_dry;         /* dry-row skipping; bitwise-neutral (kernel.rs:605-612)     */
+  double inflow_scale;      /* must be 1.0                                               */
+} itr_params;
+
+/* The shared TerrainBase<f32> of one call (terrain.rs:237-257): every design in a call
+ * shares it, as run_batch requires (Arc::ptr_eq, lib.rs:154-159). */
+typedef struct itr_grid {
+  int32_t nx, ny;
+  double dx, dy;
+  double g;                 /* 9.81 (terrain.rs:259) */
+  int32_t mode;             /* itr_face_mode */
+  const float* wet;         /* nx*ny, 1 = open cell, 0 = wall (TerrainBase::wet)      */
+  const float* gn2;         /* nx*ny, g*n^2 (TerrainBase::gn2)                        */
+  const uint8_t* bc;        /* 2*nx + 2*ny codes: north[nx], south[nx], west[ny], east[ny] */
+  int64_t wet_count;        /* number of open cells (rain volume in the ledger)       */
+} itr_grid;
+
+/* One candidate: the face jumps of its PreparedTerrain (lib.rs:177-194 packs the same
+ * arrays). dzx[r*(nx+1) + f] is x-face f of row r (f = 0 and f = nx are the domain edges
+ * and are 0); dzy[f*nx + c] is y-face f of column c (f = 0 and f = ny are 0). Crest mode
+ * adds the second jump of every face in dzx2/dzy2. */
+typedef struct itr_design {
+  const float* dzx;         /* ny*(nx+1) */
+  const float* dzy;         /* (ny+1)*nx */
+  const float* dzx2;        /* crest mode only, else NULL */
+  const float* dzy2;        /* crest mode only, else NULL */
+  const float* h0;          /* nx*ny initial depth, or NULL for params.initial_depth on open cells */
+  double cut_m3, fill_m3;   /* earthwork volumes of the edit (J's earthwork term)      */
+} itr_design;
+
+/* Objective and abort rules (objective.rs:8-150, GuardObserver evaluator.rs:88-108).
+ * Positions index the monitor list. NULL means: no objective, no aborts, J not computed. */
+typedef struct itr_objective {
+  int32_t n_assets;
+  const int32_t* asset_off;      /* n_assets+1 offsets into asset_pos */
+  const int32_t* asset_pos;      /* monitor positions of each asset's cells */
+  const double* asset_threshold; /* eta_k [m] */
+  const double* asset_weight;    /* w_k */
+  int32_t n_guard;
+  const int32_t* guard_pos;      /* monitor positions, in guard-cell order */
+  const double* baseline_max;    /* n_mon baseline maxima, or NULL (no guard test) */
+  double guard_tolerance;        /* eps_G [m] */
+  double tau;                    /* softplus scale [m] */
+  double cut_cost, fill_cost, earth_weight;
+  int32_t require_no_worsening;
+  int32_t guard_abort;           /* 1: stop a design at its first breached sync point */
+  int32_t has_incumbent;         /* 1: incumbent abort live (frozen for the batch)  */
+  double incumbent;
+} itr_objective;
+
+/* Per-design results, caller-allocated. Array members may be NULL (not wanted). The
+ * reference's BatchRun (evaluator.rs:118-125) is {monitor_max, steps, cell_updates, bad}. */
+typedef struct itr_result {
+  double* monitor_max;      /* n_mon: running max depth at monitored cells (f64) */
+  float* peak;              /* nx*ny: running max depth of every cell, or NULL */
+  float* depth;             /* nx*ny: final depth (GpuRun::depth), or NULL */
+  double* ledger;           /* max_rows * 8: t, volume, rain, inflow, outflow, infil, fix, residual */
+  int32_t max_rows;
+  /* written by the library: */
+  uint64_t steps;
+  uint64_t cell_updates;    /* steps * nx * ny (gpubench.rs:28) */
+  double t_end;
+  uint32_t sync_count;
+  int32_t status;           /* itr_run_status */
+  uint32_t breach_cell;     /* guard abort: cell id of the worst guard cell */
+  uint32_t breach_sync;     /* guard abort: sync index of the breach */
+  double violation;         /* guard abort: exceedance [m]; else guard violation of the finished run */
+  double lower_bound;       /* incumbent abort: running J lower bound */
+  double j;                 /* objective J of the run (monitor maxima so far), if obj given */
+  int32_t feasible;         /* 1 if no guard violation (objective.rs:126) */
+  int32_t n_rows;           /* ledger rows written */
+  double volume_m3;         /* stored volume at the end */
+  double rel_residual;      /* |ledger residual| / gross input at the last sync */
+} itr_result;
+
+/* GpuSolver::new (lib.rs:85). device < 0 selects the current device. Returns NULL on
+ * failure with the reason in err. */
+itr_ctx* itr_gpu_create(int device, char* err, size_t errlen);
+
+void itr_gpu_destroy(itr_ctx* ctx);
+
+/* Text of the last failure on this context (never NULL). */
+const char* itr_gpu_last_error(itr_ctx* ctx);
+
+/* GpuSolver::adapter_info (lib.rs:126): device name, SM count, memory, build. */
+int itr_gpu_info(itr_ctx* ctx, char* buf, size_t len);
+
+/* GpuSolver::run_batch (lib.rs:149) / BatchBackend::run (evaluator.rs:134): run every design
+ * to its end (or its abort), one result per design, all from host buffers. Designs run
+ * concurrently in one persistent launch, one design per thread-block cluster. */
+int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n_designs,
+                      const itr_design* designs, const uint32_t* monitors, int32_t n_mon,
+                      const itr_objective* obj, itr_result* results);
+
+/* Options (GpuSolver::steps_per_submit, lib.rs:70, is the reference's one knob):
+ *   "impl"     0 = batched cluster kernel (default), 1 = plain one-design-per-launch kernel
+ *   "threads"  threads per CTA of the batched kernel (0 = autotune)
+ *   "cluster"  CTAs per design of the batched kernel (0 = autotune)
+ *   "graph"    1 = capture the batched launch and its copies in a CUDA graph (default 1)
+ *   "steps_per_submit"  plain kernel: steps between host polls (default 64)
+ * Returns ITR_INVALID_ARG for an unknown key. */
+int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value);
+
+/* Timing of the last run_batch on the device, CUDA events on the context stream:
+ * kernel_ms = the forward kernel(s) alone, total_ms = copies + kernels. last_cell_updates
+ * mirrors GpuSolver::last_cell_updates (lib.rs:72). */
+int itr_gpu_last_timing(itr_ctx* ctx, double* kernel_ms, double* total_ms, uint64_t* last_cell_updates,
+                        int32_t* launches);
+
+/* Re-run the last batch with its inputs still resident on the device (no host copies),
+ * results kept on the device; for timing the kernel over resident inputs. */
+int itr_gpu_rerun_resident(itr_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ITR_GPU_H */

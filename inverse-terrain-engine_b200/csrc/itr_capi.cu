@@ -1,0 +1,701 @@
+// itr_capi.cu — the C ABI (include/itr_gpu.h): context, input checks, packing, launch
+// configuration and autotuning, result assembly.
+//
+// Mirrors crates/itr-gpu/src/lib.rs: GpuSolver::new (:85) -> itr_gpu_create,
+// run_batch (:149) -> itr_gpu_run_batch, adapter_info (:126) -> itr_gpu_info, and the
+// rejections of unsupported inputs (:154-176, backend.rs:53-55) -> ITR_UNSUPPORTED.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <cstdarg>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <map>
+#include <tuple>
+#include <algorithm>
+#include <chrono>
+#include "../../include/itr_gpu.h"
+#include "itr_device.cuh"
+#include "itr_batched.cuh"
+#include "itr_plain.cuh"
+
+using namespace itr;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr; n = 0;
+    size_t b = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) n = b;
+    return e;
+  }
+  void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct HostBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n && p) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr; n = 0;
+    size_t b = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMallocHost(&p, b);
+    if (e == cudaSuccess) n = b;
+    return e;
+  }
+  void release() { if (p) cudaFreeHost(p); p = nullptr; n = 0; }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct LaunchCfg {
+  int C = 1, T = 512, W = 1, S = 1;
+  size_t smem = 0;
+  bool ok = false;
+};
+
+}  // namespace
+
+struct itr_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  char name[256] = {0};
+  std::string err;
+  // options
+  int impl = 0, threads = 0, cluster = 0, graph = 1, steps_per_submit = 64;
+  // device buffers (batched path)
+  DevBuf wet, gn2, bc, dzx, dzy, dzx2, dzy2, h0, cut, fill, mon, obj_i, obj_d, peak, depth, ledger, out, mmax;
+  // plain path scratch
+  DevBuf pH, pQX, pQY, pPK, ppart, pctl;
+  HostBuf stage, hout;
+  // last run
+  double kernel_ms = 0, total_ms = 0;
+  uint64_t cell_updates = 0;
+  int launches = 0;
+  bool have_last = false;
+  BatchArgs last_args;
+  LaunchCfg last_cfg;
+  // plain rerun
+  std::vector<PlainArgs> last_plain;
+  std::vector<int> last_plain_blocks;
+  bool last_was_plain = false;
+  // autotune cache: (nx, ny, n_designs, mode) -> cfg
+  std::map<std::tuple<int, int, int, int>, LaunchCfg> tuned;
+  cudaGraphExec_t gexec = nullptr;
+};
+
+static int fail(itr_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CU(x)                                                                                    \
+  do {                                                                                           \
+    cudaError_t e_ = (x);                                                                        \
+    if (e_ != cudaSuccess) return fail(ctx, ITR_DEVICE_ERROR, "%s: %s", #x, cudaGetErrorString(e_)); \
+  } while (0)
+
+// ------------------------------------------------------------------ kernels table ----
+typedef void (*BatchedFn)(const BatchArgs);
+
+static BatchedFn batched_fn(bool crest, bool clustered, int maxt) {
+#define PICK(CR, CL)                                                  \
+  if (maxt <= 256) return k_batched<CR, CL, 256>;                     \
+  if (maxt <= 512) return k_batched<CR, CL, 512>;                     \
+  if (maxt <= 768) return k_batched<CR, CL, 768>;                     \
+  return k_batched<CR, CL, 1024>;
+  if (crest) { if (clustered) { PICK(true, true) } else { PICK(true, false) } }
+  else { if (clustered) { PICK(false, true) } else { PICK(false, false) } }
+#undef PICK
+}
+
+static int maxt_bucket(int T) { return T <= 256 ? 256 : T <= 512 ? 512 : T <= 768 ? 768 : 1024; }
+
+// Geometry of the batched kernel for (nx, ny) with C CTAs per design and about T threads.
+static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_target) {
+  LaunchCfg c;
+  c.C = C;
+  c.W = (nx + 1 + 31) / 32;
+  if (C < 1 || ny < C) return c;
+  const int nr_min = ny / C, nr_max = (ny + C - 1) / C;
+  int S = T_target / (32 * c.W);
+  if (c.W > 1 && S > 15) S = 15;   // one named barrier per strip (ids 1..15)
+  if (S > nr_min) S = nr_min;
+  if (S < 1) return c;
+  c.S = S;
+  c.T = S * 32 * c.W;
+  if (c.T > 1024) return c;
+  c.smem = batched_smem_bytes(nr_max, nx, S, c.W, c.T / 32);
+  c.ok = c.smem <= ctx->smem_optin;
+  return c;
+}
+
+static int launch_batched(itr_ctx* ctx, const BatchArgs& A, const LaunchCfg& cfg, int n_designs) {
+  const bool crest = A.mode == 1, clustered = cfg.C > 1;
+  BatchedFn fn = batched_fn(crest, clustered, maxt_bucket(cfg.T));
+  CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+  cudaLaunchConfig_t lc;
+  memset(&lc, 0, sizeof(lc));
+  lc.gridDim = dim3((unsigned)(n_designs * cfg.C), 1, 1);
+  lc.blockDim = dim3((unsigned)cfg.T, 1, 1);
+  lc.dynamicSmemBytes = cfg.smem;
+  lc.stream = ctx->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cfg.C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  CU(cudaLaunchKernelEx(&lc, fn, A));
+  return ITR_OK;
+}
+
+static int max_active_clusters(itr_ctx* ctx, const LaunchCfg& cfg, bool crest) {
+  BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T));
+  if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem) != cudaSuccess) return 0;
+  cudaLaunchConfig_t lc;
+  memset(&lc, 0, sizeof(lc));
+  lc.gridDim = dim3((unsigned)(cfg.C * 148), 1, 1);
+  lc.blockDim = dim3((unsigned)cfg.T, 1, 1);
+  lc.dynamicSmemBytes = cfg.smem;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cfg.C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, fn, &lc) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return n;
+}
+
+// Candidate configurations, best-first by a simple model: time ~ waves * work per CTA.
+static std::vector<LaunchCfg> candidates(itr_ctx* ctx, int nx, int ny, int n_designs, bool crest) {
+  std::vector<std::pair<double, LaunchCfg>> v;
+  for (int C : {1, 2, 4, 8}) {
+    for (int T : {256, 512, 768, 1024}) {
+      LaunchCfg c = make_cfg(ctx, nx, ny, C, T);
+      if (!c.ok) continue;
+      int act = max_active_clusters(ctx, c, crest);
+      if (act <= 0) continue;
+      double waves = std::ceil((double)n_designs / act);
+      double rows = std::ceil((double)ny / C);
+      // per-CTA cost ~ cells per thread; small penalty per cluster barrier
+      double per_step = rows * nx / (double)c.T * (1.0 + 0.02 * (C - 1)) + 0.5;
+      double cost = waves * per_step;
+      v.push_back({cost, c});
+    }
+  }
+  std::sort(v.begin(), v.end(), [](const std::pair<double, LaunchCfg>& a, const std::pair<double, LaunchCfg>& b) { return a.first < b.first; });
+  std::vector<LaunchCfg> out;
+  for (auto& p : v) out.push_back(p.second);
+  return out;
+}
+
+// ------------------------------------------------------------------ input checks ------
+static int check_inputs(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
+                        const uint32_t* mon, int32_t n_mon, const itr_objective* ob) {
+  if (!p || !g) return fail(ctx, ITR_INVALID_ARG, "params and grid are required");
+  if (n < 0) return fail(ctx, ITR_INVALID_ARG, "negative design count");
+  if (n > 0 && !ds) return fail(ctx, ITR_INVALID_ARG, "designs is NULL");
+  if (g->nx < 1 || g->ny < 1) return fail(ctx, ITR_INVALID_ARG, "grid must have nx, ny >= 1");
+  if ((int64_t)g->nx * g->ny > (1ll << 30)) return fail(ctx, ITR_INVALID_ARG, "grid too large");
+  if (!(g->dx > 0.0) || !(g->dy > 0.0)) return fail(ctx, ITR_INVALID_ARG, "cell size must be positive");
+  if (!g->wet || !g->gn2 || !g->bc) return fail(ctx, ITR_INVALID_ARG, "grid arrays wet, gn2, bc are required");
+  if (g->mode != ITR_FACE_SIGNED && g->mode != ITR_FACE_CREST) return fail(ctx, ITR_INVALID_ARG, "unknown face mode %d", g->mode);
+  for (int64_t i = 0; i < 2ll * g->nx + 2ll * g->ny; ++i) {
+    if (g->bc[i] == ITR_BC_STAGE) return fail(ctx, ITR_UNSUPPORTED, "Stage boundaries are not supported on the GPU backend");
+    if (g->bc[i] == ITR_BC_INFLOW) return fail(ctx, ITR_UNSUPPORTED, "Inflow boundaries are not supported on the GPU backend");
+    if (g->bc[i] > ITR_BC_INFLOW) return fail(ctx, ITR_INVALID_ARG, "unknown boundary code %d", (int)g->bc[i]);
+  }
+  if (p->inflow_scale != 1.0) return fail(ctx, ITR_UNSUPPORTED, "inflow scaling is not supported on the GPU backend");
+  if (!(p->duration_s >= 0.0) || !(p->sync_interval_s > 0.0) || !(p->cfl > 0.0) || !(p->dt_max_s > 0.0))
+    return fail(ctx, ITR_INVALID_ARG, "duration, sync interval, cfl and dt_max must be positive");
+  if (p->n_rain < 0 || p->n_rain > kMaxRain) return fail(ctx, ITR_INVALID_ARG, "hyetograph has %d points (max %d)", p->n_rain, kMaxRain);
+  if (p->n_rain > 0 && (!p->rain_t || !p->rain_rate)) return fail(ctx, ITR_INVALID_ARG, "hyetograph arrays are NULL");
+  if (n_mon < 0 || (n_mon > 0 && !mon)) return fail(ctx, ITR_INVALID_ARG, "monitor list is invalid");
+  for (int32_t k = 0; k < n_mon; ++k)
+    if ((int64_t)mon[k] >= (int64_t)g->nx * g->ny) return fail(ctx, ITR_INVALID_ARG, "monitor cell out of range");
+  for (int32_t d = 0; d < n; ++d) {
+    if (!ds[d].dzx || !ds[d].dzy) return fail(ctx, ITR_INVALID_ARG, "design %d has no face jumps", d);
+    if (g->mode == ITR_FACE_CREST && (!ds[d].dzx2 || !ds[d].dzy2)) return fail(ctx, ITR_INVALID_ARG, "design %d: crest mode needs dzx2/dzy2", d);
+  }
+  if (ob) {
+    if (ob->n_assets < 0 || ob->n_guard < 0) return fail(ctx, ITR_INVALID_ARG, "objective counts are negative");
+    if (ob->n_assets > 0 && (!ob->asset_off || !ob->asset_pos || !ob->asset_threshold || !ob->asset_weight))
+      return fail(ctx, ITR_INVALID_ARG, "objective asset arrays are NULL");
+    for (int a = 0; a < ob->n_assets; ++a)
+      for (int m = ob->asset_off[a]; m < ob->asset_off[a + 1]; ++m)
+        if (ob->asset_pos[m] < 0 || ob->asset_pos[m] >= n_mon) return fail(ctx, ITR_INVALID_ARG, "asset position out of range");
+    if (ob->n_guard > 0 && !ob->guard_pos) return fail(ctx, ITR_INVALID_ARG, "guard positions are NULL");
+    for (int k = 0; k < ob->n_guard; ++k)
+      if (ob->guard_pos[k] < 0 || ob->guard_pos[k] >= n_mon) return fail(ctx, ITR_INVALID_ARG, "guard position out of range");
+    if (!(ob->tau > 0.0)) return fail(ctx, ITR_INVALID_ARG, "tau must be positive");
+  }
+  return ITR_OK;
+}
+
+static RunParams make_run_params(const itr_params* p, const itr_grid* g) {
+  RunParams P;
+  memset(&P, 0, sizeof(P));
+  P.duration = p->duration_s; P.sync = p->sync_interval_s; P.cfl = p->cfl; P.dt_max = p->dt_max_s;
+  P.h_dry = p->h_dry; P.h_eps = p->h_eps; P.infil = p->infil_capacity; P.initial_depth = p->initial_depth;
+  P.dx = g->dx; P.dy = g->dy; P.g = g->g; P.area = g->dx * g->dy; P.wet_count = (double)g->wet_count;
+  P.n_sync = (uint32_t)std::ceil(p->duration_s / p->sync_interval_s);
+  P.skip_dry = p->skip_dry;
+  P.rain.n = p->n_rain;
+  for (int i = 0; i < p->n_rain; ++i) { P.rain.t[i] = p->rain_t[i]; P.rain.r[i] = p->rain_rate[i]; }
+  return P;
+}
+
+// Host copy of the objective (objective.rs:94-128) for J and feasibility of a finished run.
+static void host_objective(const itr_objective* ob, const double* mm, double cut, double fill, double& j, double& worst) {
+  double jr = 0.0;
+  for (int a = 0; a < ob->n_assets; ++a) {
+    double pk = 0.0;
+    for (int m = ob->asset_off[a]; m < ob->asset_off[a + 1]; ++m) { double x = mm[ob->asset_pos[m]]; pk = pk > x ? pk : x; }
+    jr += ob->asset_weight[a] * ob->tau * itr_math::softplus((pk - ob->asset_threshold[a]) / ob->tau);
+  }
+  j = jr + ob->earth_weight * (ob->cut_cost * cut + ob->fill_cost * fill);
+  worst = 0.0;
+  if (ob->baseline_max)
+    for (int k = 0; k < ob->n_guard; ++k) {
+      int mp = ob->guard_pos[k];
+      double w = mm[mp] - ob->baseline_max[mp];
+      worst = worst > w ? worst : w;
+    }
+}
+
+// Gather monitor maxima from the per-cell peak array on the device.
+__global__ void k_gather_monitors(const float* peak, const unsigned* mon, int n_mon, size_t cells, int n_designs, float* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_mon * n_designs) return;
+  int d = i / n_mon, k = i % n_mon;
+  out[i] = peak[(size_t)d * cells + mon[k]];
+}
+
+extern "C" {
+
+itr_ctx* itr_gpu_create(int device, char* err, size_t errlen) {
+  auto bad = [&](const char* what, cudaError_t e) -> itr_ctx* {
+    if (err && errlen) snprintf(err, errlen, "%s: %s", what, cudaGetErrorString(e));
+    return nullptr;
+  };
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) return bad("cudaGetDeviceCount", e);
+  if (n == 0) { if (err && errlen) snprintf(err, errlen, "no CUDA device"); return nullptr; }
+  int dev = device;
+  if (dev < 0) { e = cudaGetDevice(&dev); if (e != cudaSuccess) return bad("cudaGetDevice", e); }
+  if (dev >= n) { if (err && errlen) snprintf(err, errlen, "device %d out of range (%d devices)", dev, n); return nullptr; }
+  e = cudaSetDevice(dev);
+  if (e != cudaSuccess) return bad("cudaSetDevice", e);
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, dev);
+  if (e != cudaSuccess) return bad("cudaGetDeviceProperties", e);
+  if (prop.major < 10) {
+    if (err && errlen) snprintf(err, errlen, "device %d (%s, sm_%d%d) is not sm_100; this build targets B200 only", dev, prop.name, prop.major, prop.minor);
+    return nullptr;
+  }
+  itr_ctx* c = new itr_ctx();
+  c->device = dev;
+  c->sm_count = prop.multiProcessorCount;
+  c->smem_optin = prop.sharedMemPerBlockOptin;
+  snprintf(c->name, sizeof(c->name), "%s", prop.name);
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return bad("cudaStreamCreate", e); }
+  for (int i = 0; i < 4; ++i) cudaEventCreate(&c->ev[i]);
+  return c;
+}
+
+void itr_gpu_destroy(itr_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  for (DevBuf* b : {&ctx->wet, &ctx->gn2, &ctx->bc, &ctx->dzx, &ctx->dzy, &ctx->dzx2, &ctx->dzy2, &ctx->h0, &ctx->cut, &ctx->fill,
+                    &ctx->mon, &ctx->obj_i, &ctx->obj_d, &ctx->peak, &ctx->depth, &ctx->ledger, &ctx->out, &ctx->mmax,
+                    &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl})
+    b->release();
+  ctx->stage.release();
+  ctx->hout.release();
+  for (int i = 0; i < 4; ++i) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* itr_gpu_last_error(itr_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int itr_gpu_info(itr_ctx* ctx, char* buf, size_t len) {
+  if (!ctx || !buf || !len) return ITR_INVALID_ARG;
+  size_t fr = 0, tot = 0;
+  cudaSetDevice(ctx->device);
+  cudaMemGetInfo(&fr, &tot);
+  snprintf(buf, len, "%s (device %d, %d SMs, %.1f GB, %zu B smem/CTA opt-in; itr_gpu ABI %d, sm_100a)", ctx->name, ctx->device,
+           ctx->sm_count, tot / 1e9, ctx->smem_optin, ITR_GPU_ABI_VERSION);
+  return ITR_OK;
+}
+
+int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
+  if (!ctx || !key) return ITR_INVALID_ARG;
+  std::string k(key);
+  if (k == "impl") { if (value < 0 || value > 1) return fail(ctx, ITR_INVALID_ARG, "impl must be 0 or 1"); ctx->impl = (int)value; }
+  else if (k == "threads") { if (value < 0 || value > 1024) return fail(ctx, ITR_INVALID_ARG, "threads out of range"); ctx->threads = (int)value; }
+  else if (k == "cluster") { if (!(value == 0 || value == 1 || value == 2 || value == 4 || value == 8)) return fail(ctx, ITR_INVALID_ARG, "cluster must be 0,1,2,4,8"); ctx->cluster = (int)value; }
+  else if (k == "graph") ctx->graph = value != 0;
+  else if (k == "steps_per_submit") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "steps_per_submit must be >= 1"); ctx->steps_per_submit = (int)value; }
+  else return fail(ctx, ITR_INVALID_ARG, "unknown option '%s'", key);
+  if (k == "threads" || k == "cluster") ctx->tuned.clear();
+  return ITR_OK;
+}
+
+int itr_gpu_last_timing(itr_ctx* ctx, double* kernel_ms, double* total_ms, uint64_t* cell_updates, int32_t* launches) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (kernel_ms) *kernel_ms = ctx->kernel_ms;
+  if (total_ms) *total_ms = ctx->total_ms;
+  if (cell_updates) *cell_updates = ctx->cell_updates;
+  if (launches) *launches = ctx->launches;
+  return ITR_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ plain path ------
+static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid, int* launches) {
+  k_plain_init<<<1, 1024, 0, ctx->stream>>>(A);
+  k_plain_finalize<<<1, 32, 0, ctx->stream>>>(A, n_blocks, 1);
+  *launches += 2;
+  int done = 0;
+  PlainCtl* hctl = ctx->hout.as<PlainCtl>();
+  for (uint64_t guard = 0;; ++guard) {
+    for (int s = 0; s < ctx->steps_per_submit; ++s) {
+      if (A.mode == 1) k_plain_update<true><<<grid, 256, 0, ctx->stream>>>(A);
+      else k_plain_update<false><<<grid, 256, 0, ctx->stream>>>(A);
+      k_plain_finalize<<<1, 32, 0, ctx->stream>>>(A, n_blocks, 0);
+      *launches += 2;
+    }
+    CU(cudaMemcpyAsync(hctl, A.ctl, sizeof(PlainCtl), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    done = hctl->done;
+    if (done) break;
+    if (guard > 100000000ull) return fail(ctx, ITR_DEVICE_TIMEOUT, "plain run did not terminate");
+  }
+  return ITR_OK;
+}
+
+// ------------------------------------------------------------------ run_batch -------
+extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
+                                 const uint32_t* mon, int32_t n_mon, const itr_objective* ob, itr_result* res) {
+  if (!ctx) return ITR_INVALID_ARG;
+  int rc = check_inputs(ctx, p, g, n, ds, mon, n_mon, ob);
+  if (rc != ITR_OK) return rc;
+  if (n == 0) { ctx->kernel_ms = ctx->total_ms = 0; ctx->cell_updates = 0; ctx->launches = 0; return ITR_OK; }
+  if (!res) return fail(ctx, ITR_INVALID_ARG, "results is NULL");
+  CU(cudaSetDevice(ctx->device));
+  const int nx = g->nx, ny = g->ny;
+  const size_t N = (size_t)nx * ny, SX = (size_t)ny * (nx + 1), SY = (size_t)(ny + 1) * nx;
+  const bool crest = g->mode == ITR_FACE_CREST;
+  int max_rows = 0;
+  for (int d = 0; d < n; ++d) if (res[d].ledger && res[d].max_rows > max_rows) max_rows = res[d].max_rows;
+  const int n_assets = ob ? ob->n_assets : 0, n_guard = ob ? ob->n_guard : 0;
+  const int n_apos = ob && n_assets > 0 ? ob->asset_off[n_assets] : 0;
+
+  // ---- pack into pinned staging ----
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes, 256); return o; };
+  const size_t o_wet = take(N * 4), o_gn2 = take(N * 4), o_bc = take(2 * (size_t)(nx + ny));
+  const size_t o_dzx = take(n * SX * 4), o_dzy = take(n * SY * 4);
+  const size_t o_dzx2 = crest ? take(n * SX * 4) : 0, o_dzy2 = crest ? take(n * SY * 4) : 0;
+  const size_t o_h0 = take(n * N * 4), o_cut = take((size_t)n * 8), o_fill = take((size_t)n * 8);
+  const size_t o_mon = take((size_t)(n_mon > 0 ? n_mon : 1) * 4);
+  const size_t o_oi = take((size_t)(n_assets + 1 + n_apos + n_guard + 1) * 4);
+  const size_t o_od = take((size_t)(2 * n_assets + (n_mon > 0 ? n_mon : 1)) * 8);
+  const size_t in_bytes = off;
+  CU(ctx->stage.ensure(in_bytes));
+  unsigned char* st = ctx->stage.as<unsigned char>();
+  memcpy(st + o_wet, g->wet, N * 4);
+  memcpy(st + o_gn2, g->gn2, N * 4);
+  memcpy(st + o_bc, g->bc, 2 * (size_t)(nx + ny));
+  const float hinit = (float)(p->initial_depth > 0.0 ? p->initial_depth : 0.0);
+  for (int d = 0; d < n; ++d) {
+    memcpy(st + o_dzx + d * SX * 4, ds[d].dzx, SX * 4);
+    memcpy(st + o_dzy + d * SY * 4, ds[d].dzy, SY * 4);
+    if (crest) { memcpy(st + o_dzx2 + d * SX * 4, ds[d].dzx2, SX * 4); memcpy(st + o_dzy2 + d * SY * 4, ds[d].dzy2, SY * 4); }
+    float* h0 = reinterpret_cast<float*>(st + o_h0) + d * N;
+    if (ds[d].h0) memcpy(h0, ds[d].h0, N * 4);
+    else for (size_t i = 0; i < N; ++i) h0[i] = g->wet[i] != 0.0f ? (hinit == 0.0f ? 0.0f : hinit) : 0.0f;  // init_state
+    reinterpret_cast<double*>(st + o_cut)[d] = ds[d].cut_m3;
+    reinterpret_cast<double*>(st + o_fill)[d] = ds[d].fill_m3;
+  }
+  if (n_mon > 0) memcpy(st + o_mon, mon, (size_t)n_mon * 4);
+  int* oi = reinterpret_cast<int*>(st + o_oi);
+  double* od = reinterpret_cast<double*>(st + o_od);
+  if (ob) {
+    for (int a = 0; a <= n_assets; ++a) oi[a] = n_assets > 0 ? ob->asset_off[a] : 0;
+    for (int m = 0; m < n_apos; ++m) oi[n_assets + 1 + m] = ob->asset_pos[m];
+    for (int k = 0; k < n_guard; ++k) oi[n_assets + 1 + n_apos + k] = ob->guard_pos[k];
+    for (int a = 0; a < n_assets; ++a) { od[a] = ob->asset_threshold[a]; od[n_assets + a] = ob->asset_weight[a]; }
+    if (ob->baseline_max) for (int k = 0; k < n_mon; ++k) od[2 * n_assets + k] = ob->baseline_max[k];
+  }
+
+  // ---- device buffers ----
+  CU(ctx->dzx.ensure(in_bytes));  // one slab for all inputs
+  unsigned char* dv = ctx->dzx.as<unsigned char>();
+  CU(ctx->peak.ensure(n * N * 4));
+  CU(ctx->depth.ensure(n * N * 4));
+  CU(ctx->ledger.ensure((size_t)n * (max_rows > 0 ? max_rows : 1) * 8 * 8));
+  CU(ctx->out.ensure((size_t)n * sizeof(DesignOut)));
+  CU(ctx->mmax.ensure((size_t)n * (n_mon > 0 ? n_mon : 1) * 4));
+  const size_t out_bytes = (size_t)n * sizeof(DesignOut) + (size_t)n * (n_mon > 0 ? n_mon : 1) * 4 +
+                           (size_t)n * (max_rows > 0 ? max_rows : 1) * 64 + 2 * n * N * 4 + 1024;
+  CU(ctx->hout.ensure(out_bytes > sizeof(PlainCtl) ? out_bytes : sizeof(PlainCtl)));
+
+  RunParams P = make_run_params(p, g);
+  DevObjective DO;
+  memset(&DO, 0, sizeof(DO));
+  if (ob) {
+    DO.enabled = 1;
+    DO.n_assets = n_assets;
+    DO.asset_off = reinterpret_cast<const int*>(dv + o_oi);
+    DO.asset_pos = DO.asset_off + n_assets + 1;
+    DO.guard_pos = DO.asset_pos + n_apos;
+    DO.n_guard = n_guard;
+    DO.asset_thr = reinterpret_cast<const double*>(dv + o_od);
+    DO.asset_w = DO.asset_thr + n_assets;
+    DO.baseline = ob->baseline_max ? DO.asset_thr + 2 * n_assets : nullptr;
+    DO.tol = ob->guard_tolerance; DO.tau = ob->tau; DO.cut_cost = ob->cut_cost; DO.fill_cost = ob->fill_cost;
+    DO.earth_w = ob->earth_weight; DO.require = ob->require_no_worsening; DO.guard_abort = ob->guard_abort;
+    DO.has_incumbent = ob->has_incumbent; DO.incumbent = ob->incumbent;
+  }
+
+  CU(cudaEventRecord(ctx->ev[0], ctx->stream));
+#ifdef ITR_CHECKED
+  {
+    unsigned long long z[4] = {0, 0, 0, 0};
+    CU(cudaMemcpyToSymbolAsync(g_itr_err, z, sizeof(z), 0, cudaMemcpyHostToDevice, ctx->stream));
+  }
+#endif
+  CU(cudaMemcpyAsync(dv, st, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  int launches = 0;
+  const unsigned long long max_steps = 2000000000ull;
+
+  if (ctx->impl == 0) {
+    BatchArgs A;
+    memset(&A, 0, sizeof(A));
+    A.P = P; A.nx = nx; A.ny = ny; A.mode = g->mode; A.n_designs = n;
+    A.wet = reinterpret_cast<const float*>(dv + o_wet);
+    A.gn2 = reinterpret_cast<const float*>(dv + o_gn2);
+    A.bc = reinterpret_cast<const uint8_t*>(dv + o_bc);
+    A.dzx = reinterpret_cast<const float*>(dv + o_dzx);
+    A.dzy = reinterpret_cast<const float*>(dv + o_dzy);
+    A.dzx2 = crest ? reinterpret_cast<const float*>(dv + o_dzx2) : nullptr;
+    A.dzy2 = crest ? reinterpret_cast<const float*>(dv + o_dzy2) : nullptr;
+    A.h0 = reinterpret_cast<const float*>(dv + o_h0);
+    A.cut = reinterpret_cast<const double*>(dv + o_cut);
+    A.fill = reinterpret_cast<const double*>(dv + o_fill);
+    A.n_mon = n_mon;
+    A.mon_cells = reinterpret_cast<const unsigned*>(dv + o_mon);
+    A.obj = DO;
+    A.peak_out = ctx->peak.as<float>();
+    A.depth_out = ctx->depth.as<float>();
+    A.ledger_out = max_rows > 0 ? ctx->ledger.as<double>() : nullptr;
+    A.max_rows = max_rows;
+    A.out = ctx->out.as<DesignOut>();
+    A.max_steps = max_steps;
+    // launch configuration
+    LaunchCfg cfg;
+    auto key = std::make_tuple(nx, ny, n, (int)g->mode);
+    if (ctx->cluster > 0 || ctx->threads > 0) {
+      cfg = make_cfg(ctx, nx, ny, ctx->cluster > 0 ? ctx->cluster : 1, ctx->threads > 0 ? ctx->threads : 512);
+      if (!cfg.ok) return fail(ctx, ITR_UNSUPPORTED, "cluster=%d threads=%d does not fit a %dx%d grid in shared memory", ctx->cluster, ctx->threads, nx, ny);
+    } else if (ctx->tuned.count(key)) {
+      cfg = ctx->tuned[key];
+    } else {
+      std::vector<LaunchCfg> cands = candidates(ctx, nx, ny, n, crest);
+      if (cands.empty()) return fail(ctx, ITR_UNSUPPORTED, "a %dx%d grid does not fit the batched kernel's shared memory (max 8 CTAs per design)", nx, ny);
+      cfg = cands[0];
+      ctx->tuned[key] = cfg;
+    }
+    A.C = cfg.C; A.W = cfg.W; A.S = cfg.S;
+    CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+    rc = launch_batched(ctx, A, cfg, n);
+    if (rc != ITR_OK) return rc;
+    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+    launches += 1;
+    ctx->last_args = A;
+    ctx->last_cfg = cfg;
+    ctx->have_last = true;
+    ctx->last_was_plain = false;
+  } else {
+    // plain: one design after another
+    CU(ctx->pH.ensure(2 * N * 4)); CU(ctx->pQX.ensure(2 * N * 4)); CU(ctx->pQY.ensure(2 * N * 4));
+    CU(ctx->pPK.ensure(N * 4));
+    dim3 grid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile);
+    int nb = grid.x * grid.y;
+    CU(ctx->ppart.ensure((size_t)nb * 5 * 8));
+    CU(ctx->pctl.ensure(sizeof(PlainCtl)));
+    CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+    ctx->last_plain.clear();
+    ctx->last_plain_blocks.clear();
+    for (int d = 0; d < n; ++d) {
+      PlainArgs A;
+      memset(&A, 0, sizeof(A));
+      A.P = P; A.nx = nx; A.ny = ny; A.mode = g->mode;
+      A.wet = reinterpret_cast<const float*>(dv + o_wet);
+      A.gn2 = reinterpret_cast<const float*>(dv + o_gn2);
+      A.bc = reinterpret_cast<const uint8_t*>(dv + o_bc);
+      A.dzx = reinterpret_cast<const float*>(dv + o_dzx) + d * SX;
+      A.dzy = reinterpret_cast<const float*>(dv + o_dzy) + d * SY;
+      A.dzx2 = crest ? reinterpret_cast<const float*>(dv + o_dzx2) + d * SX : nullptr;
+      A.dzy2 = crest ? reinterpret_cast<const float*>(dv + o_dzy2) + d * SY : nullptr;
+      A.h0 = reinterpret_cast<const float*>(dv + o_h0) + d * N;
+      A.cut = ds[d].cut_m3; A.fill = ds[d].fill_m3;
+      A.n_mon = n_mon; A.mon_cells = reinterpret_cast<const unsigned*>(dv + o_mon);
+      A.obj = DO;
+      A.H = ctx->pH.as<float>(); A.QX = ctx->pQX.as<float>(); A.QY = ctx->pQY.as<float>(); A.PK = ctx->pPK.as<float>();
+      A.part = ctx->ppart.as<double>(); A.ctl = ctx->pctl.as<PlainCtl>();
+      A.ledger = max_rows > 0 ? ctx->ledger.as<double>() + (size_t)d * max_rows * 8 : nullptr;
+      A.max_rows = max_rows;
+      A.max_steps = max_steps;
+      rc = run_plain_design(ctx, A, nb, grid, &launches);
+      if (rc != ITR_OK) return rc;
+      // copy this design's outputs into the batched output slots
+      PlainCtl* hc = ctx->hout.as<PlainCtl>();
+      DesignOut o;
+      memset(&o, 0, sizeof(o));
+      o.steps = hc->step; o.t_end = hc->t; o.sync_count = hc->sync_index; o.status = hc->status;
+      o.breach_cell = hc->breach_cell; o.breach_sync = hc->breach_sync; o.violation = hc->violation;
+      o.lower_bound = hc->lower_bound; o.v0 = hc->v0; o.volume = hc->volume; o.rel_residual = hc->rel_res; o.n_rows = hc->n_rows;
+      CU(cudaMemcpyAsync(ctx->out.as<DesignOut>() + d, &o, sizeof(o), cudaMemcpyHostToDevice, ctx->stream));
+      CU(cudaMemcpyAsync(ctx->peak.as<float>() + d * N, A.PK, N * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+      CU(cudaMemcpyAsync(ctx->depth.as<float>() + d * N, A.H + (size_t)hc->par * N, N * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+      CU(cudaStreamSynchronize(ctx->stream));
+      ctx->last_plain.push_back(A);
+      ctx->last_plain_blocks.push_back(nb);
+    }
+    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+    ctx->last_was_plain = true;
+    ctx->have_last = true;
+  }
+  CU(cudaGetLastError());
+
+  // ---- results back ----
+  unsigned char* ho = ctx->hout.as<unsigned char>();
+  size_t hoff = 0;
+  DesignOut* hdo = reinterpret_cast<DesignOut*>(ho);
+  hoff = align_up((size_t)n * sizeof(DesignOut), 256);
+  float* hmm = reinterpret_cast<float*>(ho + hoff);
+  hoff = align_up(hoff + (size_t)n * (n_mon > 0 ? n_mon : 1) * 4, 256);
+  double* hled = reinterpret_cast<double*>(ho + hoff);
+  hoff = align_up(hoff + (size_t)n * (max_rows > 0 ? max_rows : 1) * 64, 256);
+  CU(cudaMemcpyAsync(hdo, ctx->out.p, (size_t)n * sizeof(DesignOut), cudaMemcpyDeviceToHost, ctx->stream));
+  if (n_mon > 0) {
+    int tot = n_mon * n;
+    k_gather_monitors<<<(tot + 255) / 256, 256, 0, ctx->stream>>>(ctx->peak.as<float>(), reinterpret_cast<const unsigned*>(dv + o_mon), n_mon, N, n,
+                                                                   ctx->mmax.as<float>());
+    launches += 1;
+    CU(cudaMemcpyAsync(hmm, ctx->mmax.p, (size_t)tot * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (max_rows > 0) CU(cudaMemcpyAsync(hled, ctx->ledger.p, (size_t)n * max_rows * 64, cudaMemcpyDeviceToHost, ctx->stream));
+  for (int d = 0; d < n; ++d) {
+    if (res[d].peak) CU(cudaMemcpyAsync(res[d].peak, ctx->peak.as<float>() + d * N, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (res[d].depth) CU(cudaMemcpyAsync(res[d].depth, ctx->depth.as<float>() + d * N, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CU(cudaEventRecord(ctx->ev[3], ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+#ifdef ITR_CHECKED
+  {
+    unsigned long long e[4];
+    CU(cudaMemcpyFromSymbol(e, g_itr_err, sizeof(e)));
+    if (e[0]) return fail(ctx, ITR_DEVICE_ERROR, "checked build: bounds violation code %llu index %lld block %llu thread %llu",
+                          e[0], (long long)e[1], e[2], e[3]);
+  }
+#endif
+  float k_ms = 0, t_ms = 0;
+  cudaEventElapsedTime(&k_ms, ctx->ev[1], ctx->ev[2]);
+  cudaEventElapsedTime(&t_ms, ctx->ev[0], ctx->ev[3]);
+  ctx->kernel_ms = k_ms; ctx->total_ms = t_ms; ctx->launches = launches;
+  uint64_t cu = 0;
+  for (int d = 0; d < n; ++d) {
+    const DesignOut& o = hdo[d];
+    itr_result& r = res[d];
+    if (o.status >= 4) return fail(ctx, ITR_DEVICE_TIMEOUT, "design %d: run exceeded its step or wait limit (status %d)", d, o.status);
+    r.steps = o.steps;
+    r.cell_updates = o.steps * (uint64_t)N;
+    cu += r.cell_updates;
+    r.t_end = o.t_end;
+    r.sync_count = o.sync_count;
+    r.status = o.status;
+    r.breach_cell = o.breach_cell;
+    r.breach_sync = o.breach_sync;
+    r.lower_bound = o.lower_bound;
+    r.n_rows = o.n_rows < r.max_rows ? o.n_rows : r.max_rows;
+    r.volume_m3 = o.volume;
+    r.rel_residual = o.rel_residual;
+    if (r.monitor_max) for (int k = 0; k < n_mon; ++k) r.monitor_max[k] = (double)hmm[(size_t)d * n_mon + k];
+    if (r.ledger && r.max_rows > 0) memcpy(r.ledger, hled + (size_t)d * max_rows * 8, (size_t)r.n_rows * 64);
+    r.j = 0.0; r.feasible = 1; r.violation = 0.0;
+    if (ob) {
+      std::vector<double> mm(n_mon > 0 ? n_mon : 1);
+      for (int k = 0; k < n_mon; ++k) mm[k] = (double)hmm[(size_t)d * n_mon + k];
+      double j, worst;
+      host_objective(ob, mm.data(), ds[d].cut_m3, ds[d].fill_m3, j, worst);
+      r.j = j;
+      if (ob->require_no_worsening && ob->baseline_max && worst > ob->guard_tolerance) r.violation = worst - ob->guard_tolerance;
+      if (o.status == ITR_RUN_GUARD_ABORT) r.violation = o.violation;
+      r.feasible = (r.violation == 0.0 && o.status != ITR_RUN_GUARD_ABORT && o.status != ITR_RUN_UNHEALTHY) ? 1 : 0;
+    } else if (o.status == ITR_RUN_UNHEALTHY) {
+      r.feasible = 0;
+    }
+  }
+  ctx->cell_updates = cu;
+  return ITR_OK;
+}
+
+extern "C" int itr_gpu_rerun_resident(itr_ctx* ctx) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (!ctx->have_last) return fail(ctx, ITR_INVALID_ARG, "no previous batch to rerun");
+  CU(cudaSetDevice(ctx->device));
+  int launches = 0;
+  CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+  if (!ctx->last_was_plain) {
+    int rc = launch_batched(ctx, ctx->last_args, ctx->last_cfg, ctx->last_args.n_designs);
+    if (rc != ITR_OK) return rc;
+    launches = 1;
+  } else {
+    for (size_t i = 0; i < ctx->last_plain.size(); ++i) {
+      const PlainArgs& A0 = ctx->last_plain[i];
+      PlainArgs A = A0;
+      dim3 grid((A.nx + kTile - 1) / kTile, (A.ny + kTile - 1) / kTile);
+      int rc = run_plain_design(ctx, A, ctx->last_plain_blocks[i], grid, &launches);
+      if (rc != ITR_OK) return rc;
+    }
+  }
+  CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  CU(cudaGetLastError());
+  float k_ms = 0;
+  cudaEventElapsedTime(&k_ms, ctx->ev[1], ctx->ev[2]);
+  ctx->kernel_ms = k_ms;
+  ctx->total_ms = k_ms;
+  ctx->launches = launches;
+  return ITR_OK;
+}
