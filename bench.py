@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""Benchmark of the batched forward operator (one JSON line on rank 0).
+
+Workload (one "step"): one population evaluation of the plain batched configuration:
+120 x 96 cells at 5 m (rolling hills, 3 Gaussian hills + 2 gullies on a 3% slope), 60 min
+storm peaking at 100 mm/h at 20 min, 64 designs of 4 primitives each, run to completion
+(abort off), f32 state with f64 time/rain/ledgers. Synthetic, seeded inputs.
+
+  value    cell-steps/s of the batched kernel over inputs already resident in HBM (CUDA
+           events on the launching stream, L2 flushed between iterations)
+  e2e      the same metric through the public C ABI call (itr_gpu_run_batch) from host
+           buffers: packing, host->device copies, kernel, device->host results
+  roofline the batched kernel against the measured HBM copy bandwidth at 32 B/cell-step
+  cpu_baseline  the f32 CPU port of the reference's fused kernel (oracle/), candidate-parallel
+           on the host cores, on a bounded sample of the same workload
+
+Multi-GPU (torchrun): designs are sharded across ranks with no data-path collective (weak
+scaling: every rank runs its own 64-design population); a barrier brackets the timed
+region and the max time over ranks is reported.
+
+--impl reference: the reference cannot be built here (Rust workspace; no cargo/rustc), so
+its CPU path is timed through the restatement in oracle/ (f32 fused kernel, all host cores).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "inverse-terrain-engine_b200")
+sys.path[:0] = [PKG, os.path.join(ROOT, "tests")]
+
+METRIC = "cell-steps/s (batched forward, 1 design per cluster)"
+BYTES_PER_CELL_STEP = 32          # read h,qx,qy + write h,qx,qy (24 B) + dzx,dzy (8 B), spec.md:620
+BYTES_PER_CELL_STEP_REF_MODEL = 40  # the reference bench's model incl. wet and gn2, main.rs:696-697
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        import statistics
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        rank = int(os.environ["RANK"])
+        local = int(os.environ.get("LOCAL_RANK", rank))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        return rank, world, local
+    return 0, 1, 0
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.zeros(1, device="cuda")
+        dist.all_reduce(t)
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def workload(rank=0, n_designs=64):
+    from itr_gpu.scenes import config
+    sc = config(2)
+    ds = sc.designs(n_designs, seed=sc.design_seed + 1000 * rank)
+    return sc, [t for _, _, t in ds]
+
+
+def cpu_baseline(sc, terrs, budget_s=20.0):
+    """f32 fused CPU port, one design per thread on every host core, on a bounded sample:
+    the first `dur` seconds of the storm for one design per thread."""
+    import oracle_ref as orc
+    from helpers import base_arrays
+    import copy
+    threads = os.cpu_count() or 1
+    p = copy.deepcopy(sc.params)
+    # calibrate on one design for a short stretch, then size the sample to the budget
+    p.duration_s = 240.0
+    t0 = time.perf_counter()
+    w, steps, _ = orc.flat_batch(1, base_arrays(sc.base), [terrs[0].dzx], [terrs[0].dzy], None, p, sc.monitors)
+    rate1 = steps[0] * sc.base.nx * sc.base.ny / max(w, 1e-9)
+    n = min(len(terrs), threads)
+    # cell-steps the sample may take: budget * threads * single-thread rate
+    want = budget_s * rate1 * n * 0.8
+    per_design = want / n
+    full_steps_guess = 4.0 * steps[0] * (sc.params.duration_s / p.duration_s)
+    frac = min(1.0, per_design / max(full_steps_guess * sc.base.nx * sc.base.ny, 1.0))
+    p.duration_s = max(120.0, min(sc.params.duration_s, sc.params.duration_s * frac))
+    wall, steps, _ = orc.flat_batch(threads, base_arrays(sc.base), [t.dzx for t in terrs[:n]], [t.dzy for t in terrs[:n]], None,
+                                    p, sc.monitors)
+    cs = float(steps.sum()) * sc.base.nx * sc.base.ny
+    return {"value": cs / wall, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{n} designs x first {p.duration_s:.0f} s of the storm (of {sc.params.duration_s:.0f} s), "
+                      f"f32 fused CPU port, candidate-parallel on {threads} threads, {wall:.1f} s wall",
+            "cell_steps": cs, "wall_s": wall}
+
+
+def run_reference(args):
+    rank, world, _ = dist_setup(args.gpus)
+    if rank != 0:
+        barrier(world)
+        return 0
+    sc, terrs = workload(0)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(sc, terrs, budget_s=max(5.0, 60.0 / max(args.steps + args.warmup, 1)))
+        if i >= args.warmup:
+            vals.append(r)
+    v = sum(x["cell_steps"] for x in vals) / sum(x["wall_s"] for x in vals)
+    line = {"metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(x["wall_s"] for x in vals) / len(vals), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded), reference CPU path via oracle/ restatement",
+            "config": {"workload": "config2 rolling hills 120x96 @5 m, 64 designs x 4 primitives, 3600 s storm (bounded sample)",
+                       "impl_note": "reference Rust workspace not buildable here (no cargo/rustc); its f32 fused kernel is timed through the C++ restatement"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": vals[0]["cores"], "kind": "port", "sample": vals[0]["sample"]},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    barrier(world)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--designs", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--duration", type=float, default=None,
+                    help="simulate only the first DURATION s of the storm (profiling case; not a bench line)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank, world, local = dist_setup(args.gpus)
+    import torch
+    torch.cuda.set_device(local)
+    from itr_gpu import GpuSolver
+    sc, terrs = workload(rank, args.designs)
+    if args.duration is not None:
+        sc.params.duration_s = float(args.duration)
+    g = GpuSolver(local)
+    N = sc.base.nx * sc.base.ny
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # warm-up through the public call (also autotunes the launch shape)
+    for _ in range(max(args.warmup, 3)):
+        runs = g.run_batch(sc.params, terrs, sc.monitors, want_depth=False)
+    steps_per_design = [r.steps for r in runs]
+    cell_steps = float(sum(steps_per_design)) * N
+
+    # ---- value: kernel over resident inputs ----
+    barrier(world)
+    torch.cuda.synchronize()
+    kern_ms = []
+    launches = 0
+    with ClockSampler(local) as clk:
+        t_wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()                       # L2 flush (256 MB > 126 MB L2) between iterations
+            torch.cuda.synchronize()
+            g.rerun_resident()
+            tm = g.last_timing()
+            kern_ms.append(tm["kernel_ms"])
+            launches += tm["launches"]
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall0
+    barrier(world)
+    k_total_ms = max_over_ranks(sum(kern_ms), world)
+    total_cs = sum_over_ranks(cell_steps * args.steps, world)
+    value = total_cs / (k_total_ms / 1e3)
+    designs_per_s = sum_over_ranks(len(terrs) * args.steps, world) / (k_total_ms / 1e3)
+
+    # ---- e2e: the public C ABI call from host buffers ----
+    barrier(world)
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        runs = g.run_batch(sc.params, terrs, sc.monitors, want_depth=False)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    barrier(world)
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+    e2e_value = total_cs / (e2e_total / 1e3)
+    nx, ny = sc.base.nx, sc.base.ny
+    h2d = len(terrs) * (ny * (nx + 1) + (ny + 1) * nx + nx * ny) * 4 + 2 * N * 4 + 2 * (nx + ny) + len(terrs) * 16 \
+        + len(sc.monitors.cells) * 4
+    from itr_gpu.solver import GpuRun  # noqa: F401
+    d2h = len(terrs) * (len(sc.monitors.cells) * 4 + 96)
+
+    if rank == 0:
+        hbm, src = peaks()
+        per_launch_bytes = cell_steps * BYTES_PER_CELL_STEP
+        avg_ms = sum(kern_ms) / len(kern_ms)
+        achieved = per_launch_bytes / (avg_ms / 1e3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "k_batched_config2_traffic.json")
+        if os.path.exists(tp):
+            try:
+                with open(tp) as f:
+                    tj = json.load(f)
+                traffic = float(tj["dram_bytes_per_launch"])
+            except Exception:
+                traffic = None
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline(sc, terrs)
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": k_total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes and designs)",
+            "config": {"workload": "config2: rolling hills 120x96 @5 m, 60 min storm (100 mm/h peak at 20 min), "
+                                   f"{len(terrs)} designs x 4 primitives per GPU, run to completion",
+                       "designs_per_gpu": len(terrs), "cells": N, "steps_per_design_mean": sum(steps_per_design) / len(steps_per_design),
+                       "parallelism": f"designs sharded over {world} GPU(s), 1 design per thread-block cluster",
+                       "l2": "flushed between timed iterations (256 MB write)"},
+            "designs_per_s": designs_per_s,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "peak_source": src,
+                         "model": f"{BYTES_PER_CELL_STEP} B/cell-step x {cell_steps:.4g} cell-steps per launch"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "wall_s_timed": t_wall,
+        }
+        print(json.dumps(line))
+    g.close()
+    if world > 1:
+        import torch.distributed as dist
+        barrier(world)
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
