@@ -6,13 +6,16 @@
 // whole simulated storm and never leaves the SM between steps.
 //
 // Layout on chip. The design's rows are split into bands, one per CTA of the cluster; a band
-// lives in shared memory as structure-of-arrays (h, qx, qy, u, v, c, peak), 28 B/cell, so the
-// state never goes back to HBM until the run ends. Inside a CTA the band is cut into S strips;
-// each strip is swept row by row by W warps (one lane per column, W = ceil((nx+1)/32)), the
-// in-place row sweep of the reference's fused kernel (crates/itr-hydro/src/kernel.rs:637-697):
+// lives in shared memory, 28 B/cell: float4 (h, qx, qy, u), float2 (v, c) and the running
+// peak depth, so the state never goes back to HBM until the run ends. Inside a CTA the band
+// is cut into S strips; each strip is swept row by row by W warps, every lane holding two
+// columns, c and c + 32W (W = ceil((nx+1)/64)), whose faces and cell updates run as paired
+// FP32 instructions (itr_device.cuh, face2 / update_cell2). It is the in-place row sweep of
+// the reference's fused kernel (crates/itr-hydro/src/kernel.rs:637-697):
 //   * the north y-face of a row is carried in registers from the row above,
-//   * the west x-face of the next row is computed one phase early; the east face is the
-//     west face of lane+1 (shuffle; lane 31 reads lane 0 of the next warp via shared memory),
+//   * the west x-face of the next row is computed one row early; the east face is the
+//     west face of lane+1 (shuffle; lane 31 reads lane 0 of the next warp, or the second
+//     column of warp 0, through shared memory),
 //   * velocities (u, v) and celerity c are stored with the state when a cell is updated, so
 //     each is computed once per cell-step (c is the sources' sqrt(g*h)),
 //   * the y-face between two strips (and between two CTAs) is computed at the start of the
@@ -24,9 +27,11 @@
 // time integrator (dt rule, sync clipping, exact rain integral, solver.rs:449-489) runs in
 // every thread redundantly on identical inputs, so no broadcast is needed.
 //
-// Ledgers are f64 per-thread accumulators reduced in a fixed order at sync points; the guard
-// test (objective.rs:130-145) and the incumbent lower bound (objective.rs:146-149) run on
-// the device at sync points, so an aborted design stops immediately.
+// Ledgers: per-step f32 warp partials of infiltration and positivity fix and the per-face
+// boundary mass fluxes go to shared memory; one warp folds them into f64 running totals in a
+// fixed order. At sync points the volume, the ledger row, the guard test (objective.rs:
+// 130-145) and the incumbent lower bound (objective.rs:146-149) are evaluated on the device,
+// so an aborted design stops at once.
 #pragma once
 #include <cooperative_groups.h>
 #include "itr_device.cuh"
@@ -61,32 +66,55 @@ struct BatchArgs {
   unsigned long long max_steps;
 };
 
-// Shared-memory carve-up of one CTA (sizes in floats unless noted).
-struct Smem {
-  float *H, *QX, *QY, *U, *V, *Cc, *PK;        // nr*nx each
-  float *BM, *BNL, *BNR, *BT;                 // (S+1)*nx strip-boundary y-faces
-  float* XB;                                  // [2][S][W][4] lane-0 x-face exchange
-  unsigned* slot;                             // [2] smax bits, [2] bad, [2] pad
-  double* red;                                // [NW][8] sync reductions
-  unsigned long long* mbar;                   // CTA split barrier
-  int ncell, nbface, nxb;                     // array lengths (bounds checks)
-};
-
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-__host__ __device__ inline size_t batched_smem_bytes(int nr, int nx, int S, int W, int nwarps) {
-  size_t b = 0;
-  b += (size_t)7 * nr * nx * 4;
-  b += (size_t)4 * (S + 1) * nx * 4;
-  b += (size_t)2 * S * W * 4 * 4;
-  b = align_up(b, 16);
-  b += 8 * 4;                       // slots
-  b = align_up(b, 16);
-  b += (size_t)nwarps * 8 * 8;      // reductions
-  b = align_up(b, 16);
-  b += 16;                          // mbarrier
-  return b;
+ITR_DEV unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Shared-memory plan of one CTA. Every CTA of a cluster uses the plan of the largest band,
+// so an offset names the same array in every CTA (DSMEM maps local pointers to peers).
+struct SmemPlan {
+  size_t s4, s2, pk, bf, xb, bx, by, wsum, led, slot, red, mbar, pf, total;
+};
+
+// Values staged per thread and row by the prefetch ring: south y-face jump, next row's
+// x-face jump, wet, g n^2 (+ the second jumps in crest mode).
+__host__ __device__ inline int prefetch_k(int crest) { return crest ? 6 : 4; }
+
+__host__ __device__ inline SmemPlan smem_plan(int nr_max, int nx, int S, int W, int nwarps, int crest = 0) {
+  SmemPlan p;
+  size_t n = (size_t)nr_max * nx, o = 0;
+  p.s4 = o;   o += n * 16;                         // float4 h, qx, qy, u
+  p.s2 = o;   o += n * 8;                          // float2 v, c
+  p.pk = o;   o += n * 4;                          // peak depth
+  o = align_up(o, 16);
+  p.bf = o;   o += (size_t)(S + 1) * nx * 16;      // float4 strip-top y-faces
+  p.xb = o;   o += (size_t)2 * S * W * 2 * 16;     // float4 lane-0 x-face exchange [2][S][W][2]
+  p.bx = o;   o += (size_t)2 * 2 * nr_max * 4;     // west/east boundary mass flux [2][2][nr]
+  p.by = o;   o += (size_t)2 * 2 * nx * 4;         // top/bottom boundary mass flux [2][2][nx]
+  o = align_up(o, 16);
+  p.wsum = o; o += (size_t)2 * nwarps * 2 * 4;     // per-warp f32 step sums [2][nwarps][2]
+  o = align_up(o, 16);
+  p.led = o;  o += 8 * 8;                          // f64 running totals: infil, fix, in, out
+  p.slot = o; o += 8 * 4;                          // smax bits [2], bad [2]
+  o = align_up(o, 16);
+  p.red = o;  o += (size_t)nwarps * 8 * 8;         // f64 reductions at sync points
+  p.mbar = o; o += 16;
+  o = align_up(o, 16);
+  p.pf = o;   o += (size_t)2 * S * prefetch_k(crest) * 64 * W * 4;   // [2 slot][S][K][64W] floats
+  p.total = align_up(o, 16);
+  return p;
 }
+
+__host__ __device__ inline size_t batched_smem_bytes(int nr_max, int nx, int S, int W, int nwarps, int crest = 0) {
+  return smem_plan(nr_max, nx, S, W, nwarps, crest).total;
+}
+
+// 4-byte asynchronous global->shared copy (cp.async, cached in L1), commit and wait.
+ITR_DEV void cp_async4(float* smem_dst, const float* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+ITR_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> ITR_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 ITR_DEV void named_bar(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
@@ -94,8 +122,6 @@ ITR_DEV void named_bar(int id, int nthreads) {
 
 ITR_DEV void cluster_arrive() { asm volatile("barrier.cluster.arrive.release;" ::: "memory"); }
 ITR_DEV void cluster_wait() { asm volatile("barrier.cluster.wait.acquire;" ::: "memory"); }
-
-ITR_DEV unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
 ITR_DEV void mbar_init(unsigned long long* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
@@ -132,20 +158,36 @@ ITR_DEV long long chk(long long i, long long lim, int code) {
   return i;
 }
 #define CK(i, lim, code) ((int)chk((long long)(i), (long long)(lim), (code)))
-#define CKZ(i, lim, code) ((size_t)chk((long long)(i), (long long)(lim), (code)))
 #else
 #define CK(i, lim, code) (i)
-#define CKZ(i, lim, code) (i)
 #endif
 
 // A cell's stored state (old values during a step).
 struct Cell { float h, qx, qy, u, v, c; };
 
+struct Smem {
+  float4* S4;      // (h, qx, qy, u)
+  float2* S2;      // (v, c)
+  float* PK;
+  float4* BF;      // strip boundary y-faces (m, nl, nr, t)
+  float4* XB;
+  float* BX;       // [2 parity][2 side][nr_max]
+  float* BY;       // [2 parity][2 side][nx]
+  float* WS;       // [2 parity][nwarps][2]
+  double* LED;     // [4]
+  unsigned* slot;  // [2] smax bits, [2] bad
+  double* red;     // [nwarps][8]
+  unsigned long long* mbar;
+  float* PF;       // prefetch ring, [2 slot][S][K][64W]
+  int ncell, nbf, nxb;
+};
+
 ITR_DEV Cell load_cell(const Smem& s, int idx) {
   idx = CK(idx, s.ncell, 1);
+  const float4 a = s.S4[idx];
+  const float2 b = s.S2[idx];
   Cell c;
-  c.h = s.H[idx]; c.qx = s.QX[idx]; c.qy = s.QY[idx];
-  c.u = s.U[idx]; c.v = s.V[idx]; c.c = s.Cc[idx];
+  c.h = a.x; c.qx = a.y; c.qy = a.z; c.u = a.w; c.v = b.x; c.c = b.y;
   return c;
 }
 
@@ -171,32 +213,42 @@ ITR_DEV FaceF shfl_down_face(FaceF f) {
   o.t = __shfl_down_sync(0xffffffffu, f.t, 1);
   return o;
 }
+ITR_DEV float4 f4(const FaceF& f) { return make_float4(f.m, f.nl, f.nr, f.t); }
+ITR_DEV FaceF ff(const float4& v) { FaceF f; f.m = v.x; f.nl = v.y; f.nr = v.z; f.t = v.w; return f; }
+
+// Per-thread views of the inputs at this thread's column: row r of x-face jumps is
+// dzx[r * (nx + 1)], y-face f is dzy[f * nx], cell (r, col) of wet/gn2 is wet[r * nx].
+struct Col {
+  const float* dzx;
+  const float* dzy;
+  const float* dzx2;
+  const float* dzy2;
+  const float* wet;
+  const float* gn2;
+  long long off_x, off_y, lim_x, lim_y;   // bounds (checked build)
+};
 
 template <bool CREST>
-ITR_DEV FaceF xface(const Cell& l, const Cell& r, const BatchArgs& A, int d, int row, int f, const StepK& k) {
-  size_t o = (size_t)d * A.ny * (A.nx + 1) + (size_t)row * (A.nx + 1) + f;
-  o = CKZ(o, (long long)A.n_designs * A.ny * (A.nx + 1), 2);
-  float d0 = __ldg(A.dzx + o);
-  float d1 = CREST ? __ldg(A.dzx2 + o) : 0.0f;
+ITR_DEV FaceF xface(const Cell& l, const Cell& r, const Col& cp, int row, int nxp1, const StepK& k) {
+  const int o = CK(row * nxp1, cp.lim_x - cp.off_x, 2);
+  const float d0 = __ldg(cp.dzx + o);
+  const float d1 = CREST ? __ldg(cp.dzx2 + o) : 0.0f;
   return face<true, CREST>(l.h, l.u, l.v, l.c, r.h, r.u, r.v, r.c, d0, d1, k);
 }
 template <bool CREST>
-ITR_DEV FaceF yface(const Cell& t, const Cell& b, const BatchArgs& A, int d, int f, int col, const StepK& k) {
-  size_t o = (size_t)d * (A.ny + 1) * A.nx + (size_t)f * A.nx + col;
-  o = CKZ(o, (long long)A.n_designs * (A.ny + 1) * A.nx, 3);
-  float d0 = __ldg(A.dzy + o);
-  float d1 = CREST ? __ldg(A.dzy2 + o) : 0.0f;
+ITR_DEV FaceF yface(const Cell& t, const Cell& b, const Col& cp, int f, int nx, const StepK& k) {
+  const int o = CK(f * nx, cp.lim_y - cp.off_y, 3);
+  const float d0 = __ldg(cp.dzy + o);
+  const float d1 = CREST ? __ldg(cp.dzy2 + o) : 0.0f;
   return face<false, CREST>(t.h, t.u, t.v, t.c, b.h, b.u, b.v, b.c, d0, d1, k);
 }
 
-ITR_DEV void store_face(float* M, float* NL, float* NR, float* Tt, int idx, const FaceF& f) {
-  M[idx] = f.m; NL[idx] = f.nl; NR[idx] = f.nr; Tt[idx] = f.t;
-}
-ITR_DEV FaceF load_face(const float* M, const float* NL, const float* NR, const float* Tt, int idx) {
-  FaceF f; f.m = M[idx]; f.nl = NL[idx]; f.nr = NR[idx]; f.t = Tt[idx]; return f;
-}
-
 ITR_DEV double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+ITR_DEV float warp_sum_f(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
@@ -220,7 +272,7 @@ struct GroupSync {
     else { if (!mbar_wait(mbar, phase & 1u)) timed_out = true; }
   }
   ITR_DEV void b1_done() { phase += 1; }
-  ITR_DEV void b2() {
+  ITR_DEV void full() {
     if (CLUSTERED) { cluster_arrive(); cluster_wait(); } else __syncthreads();
   }
 };
@@ -228,6 +280,42 @@ struct GroupSync {
 // Map a pointer into shared memory to the same offset in CTA `rank` of the cluster.
 template <class T> ITR_DEV T* remote(T* p, int rank) {
   return cg::this_cluster().map_shared_rank(p, (unsigned)rank);
+}
+
+// Two cells of a lane: column c (component x) and column c + 32W (component y).
+struct Cell2 { float2 h, qx, qy, u, v, c; };
+
+ITR_DEV Cell2 cell2_of(const Cell& a, const Cell& b) {
+  Cell2 r;
+  r.h = make_float2(a.h, b.h); r.qx = make_float2(a.qx, b.qx); r.qy = make_float2(a.qy, b.qy);
+  r.u = make_float2(a.u, b.u); r.v = make_float2(a.v, b.v); r.c = make_float2(a.c, b.c);
+  return r;
+}
+ITR_DEV Cell cx(const Cell2& a) { Cell c; c.h = a.h.x; c.qx = a.qx.x; c.qy = a.qy.x; c.u = a.u.x; c.v = a.v.x; c.c = a.c.x; return c; }
+ITR_DEV Cell cy(const Cell2& a) { Cell c; c.h = a.h.y; c.qx = a.qx.y; c.qy = a.qy.y; c.u = a.u.y; c.v = a.v.y; c.c = a.c.y; return c; }
+ITR_DEV FaceF fx_(const Face2& f) { FaceF r; r.m = f.m.x; r.nl = f.nl.x; r.nr = f.nr.x; r.t = f.t.x; return r; }
+ITR_DEV FaceF fy_(const Face2& f) { FaceF r; r.m = f.m.y; r.nl = f.nl.y; r.nr = f.nr.y; r.t = f.t.y; return r; }
+ITR_DEV Face2 face2_of(const FaceF& a, const FaceF& b) {
+  Face2 f;
+  f.m = make_float2(a.m, b.m); f.nl = make_float2(a.nl, b.nl); f.nr = make_float2(a.nr, b.nr); f.t = make_float2(a.t, b.t);
+  return f;
+}
+ITR_DEV Cell2 shfl_up_cell2(const Cell2& c) {
+  Cell2 o;
+  o.h = make_float2(__shfl_up_sync(0xffffffffu, c.h.x, 1), __shfl_up_sync(0xffffffffu, c.h.y, 1));
+  o.qx = f2(0.0f); o.qy = f2(0.0f);
+  o.u = make_float2(__shfl_up_sync(0xffffffffu, c.u.x, 1), __shfl_up_sync(0xffffffffu, c.u.y, 1));
+  o.v = make_float2(__shfl_up_sync(0xffffffffu, c.v.x, 1), __shfl_up_sync(0xffffffffu, c.v.y, 1));
+  o.c = make_float2(__shfl_up_sync(0xffffffffu, c.c.x, 1), __shfl_up_sync(0xffffffffu, c.c.y, 1));
+  return o;
+}
+ITR_DEV Face2 shfl_down_face2(const Face2& f) {
+  Face2 o;
+  o.m = make_float2(__shfl_down_sync(0xffffffffu, f.m.x, 1), __shfl_down_sync(0xffffffffu, f.m.y, 1));
+  o.nl = make_float2(__shfl_down_sync(0xffffffffu, f.nl.x, 1), __shfl_down_sync(0xffffffffu, f.nl.y, 1));
+  o.nr = make_float2(__shfl_down_sync(0xffffffffu, f.nr.x, 1), __shfl_down_sync(0xffffffffu, f.nr.y, 1));
+  o.t = make_float2(__shfl_down_sync(0xffffffffu, f.t.x, 1), __shfl_down_sync(0xffffffffu, f.t.y, 1));
+  return o;
 }
 
 template <bool CREST, bool CLUSTERED, int MAXT>
@@ -240,73 +328,116 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   const int nx = A.nx, ny = A.ny;
   const int ra = (int)((long long)q * ny / C), rb = (int)((long long)(q + 1) * ny / C);
   const int nr = rb - ra;
+  const int nr_max = (ny + C - 1) / C;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
-  const int W = A.W, S = A.S;
+  const int W = A.W, S = A.S;        // W warps per strip row, 64W columns per row
   const int s = wid / W, wis = wid % W;
-  const int col = wis * 32 + lane;
+  const int col0 = wis * 32 + lane, col1 = col0 + 32 * W;
   const bool in_strip = s < S;
-  const bool cell_lane = in_strip && col < nx;
-  const bool face_lane = in_strip && col <= nx;
+  const bool cell0 = in_strip && col0 < nx, cell1 = in_strip && col1 < nx;
+  const bool face0 = in_strip && col0 <= nx, face1 = in_strip && col1 <= nx;
+  const bool any_face = face0 || face1;
   // strip rows (global row indices)
   const int r0 = in_strip ? ra + (int)((long long)s * nr / S) : rb;
   const int r1 = in_strip ? ra + (int)((long long)(s + 1) * nr / S) : rb;
   const int L = r1 - r0;
 
-  // Every CTA of a cluster carves shared memory for the largest band, so an offset means
-  // the same array in every CTA (DSMEM reads map a local pointer to a peer CTA).
-  const int nr_max = (ny + C - 1) / C;
   Smem sm;
   {
-    float* f = reinterpret_cast<float*>(smem_raw);
-    size_t n = (size_t)nr_max * nx;
-    sm.H = f; sm.QX = f + n; sm.QY = f + 2 * n; sm.U = f + 3 * n; sm.V = f + 4 * n; sm.Cc = f + 5 * n; sm.PK = f + 6 * n;
-    float* b = f + 7 * n;
-    size_t nb = (size_t)(S + 1) * nx;
-    sm.BM = b; sm.BNL = b + nb; sm.BNR = b + 2 * nb; sm.BT = b + 3 * nb;
-    sm.XB = b + 4 * nb;
-    size_t off = align_up((size_t)((unsigned char*)(sm.XB + 2 * S * W * 4) - smem_raw), 16);
-    sm.slot = reinterpret_cast<unsigned*>(smem_raw + off);
-    off = align_up(off + 8 * 4, 16);
-    sm.red = reinterpret_cast<double*>(smem_raw + off);
-    off = align_up(off + (size_t)nwarps * 8 * 8, 16);
-    sm.mbar = reinterpret_cast<unsigned long long*>(smem_raw + off);
-    sm.ncell = (int)n; sm.nbface = (int)nb; sm.nxb = 2 * S * W * 4;
+    const SmemPlan pl = smem_plan(nr_max, nx, S, W, nwarps, CREST ? 1 : 0);
+    sm.S4 = reinterpret_cast<float4*>(smem_raw + pl.s4);
+    sm.S2 = reinterpret_cast<float2*>(smem_raw + pl.s2);
+    sm.PK = reinterpret_cast<float*>(smem_raw + pl.pk);
+    sm.BF = reinterpret_cast<float4*>(smem_raw + pl.bf);
+    sm.XB = reinterpret_cast<float4*>(smem_raw + pl.xb);
+    sm.BX = reinterpret_cast<float*>(smem_raw + pl.bx);
+    sm.BY = reinterpret_cast<float*>(smem_raw + pl.by);
+    sm.WS = reinterpret_cast<float*>(smem_raw + pl.wsum);
+    sm.LED = reinterpret_cast<double*>(smem_raw + pl.led);
+    sm.slot = reinterpret_cast<unsigned*>(smem_raw + pl.slot);
+    sm.red = reinterpret_cast<double*>(smem_raw + pl.red);
+    sm.mbar = reinterpret_cast<unsigned long long*>(smem_raw + pl.mbar);
+    sm.PF = reinterpret_cast<float*>(smem_raw + pl.pf);
+    sm.ncell = nr_max * nx; sm.nbf = (S + 1) * nx; sm.nxb = 2 * S * W * 2;
   }
   const RunParams& P = A.P;
-  const size_t cell0 = (size_t)d * nx * ny;
+  const size_t cell0_off = (size_t)d * nx * ny;
+  const int nxp1 = nx + 1;
+  // Per-thread input offsets of both columns (idle lanes point at a valid column, never
+  // read): x-face jumps of (row r, col) at dzx[ox + r (nx+1)], y-face f at dzy[oy + f nx],
+  // wet / g n^2 of (r, col) at wet[oc + r nx]. Offsets, not pointers, to save registers.
+  const int cc0 = col0 <= nx ? col0 : nx, cc1 = col1 <= nx ? col1 : nx;
+  const int oc0 = cc0 < nx ? cc0 : nx - 1, oc1 = cc1 < nx ? cc1 : nx - 1;
+  const size_t ox0 = (size_t)d * ny * nxp1 + cc0, ox1 = (size_t)d * ny * nxp1 + cc1;
+  const size_t oy0 = (size_t)d * (ny + 1) * nx + oc0, oy1 = (size_t)d * (ny + 1) * nx + oc1;
+  const int bc_w = 2 * nx, bc_e = 2 * nx + ny, bc_n = 0, bc_s = nx, nbc = 2 * nx + 2 * ny;
+
+  // Prefetch ring: row r's operands for this thread's two columns are copied one row ahead.
+  constexpr int K = CREST ? 6 : 4;
+  const int vlanes = 64 * W;
+  float* const pf_base = sm.PF + (size_t)(s < S ? s : 0) * K * vlanes + col0;   // slot 0, column col0
+  const size_t pf_slot = (size_t)S * K * vlanes;
+  auto prefetch_row = [&](int r, int slot) {
+    // dzy[r+1] (south face), dzx[r+1] (next row's west face; clamped in range for the last
+    // row, where it is not used), wet and g n^2 of row r, for columns col0 and col1
+    float* dst = pf_base + slot * pf_slot;
+    const int rn = r + 1 < ny ? r + 1 : ny - 1;
+    const size_t fy = (size_t)(r + 1) * nx, fx = (size_t)rn * nxp1, fc = (size_t)r * nx;
+    if (face0) {
+      cp_async4(dst + 0 * vlanes, A.dzy + oy0 + fy);
+      cp_async4(dst + 1 * vlanes, A.dzx + ox0 + fx);
+      cp_async4(dst + 2 * vlanes, A.wet + oc0 + fc);
+      cp_async4(dst + 3 * vlanes, A.gn2 + oc0 + fc);
+      if (CREST) {
+        cp_async4(dst + 4 * vlanes, A.dzy2 + oy0 + fy);
+        cp_async4(dst + 5 * vlanes, A.dzx2 + ox0 + fx);
+      }
+    }
+    if (face1) {
+      float* d1 = dst + 32 * W;
+      cp_async4(d1 + 0 * vlanes, A.dzy + oy1 + fy);
+      cp_async4(d1 + 1 * vlanes, A.dzx + ox1 + fx);
+      cp_async4(d1 + 2 * vlanes, A.wet + oc1 + fc);
+      cp_async4(d1 + 3 * vlanes, A.gn2 + oc1 + fc);
+      if (CREST) {
+        cp_async4(d1 + 4 * vlanes, A.dzy2 + oy1 + fy);
+        cp_async4(d1 + 5 * vlanes, A.dzx2 + ox1 + fx);
+      }
+    }
+  };
 
   // ---------------------------------------------------------------- initial state ----
   double s0_l = 0.0, v0_l = 0.0;
   for (int idx = tid; idx < nr * nx; idx += blockDim.x) {
-    int r = ra + idx / nx, c = idx % nx;
-    float h = A.h0[CKZ(cell0 + (size_t)r * nx + c, (long long)A.n_designs * nx * ny, 12)];
-    sm.H[idx] = h; sm.QX[idx] = 0.0f; sm.QY[idx] = 0.0f;
+    const int r = ra + idx / nx, c = idx % nx;
+    const float h = A.h0[cell0_off + (size_t)r * nx + c];
     float u, v, cc;
-    cell_vel(h, 0.0f, 0.0f, (float)P.g, (float)(P.h_eps * P.h_eps), u, v, cc);
-    sm.U[idx] = u; sm.V[idx] = v; sm.Cc[idx] = cc; sm.PK[idx] = 0.0f;
-    double hd = (double)h;
+    cell_vel(h, 0.0f, 0.0f, P.g_f, P.heps2_f, u, v, cc);
+    sm.S4[idx] = make_float4(h, 0.0f, 0.0f, u);
+    sm.S2[idx] = make_float2(v, cc);
+    sm.PK[idx] = 0.0f;
+    const double hd = (double)h;
     v0_l += hd;
     if (hd > P.h_dry) {  // initial_smax (solver.rs:314-332) with q = 0
-      double cd = sqrt(P.g * hd);
-      double rr = (0.0 / hd + cd) / P.dx + (0.0 / hd + cd) / P.dy;
+      const double cd = sqrt(P.g * hd);
+      const double rr = (0.0 / hd + cd) / P.dx + (0.0 / hd + cd) / P.dy;
       s0_l = s0_l > rr ? s0_l : rr;
     }
   }
-  if (tid < 8) sm.slot[tid] = 0u;
+  if (tid < 8) { sm.slot[tid] = 0u; sm.LED[tid] = 0.0; }
   if (tid == 0) mbar_init(sm.mbar, blockDim.x);
   {
-    // reduce s0 (max) and v0 (sum, fixed order) across the cluster
     double sw = s0_l;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) { double t = __shfl_xor_sync(0xffffffffu, sw, o); sw = sw > t ? sw : t; }
-    double vw = warp_sum_d(v0_l);
+    const double vw = warp_sum_d(v0_l);
     if (lane == 0) { sm.red[wid * 8 + 0] = sw; sm.red[wid * 8 + 1] = vw; }
   }
   if (CLUSTERED) { cluster_arrive(); cluster_wait(); } else __syncthreads();
   double s0 = 0.0, v0 = 0.0;
   for (int qq = 0; qq < C; ++qq) {
     const double* rr = CLUSTERED ? remote(sm.red, qq) : sm.red;
-    for (int w = 0; w < nwarps; ++w) { double a = rr[w * 8 + 0]; s0 = s0 > a ? s0 : a; v0 += rr[w * 8 + 1]; }
+    for (int w = 0; w < nwarps; ++w) { const double a = rr[w * 8 + 0]; s0 = s0 > a ? s0 : a; v0 += rr[w * 8 + 1]; }
   }
   v0 *= P.area;
   if (CLUSTERED) { cluster_arrive(); cluster_wait(); } else __syncthreads();   // red reused below
@@ -317,168 +448,247 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   unsigned sync_index = 0;
   double dt_cfl = s0 > 0.0 ? dmin_num(P.cfl / s0, P.dt_max) : P.dt_max;
   double acc_rain = 0.0;
-  // per-thread f64 ledgers (cumulative)
-  double l_infil = 0.0, l_fix = 0.0, l_in = 0.0, l_out = 0.0;
   int status = 0;
   unsigned breach_cell = 0, breach_sync = 0;
   double violation = 0.0, lower_bound = 0.0, volume = v0, rel_res = 0.0;
   int n_rows = 0;
   GroupSync<CLUSTERED> gs;
   gs.mbar = sm.mbar; gs.phase = 0; gs.timed_out = false;
+  const float heps2 = P.heps2_f;
+  RainCursor rcur;
+  rcur.seg = 0; rcur.brk = 0;
+  const int lr0 = r0 - ra;
+  const bool top_dom = (r0 == 0);
+  const int xb_next = wis + 1 < W ? wis + 1 : 0;          // warp whose lane 0 holds col0 + 1 of lane 31
+  const int xb_next_comp = wis + 1 < W ? 0 : 1;
 
-  const float heps2 = (float)(P.h_eps * P.h_eps);
+  // Loads the two cells of row lr (local) for this lane: interior cells, or the east ghost
+  // for a lane whose column is nx (built from cell nx-1 and the east code of global row r).
+  auto load_pair = [&](int lr, int r) -> Cell2 {
+    Cell a{}, b{};
+    if (cell0) a = load_cell(sm, lr * nx + col0);
+    else if (face0) a = ghost_x(load_cell(sm, lr * nx + nx - 1), A.bc[CK(bc_e + r, nbc, 13)]);
+    if (cell1) b = load_cell(sm, lr * nx + col1);
+    else if (face1) b = ghost_x(load_cell(sm, lr * nx + nx - 1), A.bc[CK(bc_e + r, nbc, 13)]);
+    return cell2_of(a, b);
+  };
+  // West neighbours of the lane's two cells in row lr: lane-1 by shuffle; lane 0 reads the
+  // cell at column-1 from shared memory (another warp's column), or the west ghost at col 0.
+  auto left_pair = [&](const Cell2& cur, int lr, int r) -> Cell2 {
+    Cell2 left = shfl_up_cell2(cur);
+    if (lane == 0) {
+      Cell a = cx(left), b = cy(left);
+      if (face0) a = col0 == 0 ? ghost_x(cx(cur), A.bc[CK(bc_w + r, nbc, 14)]) : load_cell(sm, lr * nx + col0 - 1);
+      if (face1) b = load_cell(sm, lr * nx + col1 - 1);
+      left = cell2_of(a, b);
+    }
+    return left;
+  };
 
   while (t < P.duration && sync_index < P.n_sync) {
     if (step >= A.max_steps) { status = 4; break; }
-    const StepPlan pl = plan_step(P, t, sync_index, dt_cfl);
-    const StepK k = make_consts(P, pl.dt, pl.rain);
-    const double dt_dy = pl.dt * P.dy, dt_dx = pl.dt * P.dx;
-    float smax_l = 0.0f;
+    const StepPlan pl = plan_step_c(P, t, sync_index, dt_cfl, rcur);
+    const StepK k = step_consts(P, pl.dt, pl.rain);
+    const int sp = (int)(step & 1ull);
+    float smax_l = 0.0f, infil_l = 0.0f, fix_l = 0.0f;
     bool bad_l = false;
-    double vol_l = 0.0;
     int par = 0;
 
-    // ---- strip pre-phase: first row, its west face, the strip's top y-face ----
+    // ---- strip pre-phase: first row, its west faces, the strip's top y-faces ----
     // Control flow is uniform per warp here (L is per strip); lane predicates only guard
     // loads and arithmetic, never the shuffles.
-    Cell cur{};
-    FaceF fW{}, fN{};
+    Cell2 cur{};
+    Face2 fW{}, fN{};
+    if (L > 0) prefetch_row(r0, 0);
+    cp_async_commit();
     if (L > 0) {
-      const int lr = r0 - ra;
-      if (cell_lane) cur = load_cell(sm, lr * nx + col);
-      else if (face_lane) cur = ghost_x(load_cell(sm, lr * nx + nx - 1), A.bc[CK(2 * nx + ny + r0, 2 * nx + 2 * ny, 13)]);  // east ghost lane
-      Cell left = shfl_up_cell(cur);
-      if (lane == 0 && face_lane) {
-        if (col == 0) left = ghost_x(cur, A.bc[CK(2 * nx + r0, 2 * nx + 2 * ny, 14)]);
-        else left = load_cell(sm, lr * nx + col - 1);
+      cur = load_pair(lr0, r0);
+      const Cell2 left = left_pair(cur, lr0, r0);
+      const size_t fx = (size_t)r0 * nxp1, fy = (size_t)r0 * nx;
+      const float2 dx0 = make_float2(__ldg(A.dzx + ox0 + fx), __ldg(A.dzx + ox1 + fx));
+      const float2 dx1 = CREST ? make_float2(__ldg(A.dzx2 + ox0 + fx), __ldg(A.dzx2 + ox1 + fx)) : f2(0.0f);
+      fW = face2<true, CREST>(left.h, left.u, left.v, left.c, cur.h, cur.u, cur.v, cur.c, dx0, dx1, k);
+      if (lane == 0) {
+        sm.XB[CK(((par * S + s) * W + wis) * 2 + 0, sm.nxb, 7)] = f4(fx_(fW));
+        sm.XB[CK(((par * S + s) * W + wis) * 2 + 1, sm.nxb, 7)] = f4(fy_(fW));
       }
-      if (face_lane) fW = xface<CREST>(left, cur, A, d, r0, col, k);
-      if (lane == 0 && face_lane && wis > 0) {
-        float* xb = sm.XB + CK(((par * S + s) * W + wis) * 4, sm.nxb - 3, 7);
-        xb[0] = fW.m; xb[1] = fW.nl; xb[2] = fW.nr; xb[3] = fW.t;
+      // the cells above the strip's first row: ghost, same CTA, or the CTA above
+      Cell a0{}, a1{};
+      if (top_dom) {
+        if (cell0) a0 = ghost_y(cx(cur), A.bc[CK(bc_n + col0, nbc, 15)]);
+        if (cell1) a1 = ghost_y(cy(cur), A.bc[CK(bc_n + col1, nbc, 15)]);
+      } else if (r0 - 1 >= ra) {
+        if (cell0) a0 = load_cell(sm, (lr0 - 1) * nx + col0);
+        if (cell1) a1 = load_cell(sm, (lr0 - 1) * nx + col1);
+      } else {
+        // last row of the CTA above (old state; that CTA updates it only after B1)
+        const int rap = (int)((long long)(q - 1) * ny / C);
+        Smem rs = sm;
+        rs.S4 = remote(sm.S4, q - 1);
+        rs.S2 = remote(sm.S2, q - 1);
+        if (cell0) a0 = load_cell(rs, (ra - 1 - rap) * nx + col0);
+        if (cell1) a1 = load_cell(rs, (ra - 1 - rap) * nx + col1);
       }
-      if (cell_lane) {
-        Cell above;
-        if (r0 == 0) above = ghost_y(cur, A.bc[CK(col, 2 * nx + 2 * ny, 15)]);
-        else if (r0 - 1 >= ra) above = load_cell(sm, (r0 - 1 - ra) * nx + col);
-        else {
-          // last row of the CTA above (old state; that CTA updates it only after B1)
-          const int rap = (int)((long long)(q - 1) * ny / C);
-          Smem rs = sm;
-          rs.H = remote(sm.H, q - 1); rs.QX = remote(sm.QX, q - 1); rs.QY = remote(sm.QY, q - 1);
-          rs.U = remote(sm.U, q - 1); rs.V = remote(sm.V, q - 1); rs.Cc = remote(sm.Cc, q - 1);
-          above = load_cell(rs, CK((ra - 1 - rap) * nx + col, (rb - ra > 0 ? nr_max : 0) * nx, 19));
-        }
-        fN = yface<CREST>(above, cur, A, d, r0, col, k);
-        store_face(sm.BM, sm.BNL, sm.BNR, sm.BT, CK(s * nx + col, sm.nbface, 4), fN);
-        if (r0 == 0) {  // y_boundary top (kernel.rs:452-472), per face
-          double v = (double)fN.m * dt_dx;
-          if (v > 0.0) l_in += v; else l_out -= v;
-        }
+      const Cell2 above = cell2_of(a0, a1);
+      const float2 dy0 = make_float2(__ldg(A.dzy + oy0 + fy), __ldg(A.dzy + oy1 + fy));
+      const float2 dy1 = CREST ? make_float2(__ldg(A.dzy2 + oy0 + fy), __ldg(A.dzy2 + oy1 + fy)) : f2(0.0f);
+      fN = face2<false, CREST>(above.h, above.u, above.v, above.c, cur.h, cur.u, cur.v, cur.c, dy0, dy1, k);
+      if (cell0) sm.BF[CK(s * nx + col0, sm.nbf, 4)] = f4(fx_(fN));
+      if (cell1) sm.BF[CK(s * nx + col1, sm.nbf, 4)] = f4(fy_(fN));
+      if (top_dom) {   // y_boundary top (kernel.rs:452-472)
+        if (cell0) sm.BY[(sp * 2 + 0) * nx + col0] = fN.m.x;
+        if (cell1) sm.BY[(sp * 2 + 0) * nx + col1] = fN.m.y;
       }
     }
     if (in_strip) { if (W > 1) named_bar(1 + s, 32 * W); else __syncwarp(); }
     gs.b1_arrive();
 
     // ---- row sweep ----
+#pragma unroll 1
     for (int p = 0; p < L; ++p) {
       const int r = r0 + p;
-      const int lr = r - ra;
+      const int lr = lr0 + p;
       const bool last = (p == L - 1);
       if (last) gs.b1_wait();
-      Cell nxt{};
-      FaceF fS{}, fWn{};
-      FaceF fE = shfl_down_face(fW);
-      if (lane == 31 && cell_lane) {
-        const float* xb = sm.XB + CK(((par * S + s) * W + wis + 1) * 4, sm.nxb - 3, 8);
-        fE.m = xb[0]; fE.nl = xb[1]; fE.nr = xb[2]; fE.t = xb[3];
+      if (!last) prefetch_row(r + 1, (p + 1) & 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+      const float* pfv = pf_base + (p & 1) * pf_slot;
+      const float* pfv1 = pfv + 32 * W;
+      const float2 d_s = make_float2(pfv[0 * vlanes], pfv1[0 * vlanes]);
+      const float2 d_xn = make_float2(pfv[1 * vlanes], pfv1[1 * vlanes]);
+      const float2 wet_r = make_float2(pfv[2 * vlanes], pfv1[2 * vlanes]);
+      const float2 gn2_r = make_float2(pfv[3 * vlanes], pfv1[3 * vlanes]);
+      const float2 d_s2 = CREST ? make_float2(pfv[4 * vlanes], pfv1[4 * vlanes]) : f2(0.0f);
+      const float2 d_xn2 = CREST ? make_float2(pfv[5 * vlanes], pfv1[5 * vlanes]) : f2(0.0f);
+      Cell2 nxt{};
+      Face2 fS{}, fWn{};
+      // east faces: west faces of lane+1; lane 31 reads the published face of the lane
+      // holding the next column
+      Face2 fE = shfl_down_face2(fW);
+      if (lane == 31) {
+        FaceF ex = fx_(fE), ey = fy_(fE);
+        if (cell0) ex = ff(sm.XB[CK(((par * S + s) * W + xb_next) * 2 + xb_next_comp, sm.nxb, 8)]);
+        if (cell1 && wis + 1 < W) ey = ff(sm.XB[CK(((par * S + s) * W + wis + 1) * 2 + 1, sm.nxb, 8)]);
+        fE = face2_of(ex, ey);
       }
       if (!last) {
-        const int lr1 = lr + 1;
-        if (cell_lane) nxt = load_cell(sm, lr1 * nx + col);
-        else if (face_lane) nxt = ghost_x(load_cell(sm, lr1 * nx + nx - 1), A.bc[CK(2 * nx + ny + r + 1, 2 * nx + 2 * ny, 16)]);
-        if (cell_lane) fS = yface<CREST>(cur, nxt, A, d, r + 1, col, k);
-        Cell left = shfl_up_cell(nxt);
-        if (lane == 0 && face_lane) {
-          if (col == 0) left = ghost_x(nxt, A.bc[CK(2 * nx + r + 1, 2 * nx + 2 * ny, 17)]);
-          else left = load_cell(sm, lr1 * nx + col - 1);
+        nxt = load_pair(lr + 1, r + 1);
+        fS = face2<false, CREST>(cur.h, cur.u, cur.v, cur.c, nxt.h, nxt.u, nxt.v, nxt.c, d_s, d_s2, k);
+        const Cell2 left = left_pair(nxt, lr + 1, r + 1);
+        fWn = face2<true, CREST>(left.h, left.u, left.v, left.c, nxt.h, nxt.u, nxt.v, nxt.c, d_xn, d_xn2, k);
+        if (lane == 0) {
+          sm.XB[CK((((par ^ 1) * S + s) * W + wis) * 2 + 0, sm.nxb, 9)] = f4(fx_(fWn));
+          sm.XB[CK((((par ^ 1) * S + s) * W + wis) * 2 + 1, sm.nxb, 9)] = f4(fy_(fWn));
         }
-        if (face_lane) fWn = xface<CREST>(left, nxt, A, d, r + 1, col, k);
-        if (lane == 0 && face_lane && wis > 0) {
-          float* xb = sm.XB + CK((((par ^ 1) * S + s) * W + wis) * 4, sm.nxb - 3, 9);
-          xb[0] = fWn.m; xb[1] = fWn.nl; xb[2] = fWn.nr; xb[3] = fWn.t;
-        }
-      } else if (cell_lane) {
-        if (s + 1 < S) fS = load_face(sm.BM, sm.BNL, sm.BNR, sm.BT, CK((s + 1) * nx + col, sm.nbface, 5));
-        else if (q + 1 < C) {
-          fS = load_face(remote(sm.BM, q + 1), remote(sm.BNL, q + 1), remote(sm.BNR, q + 1), remote(sm.BT, q + 1), CK(col, sm.nbface, 6));
+      } else {
+        // south faces of a strip's last row: the next strip's top faces (pre-phase), the
+        // next CTA's, or the domain's south edge
+        FaceF sx{}, sy{};
+        if (s + 1 < S) {
+          if (cell0) sx = ff(sm.BF[CK((s + 1) * nx + col0, sm.nbf, 5)]);
+          if (cell1) sy = ff(sm.BF[CK((s + 1) * nx + col1, sm.nbf, 5)]);
+          fS = face2_of(sx, sy);
+        } else if (q + 1 < C) {
+          const float4* rbf = remote(sm.BF, q + 1);
+          if (cell0) sx = ff(rbf[CK(col0, sm.nbf, 6)]);
+          if (cell1) sy = ff(rbf[CK(col1, sm.nbf, 6)]);
+          fS = face2_of(sx, sy);
         } else {
-          Cell below = ghost_y(cur, A.bc[CK(nx + col, 2 * nx + 2 * ny, 18)]);
-          fS = yface<CREST>(cur, below, A, d, ny, col, k);
-          double v = (double)fS.m * dt_dx;  // y_boundary bottom
-          if (v > 0.0) l_out += v; else l_in -= v;
+          Cell b0{}, b1{};
+          if (cell0) b0 = ghost_y(cx(cur), A.bc[CK(bc_s + col0, nbc, 18)]);
+          if (cell1) b1 = ghost_y(cy(cur), A.bc[CK(bc_s + col1, nbc, 18)]);
+          const Cell2 below = cell2_of(b0, b1);
+          fS = face2<false, CREST>(cur.h, cur.u, cur.v, cur.c, below.h, below.u, below.v, below.c, d_s, d_s2, k);
+          if (cell0) sm.BY[(sp * 2 + 1) * nx + col0] = fS.m.x;   // y_boundary bottom
+          if (cell1) sm.BY[(sp * 2 + 1) * nx + col1] = fS.m.y;
         }
       }
-      // x_boundary (kernel.rs:435-450), per face
-      if (in_strip && col == 0) { double v = (double)fW.m * dt_dy; if (v > 0.0) l_in += v; else l_out -= v; }
-      if (in_strip && col == nx) { double v = (double)fW.m * dt_dy; if (v > 0.0) l_out += v; else l_in -= v; }
-      if (cell_lane) {
-        const size_t gi = CKZ((size_t)r * nx + col, (long long)nx * ny, 11);
-        CellNew o = update_cell(cur.h, cur.qx, cur.qy, fW, fE, fN, fS, __ldg(A.wet + gi), __ldg(A.gn2 + gi), k);
-        float u, v;
-        {
-          float h2 = o.h * o.h;
-          float inv = 1.0f / (h2 + rmax(h2, heps2));
-          float tt = (o.h + o.h) * inv;
-          u = o.qx * tt; v = o.qy * tt;
+      // x_boundary (kernel.rs:435-450): mass flux of the west and east domain faces
+      if (in_strip && col0 == 0) sm.BX[(sp * 2 + 0) * nr_max + lr] = fW.m.x;
+      if (in_strip && col0 == nx) sm.BX[(sp * 2 + 1) * nr_max + lr] = fW.m.x;
+      if (in_strip && col1 == nx) sm.BX[(sp * 2 + 1) * nr_max + lr] = fW.m.y;
+      if (cell0 || cell1) {
+        const CellNew2 o = update_cell2(cur.h, cur.qx, cur.qy, fW, fE, fN, fS, wet_r, gn2_r, k);
+        const float2 h2 = mul2(o.h, o.h, k.nz);
+        const float2 inv = rcp2(add2(h2, max2(h2, f2(heps2))));
+        const float2 tt = mul2(add2(o.h, o.h), inv, k.nz);
+        const float2 uu = mul2(o.qx, tt, k.nz), vv = mul2(o.qy, tt, k.nz);
+        if (cell0) {
+          const int li = CK(lr * nx + col0, sm.ncell, 10);
+          sm.S4[li] = make_float4(o.h.x, o.qx.x, o.qy.x, uu.x);
+          sm.S2[li] = make_float2(vv.x, o.c.x);
+          const float pk = sm.PK[li];
+          if (o.h.x > pk) sm.PK[li] = o.h.x;
+          smax_l = rmax(smax_l, o.s.x);
+          bad_l = bad_l || o.bad.x;
+          infil_l += o.infil.x;
+          fix_l += o.fix.x;
         }
-        const int li = CK(lr * nx + col, nr * nx, 10);
-        sm.H[li] = o.h; sm.QX[li] = o.qx; sm.QY[li] = o.qy; sm.U[li] = u; sm.V[li] = v; sm.Cc[li] = o.c;
-        float pk = sm.PK[li];
-        if (o.h > pk) sm.PK[li] = o.h;
-        smax_l = rmax(smax_l, o.s);
-        bad_l = bad_l || o.bad;
-        l_infil += (double)o.infil;
-        l_fix += (double)o.fix;
-        if (pl.hits) vol_l += (double)o.h;
+        if (cell1) {
+          const int li = CK(lr * nx + col1, sm.ncell, 10);
+          sm.S4[li] = make_float4(o.h.y, o.qx.y, o.qy.y, uu.y);
+          sm.S2[li] = make_float2(vv.y, o.c.y);
+          const float pk = sm.PK[li];
+          if (o.h.y > pk) sm.PK[li] = o.h.y;
+          smax_l = rmax(smax_l, o.s.y);
+          bad_l = bad_l || o.bad.y;
+          infil_l += o.infil.y;
+          fix_l += o.fix.y;
+        }
       }
       cur = nxt; fN = fS; fW = fWn; par ^= 1;
       if (in_strip) { if (W > 1) named_bar(1 + s, 32 * W); else __syncwarp(); }
     }
     if (L == 0) gs.b1_wait();
     gs.b1_done();
-
-    // ---- end of step: CFL max, health, sync-point reductions ----
-    const int sp = (int)(step & 1ull);
+    (void)any_face;
+    // ---- end of step: CFL max, health, per-warp ledger partials ----
     {
-      float m = warp_max_f(smax_l);
-      unsigned b = __any_sync(0xffffffffu, bad_l) ? 1u : 0u;
+      const float m = warp_max_f(smax_l);
+      const unsigned b = __any_sync(0xffffffffu, bad_l) ? 1u : 0u;
+      const float wi = warp_sum_f(infil_l), wf = warp_sum_f(fix_l);
       if (lane == 0) {
         if (m > 0.0f) atomicMax(&sm.slot[sp], __float_as_uint(m));
         if (b) atomicOr(&sm.slot[2 + sp], 1u);
-      }
-      if (pl.hits) {
-        double a0 = warp_sum_d(vol_l), a1 = warp_sum_d(l_infil), a2 = warp_sum_d(l_fix);
-        double a3 = warp_sum_d(l_in), a4 = warp_sum_d(l_out);
-        if (lane == 0) {
-          double* rr = sm.red + wid * 8;
-          rr[0] = a0; rr[1] = a1; rr[2] = a2; rr[3] = a3; rr[4] = a4;
-        }
+        sm.WS[(sp * nwarps + wid) * 2 + 0] = wi;
+        sm.WS[(sp * nwarps + wid) * 2 + 1] = wf;
       }
     }
-    gs.b2();
+    gs.full();
     unsigned smax_bits = 0u, badv = 0u;
-    double tot[5] = {0, 0, 0, 0, 0};
     for (int qq = 0; qq < C; ++qq) {
       const unsigned* sl = CLUSTERED ? remote(sm.slot, qq) : sm.slot;
-      unsigned a = sl[sp];
+      const unsigned a = sl[sp];
       smax_bits = smax_bits > a ? smax_bits : a;
       badv |= sl[2 + sp];
-      if (pl.hits) {
-        const double* rr = CLUSTERED ? remote(sm.red, qq) : sm.red;
-        for (int w = 0; w < nwarps; ++w)
-          for (int j = 0; j < 5; ++j) tot[j] += rr[w * 8 + j];
+    }
+    if (wid == 0) {
+      // fold this CTA's step partials into its f64 running totals, in a fixed order
+      double di = 0.0, df = 0.0, din = 0.0, dout = 0.0;
+      for (int w = lane; w < nwarps; w += 32) {
+        di += (double)sm.WS[(sp * nwarps + w) * 2 + 0];
+        df += (double)sm.WS[(sp * nwarps + w) * 2 + 1];
       }
+      const double dt_dy = pl.dt * P.dy, dt_dx = pl.dt * P.dx;
+      for (int j = lane; j < nr; j += 32) {
+        const double vw = (double)sm.BX[(sp * 2 + 0) * nr_max + j] * dt_dy;   // west: inflow when m > 0
+        if (vw > 0.0) din += vw; else dout -= vw;
+        const double ve = (double)sm.BX[(sp * 2 + 1) * nr_max + j] * dt_dy;   // east: outflow when m > 0
+        if (ve > 0.0) dout += ve; else din -= ve;
+      }
+      if (q == 0)
+        for (int j = lane; j < nx; j += 32) {
+          const double v = (double)sm.BY[(sp * 2 + 0) * nx + j] * dt_dx;
+          if (v > 0.0) din += v; else dout -= v;
+        }
+      if (q == C - 1)
+        for (int j = lane; j < nx; j += 32) {
+          const double v = (double)sm.BY[(sp * 2 + 1) * nx + j] * dt_dx;
+          if (v > 0.0) dout += v; else din -= v;
+        }
+      di = warp_sum_d(di); df = warp_sum_d(df); din = warp_sum_d(din); dout = warp_sum_d(dout);
+      if (lane == 0) { sm.LED[0] += di; sm.LED[1] += df; sm.LED[2] += din; sm.LED[3] += dout; }
     }
     if (tid == 0) { sm.slot[sp ^ 1] = 0u; sm.slot[2 + (sp ^ 1)] = 0u; }
     const double smax = (double)__uint_as_float(smax_bits);
@@ -488,7 +698,20 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     if (badv) { status = 3; break; }
     dt_cfl = smax > 0.0 ? P.cfl / smax : P.dt_max;
     if (pl.hits) {
+      // ---- sync point: volume, ledger row, guard and incumbent tests ----
       sync_index += 1;
+      double vol_l = 0.0;
+      for (int idx = tid; idx < nr * nx; idx += blockDim.x) vol_l += (double)sm.S4[idx].x;
+      vol_l = warp_sum_d(vol_l);
+      if (lane == 0) sm.red[wid * 8 + 0] = vol_l;
+      gs.full();   // volume partials and ledger totals of every CTA visible
+      double tot[5] = {0, 0, 0, 0, 0};
+      for (int qq = 0; qq < C; ++qq) {
+        const double* rr = CLUSTERED ? remote(sm.red, qq) : sm.red;
+        const double* lg = CLUSTERED ? remote(sm.LED, qq) : sm.LED;
+        for (int w = 0; w < nwarps; ++w) tot[0] += rr[w * 8 + 0];
+        for (int j = 0; j < 4; ++j) tot[1 + j] += lg[j];
+      }
       const double v = tot[0] * P.area;
       const double infil = tot[1] * P.area, fix = tot[2] * P.area;
       const double expected = v0 + acc_rain + tot[3] - tot[4] - infil + fix;
@@ -501,36 +724,36 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       }
       n_rows += 1;
       // guard breach (objective.rs:132-145) and incumbent bound (objective.rs:147-149).
-      // Every warp decides from the same peaks; a barrier follows before any thread acts, so
-      // no warp can start writing next-step peaks while another is still reading them.
+      // Every warp decides from the same peaks; the barrier below comes before any thread
+      // acts, so no warp writes next-step peaks (or red, LED) while another still reads them.
       const DevObjective& ob = A.obj;
       int decision = 0;
       if (ob.enabled) {
         auto peak_of = [&](int mpos) -> double {
-          unsigned cell = A.mon_cells[mpos];
-          int rr_ = (int)(cell / (unsigned)nx), cc_ = (int)(cell % (unsigned)nx);
+          const unsigned cell = A.mon_cells[mpos];
+          const int rr_ = (int)(cell / (unsigned)nx), cc_ = (int)(cell % (unsigned)nx);
           int owner = 0;
           while (owner + 1 < C && rr_ >= (int)((long long)(owner + 1) * ny / C)) ++owner;
-          int ra_o = (int)((long long)owner * ny / C);
+          const int ra_o = (int)((long long)owner * ny / C);
           const float* pk = CLUSTERED ? remote(sm.PK, owner) : sm.PK;
           return (double)pk[CK((rr_ - ra_o) * nx + cc_, sm.ncell, 21)];
         };
         if (ob.guard_abort && ob.require && ob.baseline) {
           double best = 0.0; int bk = -1;
           for (int g0 = 0; g0 < ob.n_guard; g0 += 32) {
-            int gk = g0 + lane;
+            const int gk = g0 + lane;
             double w = 0.0; int kk = -1;
             if (gk < ob.n_guard) {
-              int mp = ob.guard_pos[gk];
+              const int mp = ob.guard_pos[gk];
               w = peak_of(mp) - ob.baseline[mp] - ob.tol;
               if (w > 0.0) kk = gk;
             }
             // warp argmax, first index on ties
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
-              double w2 = __shfl_xor_sync(0xffffffffu, w, o);
-              int k2 = __shfl_xor_sync(0xffffffffu, kk, o);
-              bool take = (k2 >= 0) && (kk < 0 || w2 > w || (w2 == w && k2 < kk));
+              const double w2 = __shfl_xor_sync(0xffffffffu, w, o);
+              const int k2 = __shfl_xor_sync(0xffffffffu, kk, o);
+              const bool take = (k2 >= 0) && (kk < 0 || w2 > w || (w2 == w && k2 < kk));
               if (take) { w = w2; kk = k2; }
             }
             if (kk >= 0 && (bk < 0 || w > best)) { best = w; bk = kk; }
@@ -547,19 +770,19 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
           for (int a = 0; a < ob.n_assets; ++a) {
             double pkv = 0.0;
             for (int m = ob.asset_off[a] + lane; m < ob.asset_off[a + 1]; m += 32) {
-              double x = peak_of(ob.asset_pos[m]);
+              const double x = peak_of(ob.asset_pos[m]);
               pkv = pkv > x ? pkv : x;
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) { double x = __shfl_xor_sync(0xffffffffu, pkv, o); pkv = pkv > x ? pkv : x; }
+            for (int o = 16; o > 0; o >>= 1) { const double x = __shfl_xor_sync(0xffffffffu, pkv, o); pkv = pkv > x ? pkv : x; }
             jr += ob.asset_w[a] * ob.tau * itr_math::softplus((pkv - ob.asset_thr[a]) / ob.tau);
           }
           const double je = ob.cut_cost * A.cut[d] + ob.fill_cost * A.fill[d];
           const double lb = jr + ob.earth_w * je;
           if (lb >= ob.incumbent) { decision = 2; lower_bound = lb; }
         }
-        gs.b2();
       }
+      gs.full();
       if (decision != 0) { status = decision; break; }
     }
   }
@@ -569,8 +792,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   // All CTAs of the cluster leave the loop at the same step (identical decisions).
   if (CLUSTERED) { cluster_arrive(); cluster_wait(); } else __syncthreads();
   for (int idx = tid; idx < nr * nx; idx += blockDim.x) {
-    size_t g = CKZ(cell0 + (size_t)ra * nx + idx, (long long)A.n_designs * nx * ny, 20);
-    A.depth_out[g] = sm.H[idx];
+    const size_t g = cell0_off + (size_t)ra * nx + idx;
+    A.depth_out[g] = sm.S4[idx].x;
     A.peak_out[g] = sm.PK[idx];
   }
   if (q == 0 && tid == 0) {

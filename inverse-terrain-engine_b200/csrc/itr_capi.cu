@@ -74,6 +74,8 @@ struct itr_ctx {
   std::string err;
   // options
   int impl = 0, threads = 0, cluster = 0, graph = 1, steps_per_submit = 64;
+  int autotune = 1, autotune_top = 6, probe_steps = 200;
+  float tune_ms = 0.0f;
   // device buffers (batched path)
   DevBuf wet, gn2, bc, dzx, dzy, dzx2, dzy2, h0, cut, fill, mon, obj_i, obj_d, peak, depth, ledger, out, mmax;
   // plain path scratch
@@ -128,10 +130,10 @@ static BatchedFn batched_fn(bool crest, bool clustered, int maxt) {
 static int maxt_bucket(int T) { return T <= 256 ? 256 : T <= 512 ? 512 : T <= 768 ? 768 : 1024; }
 
 // Geometry of the batched kernel for (nx, ny) with C CTAs per design and about T threads.
-static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_target) {
+static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_target, bool crest) {
   LaunchCfg c;
   c.C = C;
-  c.W = (nx + 1 + 31) / 32;
+  c.W = (nx + 1 + 63) / 64;   // warps per strip row; each lane holds two columns
   if (C < 1 || ny < C) return c;
   const int nr_min = ny / C, nr_max = (ny + C - 1) / C;
   int S = T_target / (32 * c.W);
@@ -141,7 +143,7 @@ static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_targe
   c.S = S;
   c.T = S * 32 * c.W;
   if (c.T > 1024) return c;
-  c.smem = batched_smem_bytes(nr_max, nx, S, c.W, c.T / 32);
+  c.smem = batched_smem_bytes(nr_max, nx, S, c.W, c.T / 32, crest ? 1 : 0);
   c.ok = c.smem <= ctx->smem_optin;
   return c;
 }
@@ -191,9 +193,12 @@ static int max_active_clusters(itr_ctx* ctx, const LaunchCfg& cfg, bool crest) {
 static std::vector<LaunchCfg> candidates(itr_ctx* ctx, int nx, int ny, int n_designs, bool crest) {
   std::vector<std::pair<double, LaunchCfg>> v;
   for (int C : {1, 2, 4, 8}) {
-    for (int T : {256, 512, 768, 1024}) {
-      LaunchCfg c = make_cfg(ctx, nx, ny, C, T);
+    for (int T : {256, 384, 512, 640, 768, 896, 1024}) {
+      LaunchCfg c = make_cfg(ctx, nx, ny, C, T, crest);
       if (!c.ok) continue;
+      bool dup = false;
+      for (auto& e : v) if (e.second.C == c.C && e.second.T == c.T) dup = true;
+      if (dup) continue;
       int act = max_active_clusters(ctx, c, crest);
       if (act <= 0) continue;
       double waves = std::ceil((double)n_designs / act);
@@ -208,6 +213,34 @@ static std::vector<LaunchCfg> candidates(itr_ctx* ctx, int nx, int ny, int n_des
   std::vector<LaunchCfg> out;
   for (auto& p : v) out.push_back(p.second);
   return out;
+}
+
+// Time `probe_steps` steps of the batch under each candidate shape (CUDA events on the
+// context stream) and return the fastest. The probe runs write only scratch outputs.
+static int autotune(itr_ctx* ctx, const BatchArgs& A0, const std::vector<LaunchCfg>& cands, int n, LaunchCfg* best) {
+  BatchArgs A = A0;
+  A.max_steps = (unsigned long long)ctx->probe_steps;
+  A.ledger_out = nullptr;
+  A.max_rows = 0;
+  A.obj.enabled = 0;
+  float best_ms = 1e30f;
+  const size_t k = cands.size() < (size_t)ctx->autotune_top ? cands.size() : (size_t)ctx->autotune_top;
+  for (size_t i = 0; i < k; ++i) {
+    LaunchCfg c = cands[i];
+    A.C = c.C; A.W = c.W; A.S = c.S;
+    float ms = 0.0f;
+    for (int rep = 0; rep < 2; ++rep) {   // first launch warms the instruction cache
+      CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+      int rc = launch_batched(ctx, A, c, n);
+      if (rc != ITR_OK) return rc;
+      CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+      CU(cudaEventSynchronize(ctx->ev[2]));
+      CU(cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]));
+    }
+    if (ms < best_ms) { best_ms = ms; *best = c; }
+  }
+  ctx->tune_ms = best_ms;
+  return ITR_OK;
 }
 
 // ------------------------------------------------------------------ input checks ------
@@ -263,6 +296,12 @@ static RunParams make_run_params(const itr_params* p, const itr_grid* g) {
   P.skip_dry = p->skip_dry;
   P.rain.n = p->n_rain;
   for (int i = 0; i < p->n_rain; ++i) { P.rain.t[i] = p->rain_t[i]; P.rain.r[i] = p->rain_rate[i]; }
+  P.rain_sorted = 1;
+  for (int i = 1; i < p->n_rain; ++i) if (!(p->rain_t[i] >= p->rain_t[i - 1])) P.rain_sorted = 0;
+  P.g_f = (float)g->g; P.g_half_f = (float)(0.5 * g->g);
+  P.inv_dx_f = (float)(1.0 / g->dx); P.inv_dy_f = (float)(1.0 / g->dy);
+  P.h_dry_f = (float)p->h_dry; P.heps2_f = (float)(p->h_eps * p->h_eps); P.q_min_f = (float)1e-30;
+  P.nz = -0.0f;
   return P;
 }
 
@@ -362,6 +401,8 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   else if (k == "cluster") { if (!(value == 0 || value == 1 || value == 2 || value == 4 || value == 8)) return fail(ctx, ITR_INVALID_ARG, "cluster must be 0,1,2,4,8"); ctx->cluster = (int)value; }
   else if (k == "graph") ctx->graph = value != 0;
   else if (k == "steps_per_submit") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "steps_per_submit must be >= 1"); ctx->steps_per_submit = (int)value; }
+  else if (k == "autotune") { ctx->autotune = value != 0; ctx->tuned.clear(); }
+  else if (k == "probe_steps") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "probe_steps must be >= 1"); ctx->probe_steps = (int)value; }
   else return fail(ctx, ITR_INVALID_ARG, "unknown option '%s'", key);
   if (k == "threads" || k == "cluster") ctx->tuned.clear();
   return ITR_OK;
@@ -524,14 +565,20 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     LaunchCfg cfg;
     auto key = std::make_tuple(nx, ny, n, (int)g->mode);
     if (ctx->cluster > 0 || ctx->threads > 0) {
-      cfg = make_cfg(ctx, nx, ny, ctx->cluster > 0 ? ctx->cluster : 1, ctx->threads > 0 ? ctx->threads : 512);
+      cfg = make_cfg(ctx, nx, ny, ctx->cluster > 0 ? ctx->cluster : 1, ctx->threads > 0 ? ctx->threads : 512, crest);
       if (!cfg.ok) return fail(ctx, ITR_UNSUPPORTED, "cluster=%d threads=%d does not fit a %dx%d grid in shared memory", ctx->cluster, ctx->threads, nx, ny);
     } else if (ctx->tuned.count(key)) {
       cfg = ctx->tuned[key];
     } else {
       std::vector<LaunchCfg> cands = candidates(ctx, nx, ny, n, crest);
       if (cands.empty()) return fail(ctx, ITR_UNSUPPORTED, "a %dx%d grid does not fit the batched kernel's shared memory (max 8 CTAs per design)", nx, ny);
+      // Measured autotuning: time a short probe (the first steps of this very batch) of the
+      // best few shapes by the model and keep the fastest for this (grid, population) key.
       cfg = cands[0];
+      if (ctx->autotune && cands.size() > 1) {
+        rc = autotune(ctx, A, cands, n, &cfg);
+        if (rc != ITR_OK) return rc;
+      }
       ctx->tuned[key] = cfg;
     }
     A.C = cfg.C; A.W = cfg.W; A.S = cfg.S;

@@ -42,6 +42,7 @@ ITR_DEV float rcbrt(float x) {
 // Step constants, all rounded once from f64 (solver.rs:269-285).
 struct StepK {
   float g, g_half, dt, dtdx, dtdy, inv_dx, inv_dy, h_dry, heps2, q_min, rain, cap;
+  float nz;   // -0.0f read from the kernel parameters at run time (see mul2)
 };
 
 // A face flux tuple: mass, normal momentum seen from the low-index (n_l) and high-index
@@ -49,13 +50,26 @@ struct StepK {
 struct FaceF { float m, nl, nr, t; };
 
 // Desingularised velocity and celerity of a cell.
+// 1/x rounded to nearest (IEEE): the same value as 1.0f / x compiled with IEEE division,
+// through the reciprocal instruction path.
+ITR_DEV float rcp(float x) { return __frcp_rn(x); }
+
+// IEEE square root with zero kept off the instruction's special-case path: sqrt(+-0) is
+// +-0 exactly, so returning x for x == 0 gives the same bits as sqrtf(x) for every input,
+// while dry faces and cells (reduced depth 0) stay on the fast path.
+ITR_DEV float sqrt_rn(float x) {
+  const bool z = x == 0.0f;
+  const float r = sqrtf(z ? 1.0f : x);
+  return z ? x : r;
+}
+
 ITR_DEV void cell_vel(float h, float qx, float qy, float g, float heps2, float& u, float& v, float& c) {
   float h2 = h * h;
-  float inv = 1.0f / (h2 + rmax(h2, heps2));
+  float inv = rcp(h2 + rmax(h2, heps2));
   float t = (h + h) * inv;
   u = qx * t;
   v = qy * t;
-  c = sqrtf(g * h);
+  c = sqrt_rn(g * h);
 }
 
 // HLL flux with two-rarefaction wave speeds; dry-dry faces give exactly zero.
@@ -78,7 +92,7 @@ ITR_DEV FaceF hll(float hl, float ul, float tl, float cl, float hr, float ur, fl
   const bool use_l = sl >= 0.0f;
   const bool use_r = sr <= 0.0f;
   float den = (both_dry || use_l || use_r) ? 1.0f : sr - sl;
-  float inv = 1.0f / den;
+  float inv = rcp(den);
   float slsr = sl * sr;
   float fm_star = (sr * ml - sl * mr + slsr * (hr - hl)) * inv;
   float fn_star = (sr * pl - sl * pr + slsr * (mr - ml)) * inv;
@@ -99,7 +113,7 @@ ITR_DEV FaceF face_signed(float hl, float ul, float vl, float cl, float hr, floa
   float hsl = rmax(hl - rmax(dz, 0.0f), 0.0f);
   float hsr = rmax(hr - rmax(-dz, 0.0f), 0.0f);
   float hred = pos ? hsl : hsr;
-  float cred = sqrtf(g * hred);
+  float cred = sqrt_rn(g * hred);
   float csl = pos ? cred : cl;
   float csr = pos ? cr : cred;
   if (NORMAL_X) return hll(hsl, ul, vl, csl, hsr, ur, vr, csr, g_half);
@@ -112,8 +126,8 @@ ITR_DEV FaceF face_crest(float hl, float ul, float vl, float cl, float hr, float
                          float d_l, float d_r, float g, float g_half) {
   float hsl = rmax(hl - d_l, 0.0f);
   float hsr = rmax(hr - d_r, 0.0f);
-  float csl = d_l > 0.0f ? sqrtf(g * hsl) : cl;
-  float csr = d_r > 0.0f ? sqrtf(g * hsr) : cr;
+  float csl = d_l > 0.0f ? sqrt_rn(g * hsl) : cl;
+  float csr = d_r > 0.0f ? sqrt_rn(g * hsr) : cr;
   if (NORMAL_X) return hll(hsl, ul, vl, csl, hsr, ur, vr, csr, g_half);
   return hll(hsl, vl, ul, csl, hsr, vr, ur, csr, g_half);
 }
@@ -149,14 +163,14 @@ ITR_DEV CellNew update_cell(float h, float qx, float qy, const FaceF& w, const F
   float r = rcbrt(dry ? 1.0f : h3);
   float r3 = r * r * r;
   float r7 = r3 * r3 * r;
-  float qm = sqrtf(qx1 * qx1 + qy1 * qy1);
-  float inv = 1.0f / (1.0f + k.dt * gn2 * qm * r7);
+  float qm = sqrt_rn(qx1 * qx1 + qy1 * qy1);
+  float inv = rcp(1.0f + k.dt * gn2 * qm * r7);
   float keep = dry ? 0.0f : 1.0f;
   float qx2 = qx1 * inv * keep;
   float qy2 = qy1 * inv * keep;
   if (rabs(qx2) < k.q_min) qx2 = 0.0f;
   if (rabs(qy2) < k.q_min) qy2 = 0.0f;
-  float c = sqrtf(k.g * h3);
+  float c = sqrt_rn(k.g * h3);
   o.s = (rabs(qx2) * r3 + c) * k.inv_dx + (rabs(qy2) * r3 + c) * k.inv_dy;
   o.bad = bad || !(qm == qm);
   o.h = canon(h3);
@@ -208,13 +222,58 @@ ITR_DEV double rain_integral(const Rain& R, double a, double b) {
   return total;
 }
 
+// The same rate and integral, for sorted breakpoints, with a cursor that only moves
+// forward (simulated time is monotone): identical arithmetic on identical operands, so
+// identical bits, without rescanning the table every step.
+struct RainCursor {
+  int seg;   // first k with t[k+1] >= last query (rate) ...
+  int brk;   // first breakpoint index with t[k] > last lower limit
+};
+
+ITR_DEV double rain_rate_c(const Rain& R, double x, int& seg) {
+  if (R.n == 0) return 0.0;
+  if (x <= R.t[0]) return R.r[0];
+  while (seg + 1 < R.n && R.t[seg + 1] < x) ++seg;
+  if (seg + 1 < R.n) {
+    double t0 = R.t[seg], r0 = R.r[seg], t1 = R.t[seg + 1], r1 = R.r[seg + 1];
+    if (t1 == t0) return r1;
+    return r0 + (r1 - r0) * (x - t0) / (t1 - t0);
+  }
+  return R.r[R.n - 1];
+}
+
+ITR_DEV double rain_integral_c(const Rain& R, double a, double b, RainCursor& cu) {
+  if (b <= a) return 0.0;
+  if (R.n == 0) return 0.0;
+  int seg = cu.seg;
+  double total = 0.0, tt = a, rr = rain_rate_c(R, a, seg);
+  cu.seg = seg;
+  while (cu.brk < R.n && !(R.t[cu.brk] > a)) ++cu.brk;
+  for (int k = cu.brk; k < R.n && R.t[k] < b; ++k) {
+    double tk = R.t[k];
+    int s2 = seg;
+    double rk = rain_rate_c(R, tk, s2);
+    total += 0.5 * (rr + rk) * (tk - tt);
+    tt = tk;
+    rr = rk;
+    seg = s2;
+  }
+  double rb = rain_rate_c(R, b, seg);
+  total += 0.5 * (rr + rb) * (b - tt);
+  return total;
+}
+
 // Run-wide scalars of one call.
 struct RunParams {
   double duration, sync, cfl, dt_max, h_dry, h_eps, infil, initial_depth;
   double dx, dy, g, area, wet_count;
   uint32_t n_sync;
   int skip_dry;
+  int rain_sorted;   // breakpoints non-decreasing in time: the cursor path is exact
   Rain rain;
+  // step-invariant f32 constants (solver.rs:269-285), rounded once on the host
+  float g_f, g_half_f, inv_dx_f, inv_dy_f, h_dry_f, heps2_f, q_min_f;
+  float nz;   // -0.0f, supplied at run time (see mul2)
 };
 
 ITR_DEV double dmin_num(double a, double b) { return a < b ? a : b; }  // operands never NaN here
@@ -237,6 +296,32 @@ ITR_DEV StepPlan plan_step(const RunParams& P, double t, uint32_t sync_index, do
   return s;
 }
 
+ITR_DEV StepPlan plan_step_c(const RunParams& P, double t, uint32_t sync_index, double dt_cfl, RainCursor& cu) {
+  StepPlan s;
+  double t_sync = dmin_num((double)(sync_index + 1) * P.sync, P.duration);
+  double dt = dmin_num(dt_cfl, P.dt_max);
+  s.hits = t + dt >= t_sync - 1e-9 * P.sync;
+  if (s.hits) dt = t_sync - t;
+  s.rain = P.rain_sorted ? rain_integral_c(P.rain, t, t + dt, cu) : rain_integral(P.rain, t, t + dt);
+  s.t_new = s.hits ? t_sync : t + dt;
+  s.dt = dt;
+  return s;
+}
+
+// Per-step constants from the host-rounded invariants and this step's dt and rain.
+ITR_DEV StepK step_consts(const RunParams& P, double dt, double rain) {
+  StepK k;
+  k.g = P.g_f; k.g_half = P.g_half_f; k.inv_dx = P.inv_dx_f; k.inv_dy = P.inv_dy_f;
+  k.h_dry = P.h_dry_f; k.heps2 = P.heps2_f; k.q_min = P.q_min_f;
+  k.dt = (float)dt;
+  k.dtdx = (float)(dt / P.dx);
+  k.dtdy = (float)(dt / P.dy);
+  k.rain = (float)rain;
+  k.cap = (float)(P.infil * dt);
+  k.nz = P.nz;
+  return k;
+}
+
 ITR_DEV StepK make_consts(const RunParams& P, double dt, double rain) {
   StepK k;
   k.g = (float)P.g;
@@ -251,6 +336,7 @@ ITR_DEV StepK make_consts(const RunParams& P, double dt, double rain) {
   k.q_min = (float)1e-30;
   k.rain = (float)rain;
   k.cap = (float)(P.infil * dt);
+  k.nz = P.nz;
   return k;
 }
 
@@ -286,5 +372,186 @@ struct DesignOut {
   int n_rows;
   int pad;
 };
+
+}  // namespace itr
+
+// --------------------------------------------------------------- two cells at once ----
+// The same arithmetic on pairs of cells: every add and multiply is a paired FP32
+// instruction (__fadd2_rn / __fmul2_rn: each component is the IEEE round-to-nearest
+// result of the scalar operation), every compare, select, square root and reciprocal is
+// done per component. Association order is the scalar code's, so each component has the
+// same bits as the scalar path (and as the reference's f32 kernel).
+namespace itr {
+
+struct B2 { bool x, y; };
+struct Face2 { float2 m, nl, nr, t; };
+
+ITR_DEV float2 f2(float a) { return make_float2(a, a); }
+// Packed FP32 pairs through PTX with an explicit .rn rounding modifier: such instructions are
+// never contracted into fused multiply-adds (the float2 intrinsics may be), so each component
+// is exactly the scalar IEEE result.
+ITR_DEV unsigned long long pk2(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+ITR_DEV float2 upk2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+ITR_DEV float2 add2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+ITR_DEV float2 sub2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+// Paired product as fma(a, b, -0): exactly round(a*b) for every input (x + -0 == x, zeros
+// keep their sign). The -0 must not be a compile-time constant, else the compiler turns the
+// fma back into a multiply and fuses it with the next add (observed on sm_100a), which
+// would round once instead of twice; it is the kernel parameter StepK::nz.
+ITR_DEV float2 mul2(float2 a, float2 b, float nz) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)), "l"(pk2(make_float2(nz, nz))));
+  return upk2(r);
+}
+ITR_DEV float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+ITR_DEV float2 sel2(B2 c, float2 a, float2 b) { return make_float2(c.x ? a.x : b.x, c.y ? a.y : b.y); }
+ITR_DEV float2 max2(float2 a, float2 b) { return make_float2(rmax(a.x, b.x), rmax(a.y, b.y)); }
+ITR_DEV float2 min2(float2 a, float2 b) { return make_float2(rmin(a.x, b.x), rmin(a.y, b.y)); }
+ITR_DEV B2 gt2(float2 a, float b) { return B2{a.x > b, a.y > b}; }
+ITR_DEV B2 ge2(float2 a, float b) { return B2{a.x >= b, a.y >= b}; }
+ITR_DEV B2 le2(float2 a, float b) { return B2{a.x <= b, a.y <= b}; }
+ITR_DEV B2 lt2(float2 a, float b) { return B2{a.x < b, a.y < b}; }
+ITR_DEV B2 not2(B2 a) { return B2{!a.x, !a.y}; }
+ITR_DEV B2 and2(B2 a, B2 b) { return B2{a.x && b.x, a.y && b.y}; }
+ITR_DEV B2 or2(B2 a, B2 b) { return B2{a.x || b.x, a.y || b.y}; }
+ITR_DEV float2 sqrt2(float2 a) { return make_float2(sqrt_rn(a.x), sqrt_rn(a.y)); }
+ITR_DEV float2 rcp2(float2 a) { return make_float2(rcp(a.x), rcp(a.y)); }
+ITR_DEV float2 canon2(float2 a) { return make_float2(canon(a.x), canon(a.y)); }
+ITR_DEV float2 abs2(float2 a) { return make_float2(rabs(a.x), rabs(a.y)); }
+
+ITR_DEV float2 rcbrt2(float2 x, float nz) {
+  float2 r = make_float2(__uint_as_float(0x54A23280u - __float_as_uint(x.x) / 3u),
+                         __uint_as_float(0x54A23280u - __float_as_uint(x.y) / 3u));
+  const float2 x3 = mul2(x, f2((float)(1.0 / 3.0)), nz);
+  const float2 c43 = f2((float)(4.0 * (1.0 / 3.0)));
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float2 r2 = mul2(r, r, nz);
+    r = sub2(mul2(r, c43, nz), mul2(x3, mul2(r2, r2, nz), nz));
+  }
+  return r;
+}
+
+// hll (numerics.rs:56-93) on two faces.
+ITR_DEV Face2 hll2(float2 hl, float2 ul, float2 tl, float2 cl, float2 hr, float2 ur, float2 tr, float2 cr, float g_half, float nz) {
+  const float NZ = nz;
+  const B2 dry_l = not2(gt2(hl, 0.0f));
+  const B2 dry_r = not2(gt2(hr, 0.0f));
+  const float2 ustar = sub2(add2(mul2(f2(0.5f), add2(ul, ur), NZ), cl), cr);
+  const float2 cstar = add2(mul2(f2(0.5f), add2(cl, cr), NZ), mul2(f2(0.25f), sub2(ul, ur), NZ));
+  const float2 ul_cl = sub2(ul, cl);
+  const float2 ur_cr = add2(ur, cr);
+  const float2 slw = min2(ul_cl, sub2(ustar, cstar));
+  const float2 srw = max2(ur_cr, add2(ustar, cstar));
+  const float2 sl = sel2(dry_l, sub2(ur, mul2(f2(2.0f), cr, NZ)), sel2(dry_r, ul_cl, slw));
+  const float2 sr = sel2(dry_l, ur_cr, sel2(dry_r, add2(ul, mul2(f2(2.0f), cl, NZ)), srw));
+  const float2 ml = mul2(hl, ul, NZ);
+  const float2 mr = mul2(hr, ur, NZ);
+  const float2 gh = f2(g_half);
+  const float2 pl_ = mul2(mul2(gh, hl, NZ), hl, NZ);
+  const float2 pr_ = mul2(mul2(gh, hr, NZ), hr, NZ);
+  const float2 pl = add2(mul2(ml, ul, NZ), pl_);
+  const float2 pr = add2(mul2(mr, ur, NZ), pr_);
+  const B2 both_dry = and2(dry_l, dry_r);
+  const B2 use_l = ge2(sl, 0.0f);
+  const B2 use_r = le2(sr, 0.0f);
+  const B2 trivial = or2(or2(both_dry, use_l), use_r);
+  const float2 den = sel2(trivial, f2(1.0f), sub2(sr, sl));
+  const float2 inv = rcp2(den);
+  const float2 slsr = mul2(sl, sr, NZ);
+  const float2 fm_star = mul2(add2(sub2(mul2(sr, ml, NZ), mul2(sl, mr, NZ)), mul2(slsr, sub2(hr, hl), NZ)), inv, NZ);
+  const float2 fn_star = mul2(add2(sub2(mul2(sr, pl, NZ), mul2(sl, pr, NZ)), mul2(slsr, sub2(mr, ml), NZ)), inv, NZ);
+  const float2 fm = sel2(both_dry, f2(0.0f), sel2(use_l, ml, sel2(use_r, mr, fm_star)));
+  const float2 fn = sel2(both_dry, f2(0.0f), sel2(use_l, pl, sel2(use_r, pr, fn_star)));
+  Face2 f;
+  f.m = fm;
+  f.nl = sub2(fn, pl_);
+  f.nr = sub2(fn, pr_);
+  f.t = mul2(fm, sel2(gt2(fm, 0.0f), tl, tr), NZ);
+  return f;
+}
+
+// face_signed / face_crest (numerics.rs:95-129) on two faces; (ul,vl,cl) of the low side.
+template <bool NORMAL_X, bool CREST>
+ITR_DEV Face2 face2(float2 hl, float2 ul, float2 vl, float2 cl, float2 hr, float2 ur, float2 vr, float2 cr,
+                    float2 d0, float2 d1, const StepK& k) {
+  const float NZ = k.nz;
+  float2 hsl, hsr, csl, csr;
+  if (!CREST) {
+    const B2 pos = gt2(d0, 0.0f);
+    hsl = max2(sub2(hl, max2(d0, f2(0.0f))), f2(0.0f));
+    hsr = max2(sub2(hr, max2(neg2(d0), f2(0.0f))), f2(0.0f));
+    const float2 cred = sqrt2(mul2(f2(k.g), sel2(pos, hsl, hsr), NZ));
+    csl = sel2(pos, cred, cl);
+    csr = sel2(pos, cr, cred);
+  } else {
+    hsl = max2(sub2(hl, d0), f2(0.0f));
+    hsr = max2(sub2(hr, d1), f2(0.0f));
+    const B2 pl = gt2(d0, 0.0f), pr = gt2(d1, 0.0f);
+    const float2 sl = sqrt2(mul2(f2(k.g), hsl, NZ)), sr = sqrt2(mul2(f2(k.g), hsr, NZ));
+    csl = sel2(pl, sl, cl);
+    csr = sel2(pr, sr, cr);
+  }
+  if (NORMAL_X) return hll2(hsl, ul, vl, csl, hsr, ur, vr, csr, k.g_half, NZ);
+  return hll2(hsl, vl, ul, csl, hsr, vr, ur, csr, k.g_half, NZ);
+}
+
+struct CellNew2 {
+  float2 h, qx, qy, s, infil, fix, c;
+  B2 bad;
+};
+
+// flux_update then sources (numerics.rs:144-195) on two cells.
+ITR_DEV CellNew2 update_cell2(float2 h, float2 qx, float2 qy, const Face2& w, const Face2& e, const Face2& n,
+                              const Face2& s, float2 wet, float2 gn2, const StepK& k) {
+  const float NZ = k.nz;
+  const float2 dtdx = f2(k.dtdx), dtdy = f2(k.dtdy);
+  float2 h1 = sub2(sub2(h, mul2(dtdx, sub2(e.m, w.m), NZ)), mul2(dtdy, sub2(s.m, n.m), NZ));
+  const float2 qx1 = sub2(sub2(qx, mul2(dtdx, sub2(e.nl, w.nr), NZ)), mul2(dtdy, sub2(s.t, n.t), NZ));
+  const float2 qy1 = sub2(sub2(qy, mul2(dtdx, sub2(e.t, w.t), NZ)), mul2(dtdy, sub2(s.nl, n.nr), NZ));
+  CellNew2 o;
+  B2 bad = not2(B2{h1.x >= -k.h_dry, h1.y >= -k.h_dry});
+  const B2 neg = lt2(h1, 0.0f);
+  o.fix = sel2(neg, neg2(h1), f2(0.0f));
+  h1 = sel2(neg, f2(0.0f), h1);
+  const float2 h2 = add2(h1, mul2(f2(k.rain), wet, NZ));
+  o.infil = min2(mul2(f2(k.cap), wet, NZ), h2);
+  const float2 h3 = sub2(h2, o.infil);
+  const B2 dry = lt2(h3, k.h_dry);
+  const float2 r = rcbrt2(sel2(dry, f2(1.0f), h3), NZ);
+  const float2 r3 = mul2(mul2(r, r, NZ), r, NZ);
+  const float2 r7 = mul2(mul2(r3, r3, NZ), r, NZ);
+  const float2 qm = sqrt2(add2(mul2(qx1, qx1, NZ), mul2(qy1, qy1, NZ)));
+  const float2 inv = rcp2(add2(f2(1.0f), mul2(mul2(mul2(f2(k.dt), gn2, NZ), qm, NZ), r7, NZ)));
+  const float2 keep = sel2(dry, f2(0.0f), f2(1.0f));
+  float2 qx2 = mul2(mul2(qx1, inv, NZ), keep, NZ);
+  float2 qy2 = mul2(mul2(qy1, inv, NZ), keep, NZ);
+  qx2 = sel2(lt2(abs2(qx2), k.q_min), f2(0.0f), qx2);
+  qy2 = sel2(lt2(abs2(qy2), k.q_min), f2(0.0f), qy2);
+  const float2 c = sqrt2(mul2(f2(k.g), h3, NZ));
+  o.s = add2(mul2(add2(mul2(abs2(qx2), r3, NZ), c), f2(k.inv_dx), NZ), mul2(add2(mul2(abs2(qy2), r3, NZ), c), f2(k.inv_dy), NZ));
+  o.bad = B2{bad.x || !(qm.x == qm.x), bad.y || !(qm.y == qm.y)};
+  o.h = canon2(h3);
+  o.qx = canon2(qx2);
+  o.qy = canon2(qy2);
+  o.c = c;
+  return o;
+}
 
 }  // namespace itr

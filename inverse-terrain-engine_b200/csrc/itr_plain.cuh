@@ -241,7 +241,7 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
     if (!(c.t < P.duration && c.sync_index < P.n_sync)) { c.done = 1; return; }
     if (c.step >= A.max_steps) { c.status = 4; c.done = 1; return; }
     c.pl = plan_step(P, c.t, c.sync_index, c.dt_cfl);
-    c.k = make_consts(P, c.pl.dt, c.pl.rain);
+    c.k = step_consts(P, c.pl.dt, c.pl.rain);
   }
 }
 

@@ -892,59 +892,78 @@ template <class T> struct Solver {
 
   // step_fused (kernel.rs:590-727), single strip: in-place row sweep, carried y-face row,
   // dry-row skipping. Bitwise identical to step_oracle (checked by the tests).
+  // Buffers of the fused sweep, allocated once per run (the reference's fused kernel makes
+  // no heap allocation in steady state, crates/itr-hydro/tests/equivalence.rs:186-207).
+  struct FusedBufs {
+    std::vector<uint8_t> dry;
+    std::vector<T> tu, tv, tc, bu, bv, bcv;
+    std::vector<T> top_m, top_nl, top_nr, top_t, bot_m, bot_nl, bot_nr, bot_t;
+    std::vector<T> cu, cv, cc, nu, nv, nc;
+    std::vector<T> pm, pnl, pnr, pt, qm, qnl, qnr, qt;
+    std::vector<T> xm, xnl, xnr, xt;
+    std::vector<RowAcc> accs;
+    std::vector<double> ssr;
+    void init(size_t nx, size_t ny) {
+      size_t W = nx + 2;
+      dry.assign(ny + 2, 0);
+      for (auto* v : {&tu, &tv, &tc, &bu, &bv, &bcv, &top_m, &top_nl, &top_nr, &top_t, &bot_m, &bot_nl, &bot_nr, &bot_t,
+                      &cu, &cv, &cc, &nu, &nv, &nc, &pm, &pnl, &pnr, &pt, &qm, &qnl, &qnr, &qt, &xm, &xnl, &xnr, &xt})
+        v->assign(W, T(0));
+      accs.assign(ny, RowAcc());
+      ssr.assign(ny, 0.0);
+    }
+  } fb;
+
+  // step_fused (kernel.rs:590-727), single strip: in-place row sweep, carried y-face row,
+  // dry-row skipping. Bitwise identical to step_oracle (checked by the tests).
   StepStats<T> step_fused(const StepConsts<T>& k, double dt, double t_new, bool want_sum_s) {
-    size_t nx = L.nx, ny = L.ny, W = nx + 2;
+    size_t ny = L.ny;
+    FusedBufs& B = fb;
     bool rain_zero = !(k.rain > T(0));
-    std::vector<uint8_t> dry(ny + 2);
-    for (size_t j = 0; j < ny + 2; ++j) dry[j] = row_dry[j] && !ghost_wet[j];
-    auto skippable = [&](size_t j) { return p.skip_dry && rain_zero && dry[j - 1] && dry[j] && dry[j + 1]; };
+    for (size_t j = 0; j < ny + 2; ++j) B.dry[j] = row_dry[j] && !ghost_wet[j];
+    auto skippable = [&](size_t j) { return p.skip_dry && rain_zero && B.dry[j - 1] && B.dry[j] && B.dry[j + 1]; };
     // Pre-phase: boundary y-face rows (top = face 0, bottom = face ny), old state.
-    std::vector<T> tu(W), tv(W), tc(W), bu(W), bv(W), bc(W);
-    std::vector<T> top_m(W, T(0)), top_nl(W, T(0)), top_nr(W, T(0)), top_t(W, T(0));
-    std::vector<T> bot_m(W, T(0)), bot_nl(W, T(0)), bot_nr(W, T(0)), bot_t(W, T(0));
-    vel_row(0, tu.data(), tv.data(), tc.data(), k); vel_row(1, bu.data(), bv.data(), bc.data(), k);
-    yface_row(0, tu.data(), tv.data(), tc.data(), bu.data(), bv.data(), bc.data(), top_m.data(), top_nl.data(), top_nr.data(), top_t.data(), k);
-    vel_row(ny, tu.data(), tv.data(), tc.data(), k); vel_row(ny + 1, bu.data(), bv.data(), bc.data(), k);
-    yface_row(ny, tu.data(), tv.data(), tc.data(), bu.data(), bv.data(), bc.data(), bot_m.data(), bot_nl.data(), bot_nr.data(), bot_t.data(), k);
+    vel_row(0, B.tu.data(), B.tv.data(), B.tc.data(), k); vel_row(1, B.bu.data(), B.bv.data(), B.bcv.data(), k);
+    yface_row(0, B.tu.data(), B.tv.data(), B.tc.data(), B.bu.data(), B.bv.data(), B.bcv.data(), B.top_m.data(), B.top_nl.data(),
+              B.top_nr.data(), B.top_t.data(), k);
+    vel_row(ny, B.tu.data(), B.tv.data(), B.tc.data(), k); vel_row(ny + 1, B.bu.data(), B.bv.data(), B.bcv.data(), k);
+    yface_row(ny, B.tu.data(), B.tv.data(), B.tc.data(), B.bu.data(), B.bv.data(), B.bcv.data(), B.bot_m.data(), B.bot_nl.data(),
+              B.bot_nr.data(), B.bot_t.data(), k);
     double dt_dy = dt * tb->dy, dt_dx = dt * tb->dx;
-    auto top = y_boundary(top_m.data(), dt_dx, true);
-    auto bot = y_boundary(bot_m.data(), dt_dx, false);
-    std::vector<T> cu(W), cv(W), cc(W), nu(W), nv(W), nc(W);
-    std::vector<T> pm = top_m, pnl = top_nl, pnr = top_nr, pt = top_t;   // g_prev
-    std::vector<T> qm(W, T(0)), qnl(W, T(0)), qnr(W, T(0)), qt(W, T(0)); // g_next
-    std::vector<T> xm(W), xnl(W), xnr(W), xt(W);
-    std::vector<RowAcc> accs(ny);
-    std::vector<double> ssr(ny, 0.0);
+    auto top = y_boundary(B.top_m.data(), dt_dx, true);
+    auto bot = y_boundary(B.bot_m.data(), dt_dx, false);
+    B.pm = B.top_m; B.pnl = B.top_nl; B.pnr = B.top_nr; B.pt = B.top_t;   // g_prev
     bool cur_valid = false;
     for (size_t j = 1; j <= ny; ++j) {
       if (skippable(j)) {
-        RowAcc a; a.skipped = true; accs[j - 1] = a;
-        new_dry[j] = 1; ssr[j - 1] = 0.0;
-        std::fill(qm.begin(), qm.end(), T(0)); std::fill(qnl.begin(), qnl.end(), T(0));
-        std::fill(qnr.begin(), qnr.end(), T(0)); std::fill(qt.begin(), qt.end(), T(0));
-        std::swap(pm, qm); std::swap(pnl, qnl); std::swap(pnr, qnr); std::swap(pt, qt);
+        RowAcc a; a.skipped = true; B.accs[j - 1] = a;
+        new_dry[j] = 1; B.ssr[j - 1] = 0.0;
+        std::fill(B.qm.begin(), B.qm.end(), T(0)); std::fill(B.qnl.begin(), B.qnl.end(), T(0));
+        std::fill(B.qnr.begin(), B.qnr.end(), T(0)); std::fill(B.qt.begin(), B.qt.end(), T(0));
+        std::swap(B.pm, B.qm); std::swap(B.pnl, B.qnl); std::swap(B.pnr, B.qnr); std::swap(B.pt, B.qt);
         cur_valid = false;
         continue;
       }
-      if (!cur_valid) vel_row(j, cu.data(), cv.data(), cc.data(), k);
+      if (!cur_valid) vel_row(j, B.cu.data(), B.cv.data(), B.cc.data(), k);
       if (j + 1 <= ny) {
-        vel_row(j + 1, nu.data(), nv.data(), nc.data(), k);
-        yface_row(j, cu.data(), cv.data(), cc.data(), nu.data(), nv.data(), nc.data(), qm.data(), qnl.data(), qnr.data(), qt.data(), k);
+        vel_row(j + 1, B.nu.data(), B.nv.data(), B.nc.data(), k);
+        yface_row(j, B.cu.data(), B.cv.data(), B.cc.data(), B.nu.data(), B.nv.data(), B.nc.data(), B.qm.data(), B.qnl.data(),
+                  B.qnr.data(), B.qt.data(), k);
         cur_valid = true;
       } else {
-        qm = bot_m; qnl = bot_nl; qnr = bot_nr; qt = bot_t;
+        B.qm = B.bot_m; B.qnl = B.bot_nl; B.qnr = B.bot_nr; B.qt = B.bot_t;
         cur_valid = false;
       }
-      xface_row(j, cu.data(), cv.data(), cc.data(), xm.data(), xnl.data(), xnr.data(), xt.data(), k);
-      RowAcc a = update_row(j, xm.data(), xnl.data(), xnr.data(), xt.data(), pm.data(), pnl.data(), pnr.data(), pt.data(),
-                            qm.data(), qnl.data(), qnr.data(), qt.data(), k, want_sum_s, dt_dy, t_new);
-      new_dry[j] = !a.wet; ssr[j - 1] = a.sum_s; accs[j - 1] = a;
-      std::swap(pm, qm); std::swap(pnl, qnl); std::swap(pnr, qnr); std::swap(pt, qt);
-      if (cur_valid) { std::swap(cu, nu); std::swap(cv, nv); std::swap(cc, nc); }
+      xface_row(j, B.cu.data(), B.cv.data(), B.cc.data(), B.xm.data(), B.xnl.data(), B.xnr.data(), B.xt.data(), k);
+      RowAcc a = update_row(j, B.xm.data(), B.xnl.data(), B.xnr.data(), B.xt.data(), B.pm.data(), B.pnl.data(), B.pnr.data(),
+                            B.pt.data(), B.qm.data(), B.qnl.data(), B.qnr.data(), B.qt.data(), k, want_sum_s, dt_dy, t_new);
+      new_dry[j] = !a.wet; B.ssr[j - 1] = a.sum_s; B.accs[j - 1] = a;
+      std::swap(B.pm, B.qm); std::swap(B.pnl, B.qnl); std::swap(B.pnr, B.qnr); std::swap(B.pt, B.qt);
+      if (cur_valid) { std::swap(B.cu, B.nu); std::swap(B.cv, B.nv); std::swap(B.cc, B.nc); }
     }
     new_dry[0] = 1; new_dry[ny + 1] = 1;
-    row_dry = new_dry;
-    return finalize(accs, top, bot, ssr);
+    std::swap(row_dry, new_dry);
+    return finalize(B.accs, top, bot, B.ssr);
   }
 
   double volume(double area) const {
@@ -1004,6 +1023,7 @@ template <class T> struct Solver {
     h.assign(L.len(), T(0)); qx.assign(L.len(), T(0)); qy.assign(L.len(), T(0));
     row_dry.assign(ny + 2, 0); ghost_wet.assign(ny + 2, 0); new_dry.assign(ny + 2, 0);
     rs_infil.assign(nx + 2, T(0)); rs_fix.assign(nx + 2, T(0)); rs_s.assign(nx + 2, T(0));
+    fb.init(nx, ny);
     zlev = pt.z_level();
     mon.init(monitors, nx, ny);
     track_peak = want_peak;
