@@ -179,6 +179,26 @@ int itr_gpu_last_timing(itr_ctx* ctx, double* kernel_ms, double* total_ms, uint6
  * results kept on the device; for timing the kernel over resident inputs. */
 int itr_gpu_rerun_resident(itr_ctx* ctx);
 
+/* ---- Allocation-free plain forward. No reference counterpart. ----
+ * For callers that cannot allocate device memory when they run a design: a process that
+ * has committed the whole device to its own pool, a caller whose other streams must not be
+ * stalled by the device-wide synchronisation of cudaMalloc/cudaFree, a search loop that
+ * must not fail mid-way on an out-of-memory error. It runs the plain path's kernels (same
+ * bits as itr_gpu_run_batch) for ONE design on scratch held in a static device array of
+ * fixed size, reserved when the library's module loads; the call allocates nothing, on the
+ * device or the host. Inputs and results are host buffers with run_batch's meaning;
+ * there is no objective (j = 0, no aborts). Runs on the device's legacy default stream
+ * and returns when the results are in the host buffers.
+ * Limits, rejected with ITR_INVALID_ARG and a message in err before any device work: */
+#define ITR_STATIC_MAX_POINTS 263169      /* (nx+1)*(ny+1), e.g. 512 x 512 cells      */
+#define ITR_STATIC_MAX_TILES 16384        /* ceil(nx/16) * ceil(ny/16)                 */
+#define ITR_STATIC_MAX_MONITORS 65536     /* n_mon                                     */
+#define ITR_STATIC_MAX_LEDGER_ROWS 4096   /* result->max_rows when result->ledger set  */
+/* One static array per device: calls on the same device that overlap in time (several
+ * host threads or streams) race on it and corrupt each other's results. */
+int itr_gpu_run_plain_static(int device, const itr_params* p, const itr_grid* g, const itr_design* design,
+                             const uint32_t* monitors, int32_t n_mon, itr_result* result, char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

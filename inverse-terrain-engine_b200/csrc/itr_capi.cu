@@ -15,6 +15,7 @@
 #include <tuple>
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 #include "../../include/itr_gpu.h"
 #include "itr_device.cuh"
 #include "itr_batched.cuh"
@@ -746,3 +747,6 @@ extern "C" int itr_gpu_rerun_resident(itr_ctx* ctx) {
   ctx->launches = launches;
   return ITR_OK;
 }
+
+// Allocation-free variant of the plain path (static device scratch).
+#include "itr_static.cuh"
