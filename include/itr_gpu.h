@@ -194,8 +194,12 @@ int itr_gpu_rerun_resident(itr_ctx* ctx);
 #define ITR_STATIC_MAX_TILES 16384        /* ceil(nx/16) * ceil(ny/16)                 */
 #define ITR_STATIC_MAX_MONITORS 65536     /* n_mon                                     */
 #define ITR_STATIC_MAX_LEDGER_ROWS 4096   /* result->max_rows when result->ledger set  */
-/* One static array per device: calls on the same device that overlap in time (several
- * host threads or streams) race on it and corrupt each other's results. */
+/* One static array per device, shared by every call, which finds it holding the previous
+ * call's contents (the call clears what must start at zero). Calls on the same device that
+ * overlap in time (several host threads or streams) race on it and corrupt each other's
+ * results. The first call on a device does the set-up: with that device current it looks
+ * up the array's device address (cudaGetSymbolAddress) and keeps it; make that first call
+ * before any stream capture. */
 int itr_gpu_run_plain_static(int device, const itr_params* p, const itr_grid* g, const itr_design* design,
                              const uint32_t* monitors, int32_t n_mon, itr_result* result, char* err, size_t errlen);
 

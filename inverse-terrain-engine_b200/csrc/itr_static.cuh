@@ -19,9 +19,11 @@
 // Limits (rejected with ITR_INVALID_ARG and a message before any device work):
 //   (nx+1)*(ny+1) <= ITR_STATIC_MAX_POINTS, ceil(nx/16)*ceil(ny/16) <= ITR_STATIC_MAX_TILES,
 //   n_mon <= ITR_STATIC_MAX_MONITORS, ledger rows <= ITR_STATIC_MAX_LEDGER_ROWS, no objective.
-// One static array per device: calls on the same device that overlap in time (two host
-// threads, or several streams) race on it and corrupt each other's results; callers
-// serialise them.
+// One static array per device, kept from call to call: each call clears what must start at
+// zero. Calls on the same device that overlap in time (two host threads, or several
+// streams) race on it and corrupt each other's results; callers serialise them. The first
+// call on a device looks up the array's address (see static_scratch) and should come
+// before any stream capture.
 #pragma once
 
 namespace itr {
@@ -101,7 +103,9 @@ struct DeviceGuard {
 };
 
 // Device address of the static array on `device`, looked up once per device with that
-// device current (the symbol has one instance per device).
+// device current (the symbol has one instance per device). In host code the array's name
+// is only a host-side stand-in, so kernels get this address, never the name. The lookup
+// happens in the first call on a device; that first call belongs before any stream capture.
 int static_scratch(int device, unsigned char** out, char* err, size_t errlen) {
   std::lock_guard<std::mutex> lk(g_static_mu);
   if (!g_static_addr[device]) {

@@ -3,7 +3,10 @@
 Two consecutive calls must each reproduce the context entry point (itr_gpu_run_batch) bit
 for bit on the same design: everything, ledger included, against its plain path (the same
 kernels), and the state (depth, peaks, monitor maxima, steps) against its default batched
-path. The second call checks that nothing of the first survives in the static scratch. The size limit is checked on the host, before any device work.
+path. The second call checks that nothing of the first survives in the static scratch.
+The size limit is checked on the host, before any device work. The entry point exists for
+callers that cannot allocate device memory when they run a design (a device committed to
+their own pool, other streams that cudaMalloc's device-wide synchronisation would stall).
 This file sorts last so that it also runs after every other GPU test in one process.
 """
 from __future__ import annotations
