@@ -166,6 +166,9 @@ int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int3
  *   "cluster"  CTAs per design of the batched kernel (0 = autotune)
  *   "graph"    1 = capture the batched launch and its copies in a CUDA graph (default 1)
  *   "steps_per_submit"  plain kernel: steps between host polls (default 64)
+ *   "exact_special"     1 = the batched kernel computes every reciprocal and square root
+ *                       with the IEEE-exact library routines instead of its own branch-free
+ *                       ones (identical results; for checking, default 0)
  * Returns ITR_INVALID_ARG for an unknown key. */
 int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value);
 

@@ -39,6 +39,7 @@
 namespace itr {
 namespace cg = cooperative_groups;
 
+
 struct BatchArgs {
   RunParams P;
   int nx, ny, mode;
@@ -64,6 +65,7 @@ struct BatchArgs {
   int max_rows;
   DesignOut* out;     // n_designs
   unsigned long long max_steps;
+  unsigned exact;     // 1: every paired reciprocal through the IEEE routine (checking)
 };
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -424,6 +426,9 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       s0_l = s0_l > rr ? s0_l : rr;
     }
   }
+  // prefetch slots of columns past the grid are never written: zero them once, so the lanes
+  // that carry no cell compute on zeros (finite operands, no needless reciprocal fallbacks)
+  for (int i = tid; i < 2 * S * K * vlanes; i += blockDim.x) sm.PF[i] = 0.0f;
   if (tid < 8) { sm.slot[tid] = 0u; sm.LED[tid] = 0.0; }
   if (tid == 0) mbar_init(sm.mbar, blockDim.x);
   {
@@ -488,7 +493,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   while (t < P.duration && sync_index < P.n_sync) {
     if (step >= A.max_steps) { status = 4; break; }
     const StepPlan pl = plan_step_c(P, t, sync_index, dt_cfl, rcur);
-    const StepK k = step_consts(P, pl.dt, pl.rain);
+    StepK k = step_consts(P, pl.dt, pl.rain);
+    k.exact = A.exact;
     const int sp = (int)(step & 1ull);
     float smax_l = 0.0f, infil_l = 0.0f, fix_l = 0.0f;
     bool bad_l = false;
@@ -507,11 +513,6 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       const size_t fx = (size_t)r0 * nxp1, fy = (size_t)r0 * nx;
       const float2 dx0 = make_float2(__ldg(A.dzx + ox0 + fx), __ldg(A.dzx + ox1 + fx));
       const float2 dx1 = CREST ? make_float2(__ldg(A.dzx2 + ox0 + fx), __ldg(A.dzx2 + ox1 + fx)) : f2(0.0f);
-      fW = face2<true, CREST>(left.h, left.u, left.v, left.c, cur.h, cur.u, cur.v, cur.c, dx0, dx1, k);
-      if (lane == 0) {
-        sm.XB[CK(((par * S + s) * W + wis) * 2 + 0, sm.nxb, 7)] = f4(fx_(fW));
-        sm.XB[CK(((par * S + s) * W + wis) * 2 + 1, sm.nxb, 7)] = f4(fy_(fW));
-      }
       // the cells above the strip's first row: ghost, same CTA, or the CTA above
       Cell a0{}, a1{};
       if (top_dom) {
@@ -532,7 +533,12 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       const Cell2 above = cell2_of(a0, a1);
       const float2 dy0 = make_float2(__ldg(A.dzy + oy0 + fy), __ldg(A.dzy + oy1 + fy));
       const float2 dy1 = CREST ? make_float2(__ldg(A.dzy2 + oy0 + fy), __ldg(A.dzy2 + oy1 + fy)) : f2(0.0f);
+      fW = face2<true, CREST>(left.h, left.u, left.v, left.c, cur.h, cur.u, cur.v, cur.c, dx0, dx1, k);
       fN = face2<false, CREST>(above.h, above.u, above.v, above.c, cur.h, cur.u, cur.v, cur.c, dy0, dy1, k);
+      if (lane == 0) {
+        sm.XB[CK(((par * S + s) * W + wis) * 2 + 0, sm.nxb, 7)] = f4(fx_(fW));
+        sm.XB[CK(((par * S + s) * W + wis) * 2 + 1, sm.nxb, 7)] = f4(fy_(fW));
+      }
       if (cell0) sm.BF[CK(s * nx + col0, sm.nbf, 4)] = f4(fx_(fN));
       if (cell1) sm.BF[CK(s * nx + col1, sm.nbf, 4)] = f4(fy_(fN));
       if (top_dom) {   // y_boundary top (kernel.rs:452-472)
@@ -572,70 +578,84 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
         if (cell1 && wis + 1 < W) ey = ff(sm.XB[CK(((par * S + s) * W + wis + 1) * 2 + 1, sm.nxb, 8)]);
         fE = face2_of(ex, ey);
       }
+      // operands of this row's new faces: the next row (and its west neighbours), or for a
+      // strip's last row the next strip's / next CTA's top faces, or the south ghost row
+      Cell2 left{}, below{};
+      Face2 fS_in{};
+      const bool bottom = last && s + 1 >= S && q + 1 >= C;
       if (!last) {
         nxt = load_pair(lr + 1, r + 1);
-        fS = face2<false, CREST>(cur.h, cur.u, cur.v, cur.c, nxt.h, nxt.u, nxt.v, nxt.c, d_s, d_s2, k);
-        const Cell2 left = left_pair(nxt, lr + 1, r + 1);
-        fWn = face2<true, CREST>(left.h, left.u, left.v, left.c, nxt.h, nxt.u, nxt.v, nxt.c, d_xn, d_xn2, k);
-        if (lane == 0) {
-          sm.XB[CK((((par ^ 1) * S + s) * W + wis) * 2 + 0, sm.nxb, 9)] = f4(fx_(fWn));
-          sm.XB[CK((((par ^ 1) * S + s) * W + wis) * 2 + 1, sm.nxb, 9)] = f4(fy_(fWn));
-        }
-      } else {
-        // south faces of a strip's last row: the next strip's top faces (pre-phase), the
-        // next CTA's, or the domain's south edge
+        left = left_pair(nxt, lr + 1, r + 1);
+      } else if (s + 1 < S) {
         FaceF sx{}, sy{};
-        if (s + 1 < S) {
-          if (cell0) sx = ff(sm.BF[CK((s + 1) * nx + col0, sm.nbf, 5)]);
-          if (cell1) sy = ff(sm.BF[CK((s + 1) * nx + col1, sm.nbf, 5)]);
-          fS = face2_of(sx, sy);
-        } else if (q + 1 < C) {
-          const float4* rbf = remote(sm.BF, q + 1);
-          if (cell0) sx = ff(rbf[CK(col0, sm.nbf, 6)]);
-          if (cell1) sy = ff(rbf[CK(col1, sm.nbf, 6)]);
-          fS = face2_of(sx, sy);
-        } else {
-          Cell b0{}, b1{};
-          if (cell0) b0 = ghost_y(cx(cur), A.bc[CK(bc_s + col0, nbc, 18)]);
-          if (cell1) b1 = ghost_y(cy(cur), A.bc[CK(bc_s + col1, nbc, 18)]);
-          const Cell2 below = cell2_of(b0, b1);
-          fS = face2<false, CREST>(cur.h, cur.u, cur.v, cur.c, below.h, below.u, below.v, below.c, d_s, d_s2, k);
-          if (cell0) sm.BY[(sp * 2 + 1) * nx + col0] = fS.m.x;   // y_boundary bottom
-          if (cell1) sm.BY[(sp * 2 + 1) * nx + col1] = fS.m.y;
-        }
+        if (cell0) sx = ff(sm.BF[CK((s + 1) * nx + col0, sm.nbf, 5)]);
+        if (cell1) sy = ff(sm.BF[CK((s + 1) * nx + col1, sm.nbf, 5)]);
+        fS_in = face2_of(sx, sy);
+      } else if (q + 1 < C) {
+        const float4* rbf = remote(sm.BF, q + 1);
+        FaceF sx{}, sy{};
+        if (cell0) sx = ff(rbf[CK(col0, sm.nbf, 6)]);
+        if (cell1) sy = ff(rbf[CK(col1, sm.nbf, 6)]);
+        fS_in = face2_of(sx, sy);
+      } else {
+        Cell b0{}, b1{};
+        if (cell0) b0 = ghost_y(cx(cur), A.bc[CK(bc_s + col0, nbc, 18)]);
+        if (cell1) b1 = ghost_y(cy(cur), A.bc[CK(bc_s + col1, nbc, 18)]);
+        below = cell2_of(b0, b1);
+      }
+      // new faces and the cell update; every lane of the strip computes (lanes past the grid
+      // on zeros or ghost values), so the warp-uniform reciprocal fallback sees all 32 lanes
+      CellNew2 o;
+      float2 uu, vv;
+      if (!last) {
+        fS = face2<false, CREST>(cur.h, cur.u, cur.v, cur.c, nxt.h, nxt.u, nxt.v, nxt.c, d_s, d_s2, k);
+        fWn = face2<true, CREST>(left.h, left.u, left.v, left.c, nxt.h, nxt.u, nxt.v, nxt.c, d_xn, d_xn2, k);
+      } else if (bottom) {
+        fS = face2<false, CREST>(cur.h, cur.u, cur.v, cur.c, below.h, below.u, below.v, below.c, d_s, d_s2, k);
+      } else {
+        fS = fS_in;
+      }
+      o = update_cell2(cur.h, cur.qx, cur.qy, fW, fE, fN, fS, wet_r, gn2_r, k);
+      {
+        const float2 h2 = mul2(o.h, o.h, k.nz);
+        const float2 inv = rcp2f(add2(h2, max2(h2, f2(heps2))), k.exact);
+        const float2 tt = mul2(add2(o.h, o.h), inv, k.nz);
+        uu = mul2(o.qx, tt, k.nz);
+        vv = mul2(o.qy, tt, k.nz);
+      }
+      if (!last && lane == 0) {
+        sm.XB[CK((((par ^ 1) * S + s) * W + wis) * 2 + 0, sm.nxb, 9)] = f4(fx_(fWn));
+        sm.XB[CK((((par ^ 1) * S + s) * W + wis) * 2 + 1, sm.nxb, 9)] = f4(fy_(fWn));
+      }
+      if (bottom) {   // y_boundary bottom (kernel.rs:452-472)
+        if (cell0) sm.BY[(sp * 2 + 1) * nx + col0] = fS.m.x;
+        if (cell1) sm.BY[(sp * 2 + 1) * nx + col1] = fS.m.y;
       }
       // x_boundary (kernel.rs:435-450): mass flux of the west and east domain faces
       if (in_strip && col0 == 0) sm.BX[(sp * 2 + 0) * nr_max + lr] = fW.m.x;
       if (in_strip && col0 == nx) sm.BX[(sp * 2 + 1) * nr_max + lr] = fW.m.x;
       if (in_strip && col1 == nx) sm.BX[(sp * 2 + 1) * nr_max + lr] = fW.m.y;
-      if (cell0 || cell1) {
-        const CellNew2 o = update_cell2(cur.h, cur.qx, cur.qy, fW, fE, fN, fS, wet_r, gn2_r, k);
-        const float2 h2 = mul2(o.h, o.h, k.nz);
-        const float2 inv = rcp2(add2(h2, max2(h2, f2(heps2))));
-        const float2 tt = mul2(add2(o.h, o.h), inv, k.nz);
-        const float2 uu = mul2(o.qx, tt, k.nz), vv = mul2(o.qy, tt, k.nz);
-        if (cell0) {
-          const int li = CK(lr * nx + col0, sm.ncell, 10);
-          sm.S4[li] = make_float4(o.h.x, o.qx.x, o.qy.x, uu.x);
-          sm.S2[li] = make_float2(vv.x, o.c.x);
-          const float pk = sm.PK[li];
-          if (o.h.x > pk) sm.PK[li] = o.h.x;
-          smax_l = rmax(smax_l, o.s.x);
-          bad_l = bad_l || o.bad.x;
-          infil_l += o.infil.x;
-          fix_l += o.fix.x;
-        }
-        if (cell1) {
-          const int li = CK(lr * nx + col1, sm.ncell, 10);
-          sm.S4[li] = make_float4(o.h.y, o.qx.y, o.qy.y, uu.y);
-          sm.S2[li] = make_float2(vv.y, o.c.y);
-          const float pk = sm.PK[li];
-          if (o.h.y > pk) sm.PK[li] = o.h.y;
-          smax_l = rmax(smax_l, o.s.y);
-          bad_l = bad_l || o.bad.y;
-          infil_l += o.infil.y;
-          fix_l += o.fix.y;
-        }
+      if (cell0) {
+        const int li = CK(lr * nx + col0, sm.ncell, 10);
+        sm.S4[li] = make_float4(o.h.x, o.qx.x, o.qy.x, uu.x);
+        sm.S2[li] = make_float2(vv.x, o.c.x);
+        const float pk = sm.PK[li];
+        if (o.h.x > pk) sm.PK[li] = o.h.x;
+        smax_l = rmax(smax_l, o.s.x);
+        bad_l = bad_l || o.bad.x;
+        infil_l += o.infil.x;
+        fix_l += o.fix.x;
+      }
+      if (cell1) {
+        const int li = CK(lr * nx + col1, sm.ncell, 10);
+        sm.S4[li] = make_float4(o.h.y, o.qx.y, o.qy.y, uu.y);
+        sm.S2[li] = make_float2(vv.y, o.c.y);
+        const float pk = sm.PK[li];
+        if (o.h.y > pk) sm.PK[li] = o.h.y;
+        smax_l = rmax(smax_l, o.s.y);
+        bad_l = bad_l || o.bad.y;
+        infil_l += o.infil.y;
+        fix_l += o.fix.y;
       }
       cur = nxt; fN = fS; fW = fWn; par ^= 1;
       if (in_strip) { if (W > 1) named_bar(1 + s, 32 * W); else __syncwarp(); }

@@ -76,6 +76,7 @@ struct itr_ctx {
   // options
   int impl = 0, threads = 0, cluster = 0, graph = 1, steps_per_submit = 64;
   int autotune = 1, autotune_top = 6, probe_steps = 200;
+  int exact_special = 0;
   float tune_ms = 0.0f;
   // device buffers (batched path)
   DevBuf wet, gn2, bc, dzx, dzy, dzx2, dzy2, h0, cut, fill, mon, obj_i, obj_d, peak, depth, ledger, out, mmax;
@@ -403,6 +404,7 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   else if (k == "graph") ctx->graph = value != 0;
   else if (k == "steps_per_submit") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "steps_per_submit must be >= 1"); ctx->steps_per_submit = (int)value; }
   else if (k == "autotune") { ctx->autotune = value != 0; ctx->tuned.clear(); }
+  else if (k == "exact_special") ctx->exact_special = value != 0;
   else if (k == "probe_steps") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "probe_steps must be >= 1"); ctx->probe_steps = (int)value; }
   else return fail(ctx, ITR_INVALID_ARG, "unknown option '%s'", key);
   if (k == "threads" || k == "cluster") ctx->tuned.clear();
@@ -562,6 +564,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.max_rows = max_rows;
     A.out = ctx->out.as<DesignOut>();
     A.max_steps = max_steps;
+    A.exact = ctx->exact_special ? 1u : 0u;
     // launch configuration
     LaunchCfg cfg;
     auto key = std::make_tuple(nx, ny, n, (int)g->mode);

@@ -43,6 +43,7 @@ ITR_DEV float rcbrt(float x) {
 struct StepK {
   float g, g_half, dt, dtdx, dtdy, inv_dx, inv_dy, h_dry, heps2, q_min, rain, cap;
   float nz;   // -0.0f read from the kernel parameters at run time (see mul2)
+  unsigned exact;   // 1: paired reciprocals always through the IEEE routine (checking)
 };
 
 // A face flux tuple: mass, normal momentum seen from the low-index (n_l) and high-index
@@ -319,6 +320,7 @@ ITR_DEV StepK step_consts(const RunParams& P, double dt, double rain) {
   k.rain = (float)rain;
   k.cap = (float)(P.infil * dt);
   k.nz = P.nz;
+  k.exact = 0u;
   return k;
 }
 
@@ -337,6 +339,7 @@ ITR_DEV StepK make_consts(const RunParams& P, double dt, double rain) {
   k.rain = (float)rain;
   k.cap = (float)(P.infil * dt);
   k.nz = P.nz;
+  k.exact = 0u;
   return k;
 }
 
@@ -432,6 +435,32 @@ ITR_DEV B2 and2(B2 a, B2 b) { return B2{a.x && b.x, a.y && b.y}; }
 ITR_DEV B2 or2(B2 a, B2 b) { return B2{a.x || b.x, a.y || b.y}; }
 ITR_DEV float2 sqrt2(float2 a) { return make_float2(sqrt_rn(a.x), sqrt_rn(a.y)); }
 ITR_DEV float2 rcp2(float2 a) { return make_float2(rcp(a.x), rcp(a.y)); }
+ITR_DEV float2 fma2(float2 a, float2 b, float2 c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)), "l"(pk2(c)));
+  return upk2(r);
+}
+
+// ---- Reciprocal without the IEEE routine's per-lane slow-path branch ----
+// 1/x as one Newton step from the hardware estimate (textbook FMA refinement: P. Markstein,
+// IBM J. Res. Dev. 34(1), 1990; J.-M. Muller et al., Handbook of Floating-Point Arithmetic,
+// 2nd ed., 2018, ch. 4): y = est(1/x); e = fma(-x, y, 1); y + y e. Checked against CUDA's
+// IEEE reciprocal on every 32-bit input with |x| in [2^-125, 2^126): identical. An operand
+// outside that range (zero, infinity, NaN, tiny or huge) sends the whole warp through the
+// IEEE routine for that call, as does k.exact; the branch is warp-uniform, so the common
+// path carries no divergence point. Results are the IEEE ones for every input. The step
+// kernel's reciprocals (HLL denominator, friction, velocity) are in range for every
+// healthy state: the fallback is for NaN/infinite states and for checking.
+ITR_DEV float rcp_est(float x) { float r; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+ITR_DEV unsigned rcp_out(float x) { return (((__float_as_uint(x) >> 23) & 0xffu) - 2u) > 250u ? 1u : 0u; }
+
+ITR_DEV float2 rcp2f(float2 x, unsigned exact) {
+  const float2 y = make_float2(rcp_est(x.x), rcp_est(x.y));
+  const float2 e = fma2(neg2(x), y, f2(1.0f));
+  float2 r = fma2(y, e, y);
+  if (__any_sync(0xffffffffu, rcp_out(x.x) | rcp_out(x.y) | exact)) r = rcp2(x);
+  return r;
+}
 ITR_DEV float2 canon2(float2 a) { return make_float2(canon(a.x), canon(a.y)); }
 ITR_DEV float2 abs2(float2 a) { return make_float2(rabs(a.x), rabs(a.y)); }
 
@@ -449,7 +478,8 @@ ITR_DEV float2 rcbrt2(float2 x, float nz) {
 }
 
 // hll (numerics.rs:56-93) on two faces.
-ITR_DEV Face2 hll2(float2 hl, float2 ul, float2 tl, float2 cl, float2 hr, float2 ur, float2 tr, float2 cr, float g_half, float nz) {
+ITR_DEV Face2 hll2(float2 hl, float2 ul, float2 tl, float2 cl, float2 hr, float2 ur, float2 tr, float2 cr, float g_half, float nz,
+                   unsigned exact) {
   const float NZ = nz;
   const B2 dry_l = not2(gt2(hl, 0.0f));
   const B2 dry_r = not2(gt2(hr, 0.0f));
@@ -473,7 +503,7 @@ ITR_DEV Face2 hll2(float2 hl, float2 ul, float2 tl, float2 cl, float2 hr, float2
   const B2 use_r = le2(sr, 0.0f);
   const B2 trivial = or2(or2(both_dry, use_l), use_r);
   const float2 den = sel2(trivial, f2(1.0f), sub2(sr, sl));
-  const float2 inv = rcp2(den);
+  const float2 inv = rcp2f(den, exact);
   const float2 slsr = mul2(sl, sr, NZ);
   const float2 fm_star = mul2(add2(sub2(mul2(sr, ml, NZ), mul2(sl, mr, NZ)), mul2(slsr, sub2(hr, hl), NZ)), inv, NZ);
   const float2 fn_star = mul2(add2(sub2(mul2(sr, pl, NZ), mul2(sl, pr, NZ)), mul2(slsr, sub2(mr, ml), NZ)), inv, NZ);
@@ -508,8 +538,8 @@ ITR_DEV Face2 face2(float2 hl, float2 ul, float2 vl, float2 cl, float2 hr, float
     csl = sel2(pl, sl, cl);
     csr = sel2(pr, sr, cr);
   }
-  if (NORMAL_X) return hll2(hsl, ul, vl, csl, hsr, ur, vr, csr, k.g_half, NZ);
-  return hll2(hsl, vl, ul, csl, hsr, vr, ur, csr, k.g_half, NZ);
+  if (NORMAL_X) return hll2(hsl, ul, vl, csl, hsr, ur, vr, csr, k.g_half, NZ, k.exact);
+  return hll2(hsl, vl, ul, csl, hsr, vr, ur, csr, k.g_half, NZ, k.exact);
 }
 
 struct CellNew2 {
@@ -538,7 +568,7 @@ ITR_DEV CellNew2 update_cell2(float2 h, float2 qx, float2 qy, const Face2& w, co
   const float2 r3 = mul2(mul2(r, r, NZ), r, NZ);
   const float2 r7 = mul2(mul2(r3, r3, NZ), r, NZ);
   const float2 qm = sqrt2(add2(mul2(qx1, qx1, NZ), mul2(qy1, qy1, NZ)));
-  const float2 inv = rcp2(add2(f2(1.0f), mul2(mul2(mul2(f2(k.dt), gn2, NZ), qm, NZ), r7, NZ)));
+  const float2 inv = rcp2f(add2(f2(1.0f), mul2(mul2(mul2(f2(k.dt), gn2, NZ), qm, NZ), r7, NZ)), k.exact);
   const float2 keep = sel2(dry, f2(0.0f), f2(1.0f));
   float2 qx2 = mul2(mul2(qx1, inv, NZ), keep, NZ);
   float2 qy2 = mul2(mul2(qy1, inv, NZ), keep, NZ);

@@ -81,6 +81,26 @@ def test_cluster_shapes_bitwise(gpu, cluster, threads):
         compare_run(runs[i], o, f"cluster={cluster} threads={threads} design {i}")
 
 
+def test_fast_reciprocal_matches_ieee_path(gpu):
+    """The batched kernel's branch-free reciprocal and its IEEE fallback (option
+    exact_special forces the fallback on every call) give the same bits, and both the
+    oracle's."""
+    sc = valley_scene(5.0)   # 90 x 70
+    sc.params.duration_s = 600.0
+    t = [t for _, _, t in sc.designs(2)]
+    runs = {}
+    for exact in (0, 1):
+        gpu.set_option("exact_special", exact)
+        try:
+            runs[exact] = gpu.run_batch(sc.params, t, sc.monitors, want_peak=True)
+        finally:
+            gpu.set_option("exact_special", 0)
+    for i in range(2):
+        o = orc.flat_run(base_arrays(sc.base), design_dict(t[i], sc.params), sc.params, sc.monitors, want_peak=True)
+        compare_run(runs[0][i], o, f"fast reciprocal design {i}")
+        compare_run(runs[1][i], o, f"IEEE reciprocal design {i}")
+
+
 def test_lake_at_rest(gpu):
     # gpu.rs:21-38
     base = synthetic_terrain(64, 48, 1.0, lambda x, y: 0.3 * math.sin(x / 7.0) * math.cos(y / 5.0) + (0.4 if x > 30.0 else 0.0),
