@@ -15,8 +15,10 @@ storm peaking at 100 mm/h at 20 min, 64 designs of 4 primitives each, run to com
            on the host cores, on a bounded sample of the same workload
 
 Multi-GPU (torchrun): designs are sharded across ranks with no data-path collective (weak
-scaling: every rank runs its own 64-design population); a barrier brackets the timed
-region and the max time over ranks is reported.
+scaling: every rank runs 64 designs of the population); a barrier brackets the timed
+region and the max time over ranks is reported. The e2e leg evaluates the whole population
+through itr_gpu.sharding.ShardedBackend, whose one all-gather returns every design's
+results to every rank.
 
 --impl reference: the reference cannot be built here (Rust workspace; no cargo/rustc), so
 its CPU path is timed through the restatement in oracle/ (f32 fused kernel, all host cores).
@@ -255,13 +257,25 @@ def main():
     designs_per_s = sum_over_ranks(len(terrs) * args.steps, world) / (k_total_ms / 1e3)
 
     # ---- e2e: the public C ABI call from host buffers ----
+    # N > 1: the whole population (every rank's designs) goes through ShardedBackend, so
+    # each step also gathers every design's results on every rank (one all-gather).
+    if world > 1:
+        from itr_gpu import GpuBackend
+        from itr_gpu.sharding import ShardedBackend
+        population = []
+        for r in range(world):
+            population += terrs if r == rank else workload(r, args.designs)[1]
+        evaluator = ShardedBackend(GpuBackend(g))
+        step_fn = lambda: evaluator.run(sc.params, population, sc.monitors)  # noqa: E731
+    else:
+        step_fn = lambda: g.run_batch(sc.params, terrs, sc.monitors, want_depth=False)  # noqa: E731
     barrier(world)
     e2e_ms = []
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        runs = g.run_batch(sc.params, terrs, sc.monitors, want_depth=False)
+        step_fn()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     barrier(world)
     e2e_total = max_over_ranks(sum(e2e_ms), world)
