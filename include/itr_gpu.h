@@ -161,11 +161,14 @@ int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int3
                       const itr_objective* obj, itr_result* results);
 
 /* Options (GpuSolver::steps_per_submit, lib.rs:70, is the reference's one knob):
- *   "impl"     0 = batched cluster kernel (default), 1 = plain one-design-per-launch kernel
+ *   "impl"     0 = batched cluster kernel (default; grids too large for 8 CTAs' shared memory
+ *              take the tiled path), 1 = plain one-design-per-launch kernel, 2 = tiled
+ *              batched path: all designs per launch, state in HBM, a CUDA graph per
+ *              steps_per_submit steps
  *   "threads"  threads per CTA of the batched kernel (0 = autotune)
  *   "cluster"  CTAs per design of the batched kernel (0 = autotune)
- *   "graph"    1 = capture the batched launch and its copies in a CUDA graph (default 1)
- *   "steps_per_submit"  plain kernel: steps between host polls (default 64)
+ *   "graph"    tiled path: 1 = replay each block of steps as one CUDA graph (default 1)
+ *   "steps_per_submit"  plain and tiled paths: steps between host polls (default 64)
  *   "exact_special"     1 = the batched kernel computes every reciprocal and square root
  *                       with the IEEE-exact library routines instead of its own branch-free
  *                       ones (identical results; for checking, default 0)

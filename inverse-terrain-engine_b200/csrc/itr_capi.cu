@@ -82,6 +82,8 @@ struct itr_ctx {
   DevBuf wet, gn2, bc, dzx, dzy, dzx2, dzy2, h0, cut, fill, mon, obj_i, obj_d, peak, depth, ledger, out, mmax;
   // plain path scratch
   DevBuf pH, pQX, pQY, pPK, ppart, pctl;
+  // tiled batched path: state planes, tile partials, control blocks of all designs
+  DevBuf tH, tQX, tQY, tpart, tctl;
   HostBuf stage, hout;
   // last run
   double kernel_ms = 0, total_ms = 0;
@@ -94,6 +96,9 @@ struct itr_ctx {
   std::vector<PlainArgs> last_plain;
   std::vector<int> last_plain_blocks;
   bool last_was_plain = false;
+  bool last_was_tiled = false;
+  PlainArgs last_tiled;
+  dim3 last_tgrid;
   // autotune cache: (nx, ny, n_designs, mode) -> cfg
   std::map<std::tuple<int, int, int, int>, LaunchCfg> tuned;
   cudaGraphExec_t gexec = nullptr;
@@ -398,7 +403,7 @@ int itr_gpu_info(itr_ctx* ctx, char* buf, size_t len) {
 int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   if (!ctx || !key) return ITR_INVALID_ARG;
   std::string k(key);
-  if (k == "impl") { if (value < 0 || value > 1) return fail(ctx, ITR_INVALID_ARG, "impl must be 0 or 1"); ctx->impl = (int)value; }
+  if (k == "impl") { if (value < 0 || value > 2) return fail(ctx, ITR_INVALID_ARG, "impl must be 0, 1 or 2"); ctx->impl = (int)value; }
   else if (k == "threads") { if (value < 0 || value > 1024) return fail(ctx, ITR_INVALID_ARG, "threads out of range"); ctx->threads = (int)value; }
   else if (k == "cluster") { if (!(value == 0 || value == 1 || value == 2 || value == 4 || value == 8)) return fail(ctx, ITR_INVALID_ARG, "cluster must be 0,1,2,4,8"); ctx->cluster = (int)value; }
   else if (k == "graph") ctx->graph = value != 0;
@@ -443,6 +448,54 @@ static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid,
     if (guard > 100000000ull) return fail(ctx, ITR_DEVICE_TIMEOUT, "plain run did not terminate");
   }
   return ITR_OK;
+}
+
+// ------------------------------------------------------------------ tiled batch ------
+// All designs per launch: one update (tiles x designs) and one finalize (a warp per design)
+// per step, driven entirely by the control blocks on the device, so a block of
+// steps_per_submit steps is captured once in a CUDA graph and replayed until every design
+// is done (the host reads the control blocks between replays).
+static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* launches) {
+  const int nb = (int)(tgrid.x * tgrid.y);
+  const dim3 grid(tgrid.x, tgrid.y, (unsigned)n);
+  const cudaStream_t st = ctx->stream;
+  k_plain_init<<<n, 1024, 0, st>>>(A);
+  k_plain_finalize<<<n, 32, 0, st>>>(A, nb, 1);
+  *launches += 2;
+  const int K = ctx->steps_per_submit;
+  auto block = [&]() {
+    for (int s = 0; s < K; ++s) {
+      if (A.mode == 1) k_plain_update<true><<<grid, 256, 0, st>>>(A);
+      else k_plain_update<false><<<grid, 256, 0, st>>>(A);
+      k_plain_finalize<<<n, 32, 0, st>>>(A, nb, 0);
+    }
+  };
+  cudaGraphExec_t ge = nullptr;
+  if (ctx->graph) {
+    cudaGraph_t gr = nullptr;
+    CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    block();
+    CU(cudaStreamEndCapture(st, &gr));
+    const cudaError_t e = cudaGraphInstantiate(&ge, gr, 0);
+    cudaGraphDestroy(gr);
+    CU(e);
+  }
+  PlainCtl* hc = ctx->hout.as<PlainCtl>();
+  int rc = ITR_OK;
+  for (uint64_t polls = 0;; ++polls) {
+    if (ge) { const cudaError_t e = cudaGraphLaunch(ge, st); if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "cudaGraphLaunch: %s", cudaGetErrorString(e)); break; } }
+    else block();
+    *launches += 2 * K;
+    cudaError_t e = cudaMemcpyAsync(hc, A.ctl, (size_t)n * sizeof(PlainCtl), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "tiled run: %s", cudaGetErrorString(e)); break; }
+    bool all = true;
+    for (int d = 0; d < n; ++d) all = all && hc[d].done;
+    if (all) break;
+    if (polls > 100000000ull) { rc = fail(ctx, ITR_DEVICE_TIMEOUT, "tiled run did not terminate"); break; }
+  }
+  if (ge) cudaGraphExecDestroy(ge);
+  return rc;
 }
 
 // ------------------------------------------------------------------ run_batch -------
@@ -510,7 +563,8 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   CU(ctx->mmax.ensure((size_t)n * (n_mon > 0 ? n_mon : 1) * 4));
   const size_t out_bytes = (size_t)n * sizeof(DesignOut) + (size_t)n * (n_mon > 0 ? n_mon : 1) * 4 +
                            (size_t)n * (max_rows > 0 ? max_rows : 1) * 64 + 2 * n * N * 4 + 1024;
-  CU(ctx->hout.ensure(out_bytes > sizeof(PlainCtl) ? out_bytes : sizeof(PlainCtl)));
+  const size_t ctl_bytes = (size_t)n * sizeof(PlainCtl);
+  CU(ctx->hout.ensure(out_bytes > ctl_bytes ? out_bytes : ctl_bytes));
 
   RunParams P = make_run_params(p, g);
   DevObjective DO;
@@ -541,6 +595,8 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   int launches = 0;
   const unsigned long long max_steps = 2000000000ull;
 
+  // impl 2, or a grid no cluster shape can hold: the tiled batched path (state in HBM)
+  bool tiled = ctx->impl == 2;
   if (ctx->impl == 0) {
     BatchArgs A;
     memset(&A, 0, sizeof(A));
@@ -575,27 +631,72 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
       cfg = ctx->tuned[key];
     } else {
       std::vector<LaunchCfg> cands = candidates(ctx, nx, ny, n, crest);
-      if (cands.empty()) return fail(ctx, ITR_UNSUPPORTED, "a %dx%d grid does not fit the batched kernel's shared memory (max 8 CTAs per design)", nx, ny);
-      // Measured autotuning: time a short probe (the first steps of this very batch) of the
-      // best few shapes by the model and keep the fastest for this (grid, population) key.
-      cfg = cands[0];
-      if (ctx->autotune && cands.size() > 1) {
-        rc = autotune(ctx, A, cands, n, &cfg);
-        if (rc != ITR_OK) return rc;
+      if (cands.empty()) {
+        tiled = true;   // a design needs more shared memory than 8 CTAs hold
+      } else {
+        // Measured autotuning: time a short probe (the first steps of this very batch) of
+        // the best few shapes by the model and keep the fastest for this (grid, population).
+        cfg = cands[0];
+        if (ctx->autotune && cands.size() > 1) {
+          rc = autotune(ctx, A, cands, n, &cfg);
+          if (rc != ITR_OK) return rc;
+        }
+        ctx->tuned[key] = cfg;
       }
-      ctx->tuned[key] = cfg;
     }
-    A.C = cfg.C; A.W = cfg.W; A.S = cfg.S;
+    if (!tiled) {
+      A.C = cfg.C; A.W = cfg.W; A.S = cfg.S;
+      CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+      rc = launch_batched(ctx, A, cfg, n);
+      if (rc != ITR_OK) return rc;
+      CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+      launches += 1;
+      ctx->last_args = A;
+      ctx->last_cfg = cfg;
+      ctx->have_last = true;
+      ctx->last_was_plain = false;
+      ctx->last_was_tiled = false;
+    }
+  }
+  if (tiled) {
+    const dim3 tgrid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile);
+    const int nb = (int)(tgrid.x * tgrid.y);
+    CU(ctx->tH.ensure((size_t)n * 2 * N * 4)); CU(ctx->tQX.ensure((size_t)n * 2 * N * 4)); CU(ctx->tQY.ensure((size_t)n * 2 * N * 4));
+    CU(ctx->tpart.ensure((size_t)n * nb * 5 * 8));
+    CU(ctx->tctl.ensure((size_t)n * sizeof(PlainCtl)));
+    PlainArgs A;
+    memset(&A, 0, sizeof(A));
+    A.P = P; A.nx = nx; A.ny = ny; A.mode = g->mode; A.n_designs = n;
+    A.wet = reinterpret_cast<const float*>(dv + o_wet);
+    A.gn2 = reinterpret_cast<const float*>(dv + o_gn2);
+    A.bc = reinterpret_cast<const uint8_t*>(dv + o_bc);
+    A.dzx = reinterpret_cast<const float*>(dv + o_dzx);
+    A.dzy = reinterpret_cast<const float*>(dv + o_dzy);
+    A.dzx2 = crest ? reinterpret_cast<const float*>(dv + o_dzx2) : nullptr;
+    A.dzy2 = crest ? reinterpret_cast<const float*>(dv + o_dzy2) : nullptr;
+    A.h0 = reinterpret_cast<const float*>(dv + o_h0);
+    A.cut_d = reinterpret_cast<const double*>(dv + o_cut);
+    A.fill_d = reinterpret_cast<const double*>(dv + o_fill);
+    A.n_mon = n_mon; A.mon_cells = reinterpret_cast<const unsigned*>(dv + o_mon);
+    A.obj = DO;
+    A.H = ctx->tH.as<float>(); A.QX = ctx->tQX.as<float>(); A.QY = ctx->tQY.as<float>();
+    A.PK = ctx->peak.as<float>();
+    A.part = ctx->tpart.as<double>(); A.ctl = ctx->tctl.as<PlainCtl>();
+    A.ledger = max_rows > 0 ? ctx->ledger.as<double>() : nullptr;
+    A.max_rows = max_rows;
+    A.max_steps = max_steps;
     CU(cudaEventRecord(ctx->ev[1], ctx->stream));
-    rc = launch_batched(ctx, A, cfg, n);
+    rc = run_tiled_batch(ctx, A, n, tgrid, &launches);
     if (rc != ITR_OK) return rc;
-    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+    k_plain_outputs<<<n, 256, 0, ctx->stream>>>(A, nb, ctx->out.as<DesignOut>(), ctx->depth.as<float>());
     launches += 1;
-    ctx->last_args = A;
-    ctx->last_cfg = cfg;
+    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+    ctx->last_tiled = A;
+    ctx->last_tgrid = tgrid;
     ctx->have_last = true;
     ctx->last_was_plain = false;
-  } else {
+    ctx->last_was_tiled = true;
+  } else if (ctx->impl == 1) {
     // plain: one design after another
     CU(ctx->pH.ensure(2 * N * 4)); CU(ctx->pQX.ensure(2 * N * 4)); CU(ctx->pQY.ensure(2 * N * 4));
     CU(ctx->pPK.ensure(N * 4));
@@ -644,6 +745,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     }
     CU(cudaEventRecord(ctx->ev[2], ctx->stream));
     ctx->last_was_plain = true;
+    ctx->last_was_tiled = false;
     ctx->have_last = true;
   }
   CU(cudaGetLastError());
@@ -727,7 +829,11 @@ extern "C" int itr_gpu_rerun_resident(itr_ctx* ctx) {
   CU(cudaSetDevice(ctx->device));
   int launches = 0;
   CU(cudaEventRecord(ctx->ev[1], ctx->stream));
-  if (!ctx->last_was_plain) {
+  if (ctx->last_was_tiled) {
+    PlainArgs A = ctx->last_tiled;
+    int rc = run_tiled_batch(ctx, A, A.n_designs, ctx->last_tgrid, &launches);
+    if (rc != ITR_OK) return rc;
+  } else if (!ctx->last_was_plain) {
     int rc = launch_batched(ctx, ctx->last_args, ctx->last_cfg, ctx->last_args.n_designs);
     if (rc != ITR_OK) return rc;
     launches = 1;

@@ -1,13 +1,17 @@
-// itr_plain.cuh — the plain forward: one design per launch sequence, global-memory ping-pong.
+// itr_plain.cuh — tiled forward with the state in HBM (global-memory ping-pong).
 //
 // This is the straightforward CUDA form of the reference's GPU backend structure
 // (crates/itr-gpu/src/shader.wgsl:135-365, lib.rs:302-328): per step one tiled `update`
 // kernel (16x16 cells, 18x18 halo in shared memory, faces computed once per tile) and one
 // single-warp `finalize` kernel that advances the f64 integrator on the device; the host
-// polls a control word every `steps_per_submit` steps. Designs run one after another.
-// It is the baseline the batched kernel is measured against, and it uses the same
-// per-cell arithmetic (itr_device.cuh), so its results are bit-identical to the batched
-// kernel's and to the f32 CPU oracle's.
+// polls a control word every `steps_per_submit` steps.
+// Launched with one design (gridDim.z = 1, designs one after another) it is the plain
+// forward, the baseline the batched cluster kernel is measured against. Launched with all
+// designs at once (design = blockIdx.z of the update, blockIdx.x of finalize/init) it is the
+// tiled batched forward for grids too large for a cluster's shared memory, and the forward
+// recomputation of the adjoint (optional argmax-of-peak and dt/rain logs). Per-cell
+// arithmetic is itr_device.cuh's, so results are bit-identical to the cluster kernel's and
+// to the f32 CPU oracle's.
 #pragma once
 #include "itr_device.cuh"
 
@@ -37,35 +41,71 @@ struct PlainArgs {
   const float* wet;
   const float* gn2;
   const uint8_t* bc;
-  const float* dzx;   // this design
-  const float* dzy;
+  const float* dzx;   // design 0; design d at + d * ny * (nx + 1)
+  const float* dzy;   //                         + d * (ny + 1) * nx
   const float* dzx2;
   const float* dzy2;
-  const float* h0;    // this design
-  double cut, fill;
+  const float* h0;    // + d * nx * ny
+  double cut, fill;   // one design, or per design in cut_d / fill_d when those are set
+  const double* cut_d;
+  const double* fill_d;
+  int n_designs;
   int n_mon;
   const unsigned* mon_cells;
   DevObjective obj;
-  float* H;           // [2][nx*ny]
+  float* H;           // per design [2][nx*ny]
   float* QX;
   float* QY;
-  float* PK;          // nx*ny
-  double* part;       // per block: [5] (infil, fix, in, out, vol)
-  PlainCtl* ctl;
-  double* ledger;     // max_rows*8
+  float* PK;          // per design nx*ny
+  double* part;       // per design, per tile: [5] (infil, fix, in, out, vol)
+  PlainCtl* ctl;      // per design
+  double* ledger;     // per design max_rows*8
   int max_rows;
   unsigned long long max_steps;
+  unsigned* tpk;      // optional, per design nx*ny: index of the state that last raised PK
+  double* dt_log;     // optional, per design max_log x (dt, rain) of every step
+  int max_log;
 };
 
+// Pointers of design d inside a launch over n_designs designs.
+struct PlainDesign {
+  const float *dzx, *dzy, *dzx2, *dzy2, *h0;
+  float *H, *QX, *QY, *PK;
+  double* part;
+  PlainCtl* ctl;
+  double* ledger;
+  unsigned* tpk;
+  double* dt_log;
+  double cut, fill;
+};
+
+ITR_DEV PlainDesign plain_design(const PlainArgs& A, int d, int n_tiles) {
+  const size_t N = (size_t)A.nx * A.ny, SX = (size_t)A.ny * (A.nx + 1), SY = (size_t)(A.ny + 1) * A.nx;
+  PlainDesign v;
+  v.dzx = A.dzx + d * SX; v.dzy = A.dzy + d * SY;
+  v.dzx2 = A.dzx2 ? A.dzx2 + d * SX : nullptr; v.dzy2 = A.dzy2 ? A.dzy2 + d * SY : nullptr;
+  v.h0 = A.h0 + d * N;
+  v.H = A.H + d * 2 * N; v.QX = A.QX + d * 2 * N; v.QY = A.QY + d * 2 * N;
+  v.PK = A.PK + d * N;
+  v.part = A.part + (size_t)d * n_tiles * 5;
+  v.ctl = A.ctl + d;
+  v.ledger = A.ledger ? A.ledger + (size_t)d * A.max_rows * 8 : nullptr;
+  v.tpk = A.tpk ? A.tpk + d * N : nullptr;
+  v.dt_log = A.dt_log ? A.dt_log + (size_t)d * A.max_log * 2 : nullptr;
+  v.cut = A.cut_d ? A.cut_d[d] : A.cut;
+  v.fill = A.fill_d ? A.fill_d[d] : A.fill;
+  return v;
+}
+
 // Old state of padded cell (gx, gy) with ghost cells outside (boundary.rs:36-87).
-ITR_DEV void plain_load(const PlainArgs& A, int par, int gx, int gy, float& h, float& qx, float& qy) {
+ITR_DEV void plain_load(const PlainArgs& A, const PlainDesign& D, int par, int gx, int gy, float& h, float& qx, float& qy) {
   const int nx = A.nx, ny = A.ny;
   const bool ox = gx < 0 || gx >= nx, oy = gy < 0 || gy >= ny;
   if (ox && oy) { h = 0.0f; qx = 0.0f; qy = 0.0f; return; }
   int sx = gx < 0 ? 0 : (gx >= nx ? nx - 1 : gx);
   int sy = gy < 0 ? 0 : (gy >= ny ? ny - 1 : gy);
   size_t i = (size_t)par * nx * ny + (size_t)sy * nx + sx;
-  h = A.H[i]; qx = A.QX[i]; qy = A.QY[i];
+  h = D.H[i]; qx = D.QX[i]; qy = D.QY[i];
   if (ox) { int code = gx < 0 ? A.bc[2 * nx + sy] : A.bc[2 * nx + ny + sy]; if (code == 0) qx = -qx; }
   else if (oy) { int code = gy < 0 ? A.bc[sx] : A.bc[nx + sx]; if (code == 0) qy = -qy; }
 }
@@ -77,7 +117,8 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
   __shared__ float wmax[8];
   __shared__ unsigned wbad[8];
   __shared__ double wsum[8][5];
-  const PlainCtl& cl = *A.ctl;
+  const PlainDesign D = plain_design(A, blockIdx.z, gridDim.x * gridDim.y);
+  const PlainCtl& cl = *D.ctl;
   if (cl.done) return;
   const int par = cl.par;
   const StepK k = cl.k;
@@ -89,7 +130,7 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
   for (int e = li; e < 324; e += 256) {
     int hx = e % 18, hy = e / 18;
     float h, qx, qy;
-    plain_load(A, par, gx0 - 1 + hx, gy0 - 1 + hy, h, qx, qy);
+    plain_load(A, D, par, gx0 - 1 + hx, gy0 - 1 + hy, h, qx, qy);
     float u, v, c;
     cell_vel(h, qx, qy, k.g, k.heps2, u, v, c);
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
@@ -102,7 +143,7 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
       if (row < ny && f <= nx) {
         int a = (fyr + 1) * 18 + fxc;
         size_t o = (size_t)row * (nx + 1) + f;
-        float d0 = A.dzx[o], d1 = CREST ? A.dzx2[o] : 0.0f;
+        float d0 = D.dzx[o], d1 = CREST ? D.dzx2[o] : 0.0f;
         fx[e] = face<true, CREST>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], d0, d1, k);
       }
     }
@@ -112,7 +153,7 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
       if (c < nx && f <= ny) {
         int a = fyr * 18 + fxc + 1, b = a + 18;
         size_t o = (size_t)f * nx + c;
-        float d0 = A.dzy[o], d1 = CREST ? A.dzy2[o] : 0.0f;
+        float d0 = D.dzy[o], d1 = CREST ? D.dzy2[o] : 0.0f;
         fy[e] = face<false, CREST>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], d0, d1, k);
       }
     }
@@ -130,8 +171,11 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
     const size_t gi = (size_t)gy * nx + gx;
     CellNew o = update_cell(sh[a], sqx[a], sqy[a], w, e, n, s, A.wet[gi], A.gn2[gi], k);
     const size_t wo = (size_t)(par ^ 1) * nx * ny + gi;
-    A.H[wo] = o.h; A.QX[wo] = o.qx; A.QY[wo] = o.qy;
-    if (o.h > A.PK[gi]) A.PK[gi] = o.h;
+    D.H[wo] = o.h; D.QX[wo] = o.qx; D.QY[wo] = o.qy;
+    if (o.h > D.PK[gi]) {
+      D.PK[gi] = o.h;
+      if (D.tpk) D.tpk[gi] = (unsigned)(cl.step + 1);   // this step makes state step+1
+    }
     smax = o.s;
     bad = o.bad;
     acc[0] = (double)o.infil; acc[1] = (double)o.fix;
@@ -154,16 +198,17 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
   if (li == 0) {
     float mm = 0.0f; unsigned bb = 0u; double ss[5] = {0, 0, 0, 0, 0};
     for (int w = 0; w < 8; ++w) { mm = rmax(mm, wmax[w]); bb |= wbad[w]; for (int j = 0; j < 5; ++j) ss[j] += wsum[w][j]; }
-    if (mm > 0.0f) atomicMax(&A.ctl->smax_bits, __float_as_uint(mm));
-    if (bb) atomicOr(&A.ctl->bad, 1u);
-    double* p = A.part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 5;
+    if (mm > 0.0f) atomicMax(&D.ctl->smax_bits, __float_as_uint(mm));
+    if (bb) atomicOr(&D.ctl->bad, 1u);
+    double* p = D.part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 5;
     for (int j = 0; j < 5; ++j) p[j] = ss[j];
   }
 }
 
 // Advance the integrator after a step (or plan the first step when `first`).
 __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
-  PlainCtl& c = *A.ctl;
+  const PlainDesign D = plain_design(A, blockIdx.x, n_blocks);
+  PlainCtl& c = *D.ctl;
   const int lane = threadIdx.x;
   const RunParams& P = A.P;
   if (c.done) return;
@@ -171,7 +216,7 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
     // sum block partials in block order
     double tot[5] = {0, 0, 0, 0, 0};
     for (int b = lane; b < n_blocks; b += 32)
-      for (int j = 0; j < 5; ++j) tot[j] += A.part[(size_t)b * 5 + j];
+      for (int j = 0; j < 5; ++j) tot[j] += D.part[(size_t)b * 5 + j];
     for (int j = 0; j < 5; ++j)
       for (int o = 16; o > 0; o >>= 1) tot[j] += __shfl_xor_sync(0xffffffffu, tot[j], o);
     const double smax = (double)__uint_as_float(c.smax_bits);
@@ -198,8 +243,8 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
         c.volume = v;
         const double gross = c.v0 + c.acc_rain + c.tot_in;
         c.rel_res = fabs(v - expected) / (gross > 1e-300 ? gross : 1e-300);
-        if (c.n_rows < A.max_rows && A.ledger) {
-          double* o = A.ledger + (size_t)c.n_rows * 8;
+        if (c.n_rows < A.max_rows && D.ledger) {
+          double* o = D.ledger + (size_t)c.n_rows * 8;
           o[0] = c.t; o[1] = v; o[2] = c.acc_rain; o[3] = c.tot_in; o[4] = c.tot_out; o[5] = infil; o[6] = fix; o[7] = v - expected;
         }
         c.n_rows += 1;
@@ -209,7 +254,7 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
             double best = 0.0; int bk = -1;
             for (int g = 0; g < ob.n_guard; ++g) {
               int mp = ob.guard_pos[g];
-              double w = (double)A.PK[A.mon_cells[mp]] - ob.baseline[mp] - ob.tol;
+              double w = (double)D.PK[A.mon_cells[mp]] - ob.baseline[mp] - ob.tol;
               if (w > 0.0 && (bk < 0 || w > best)) { best = w; bk = g; }
             }
             if (bk >= 0) {
@@ -222,12 +267,12 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
             for (int a = 0; a < ob.n_assets; ++a) {
               double pk = 0.0;
               for (int m = ob.asset_off[a]; m < ob.asset_off[a + 1]; ++m) {
-                double x = (double)A.PK[A.mon_cells[ob.asset_pos[m]]];
+                double x = (double)D.PK[A.mon_cells[ob.asset_pos[m]]];
                 pk = pk > x ? pk : x;
               }
               jr += ob.asset_w[a] * ob.tau * itr_math::softplus((pk - ob.asset_thr[a]) / ob.tau);
             }
-            const double lb = jr + ob.earth_w * (ob.cut_cost * A.cut + ob.fill_cost * A.fill);
+            const double lb = jr + ob.earth_w * (ob.cut_cost * D.cut + ob.fill_cost * D.fill);
             if (lb >= ob.incumbent) { decision = 2; c.lower_bound = lb; }
           }
         }
@@ -241,19 +286,22 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
     if (!(c.t < P.duration && c.sync_index < P.n_sync)) { c.done = 1; return; }
     if (c.step >= A.max_steps) { c.status = 4; c.done = 1; return; }
     c.pl = plan_step(P, c.t, c.sync_index, c.dt_cfl);
+    if (D.dt_log && c.step < (unsigned long long)A.max_log) { D.dt_log[2 * c.step] = c.pl.dt; D.dt_log[2 * c.step + 1] = c.pl.rain; }
     c.k = step_consts(P, c.pl.dt, c.pl.rain);
   }
 }
 
 // Initial state and the first dt (solver.rs:381-390).
 __global__ void k_plain_init(const PlainArgs A) {
+  const PlainDesign D = plain_design(A, blockIdx.x, 0);
   const int nx = A.nx, ny = A.ny, n = nx * ny;
   const RunParams& P = A.P;
   __shared__ double ss[32], sv[32];
   double s0 = 0.0, v0 = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    float h = A.h0[i];
-    A.H[i] = h; A.QX[i] = 0.0f; A.QY[i] = 0.0f; A.PK[i] = 0.0f;
+    float h = D.h0[i];
+    D.H[i] = h; D.QX[i] = 0.0f; D.QY[i] = 0.0f; D.PK[i] = 0.0f;
+    if (D.tpk) D.tpk[i] = 0u;
     double hd = (double)h;
     v0 += hd;
     if (hd > P.h_dry) {
@@ -275,7 +323,25 @@ __global__ void k_plain_init(const PlainArgs A) {
     memset(&c, 0, sizeof(c));
     c.v0 = v * P.area; c.volume = c.v0;
     c.dt_cfl = s > 0.0 ? dmin_num(P.cfl / s, P.dt_max) : P.dt_max;
-    *A.ctl = c;
+    *D.ctl = c;
+  }
+}
+
+// Per-design results of a tiled batched run: the scalar outcome from the control block and
+// the final depth (the plane the last step wrote).
+__global__ void k_plain_outputs(const PlainArgs A, int n_tiles, DesignOut* out, float* depth) {
+  const PlainDesign D = plain_design(A, blockIdx.x, n_tiles);
+  const PlainCtl& c = *D.ctl;
+  const size_t N = (size_t)A.nx * A.ny;
+  const float* H = D.H + (size_t)c.par * N;
+  for (size_t i = threadIdx.x; i < N; i += blockDim.x) depth[blockIdx.x * N + i] = H[i];
+  if (threadIdx.x == 0) {
+    DesignOut o;
+    memset(&o, 0, sizeof(o));
+    o.steps = c.step; o.t_end = c.t; o.sync_count = c.sync_index; o.status = c.status;
+    o.breach_cell = c.breach_cell; o.breach_sync = c.breach_sync; o.violation = c.violation;
+    o.lower_bound = c.lower_bound; o.v0 = c.v0; o.volume = c.volume; o.rel_residual = c.rel_res; o.n_rows = c.n_rows;
+    out[blockIdx.x] = o;
   }
 }
 

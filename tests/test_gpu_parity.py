@@ -49,12 +49,15 @@ def compare_run(g_run, o_run, what):
     np.testing.assert_array_equal(g_run.monitor_max, o_run["monitor_max"], err_msg=f"{what}: monitor maxima")
 
 
-@pytest.mark.parametrize("impl", ["batched", "plain"])
+IMPL = {"batched": 0, "plain": 1, "tiled": 2}
+
+
+@pytest.mark.parametrize("impl", ["batched", "plain", "tiled"])
 def test_valley_designs_bitwise_vs_oracle(gpu, impl):
     sc = small_valley()
     designs = sc.designs(3)
     terrs = [t for _, _, t in designs]
-    gpu.set_option("impl", 0 if impl == "batched" else 1)
+    gpu.set_option("impl", IMPL[impl])
     try:
         runs = gpu.run_batch(sc.params, terrs, sc.monitors, want_peak=True)
     finally:
@@ -99,6 +102,20 @@ def test_fast_reciprocal_matches_ieee_path(gpu):
         o = orc.flat_run(base_arrays(sc.base), design_dict(t[i], sc.params), sc.params, sc.monitors, want_peak=True)
         compare_run(runs[0][i], o, f"fast reciprocal design {i}")
         compare_run(runs[1][i], o, f"IEEE reciprocal design {i}")
+
+
+def test_large_grid_takes_tiled_path(gpu):
+    """A design too large for 8 CTAs' shared memory (400 x 300 cells, 3.4 MB of state) runs
+    on the tiled batched path, bit for bit with the oracle."""
+    base = synthetic_terrain(400, 300, 2.0, lambda x, y: 3.0 - 0.004 * x + 0.3 * math.sin(y / 40.0), n=0.035,
+                             segments=[Segment("transmissive", "east")])
+    p = SolverParams(90.0, 30.0, rain=Hyetograph.from_mm_h([(0, 0), (30, 200), (90, 0)]))
+    mon = MonitorSet(np.arange(0, 400 * 300, 997))
+    t = [PreparedTerrain(base), PreparedTerrain(base)]
+    runs = gpu.run_batch(p, t, mon, want_peak=True)
+    o = orc.flat_run(base_arrays(base), design_dict(t[0]), p, mon, want_peak=True)
+    for i in range(2):
+        compare_run(runs[i], o, f"large grid design {i}")
 
 
 def test_lake_at_rest(gpu):
@@ -183,7 +200,8 @@ def test_unsupported_inputs_rejected(gpu):
         gpu.run_batch(p, [PreparedTerrain(base)], MonitorSet())
 
 
-def test_crest_mode_level2_bitwise(gpu):
+@pytest.mark.parametrize("impl", ["batched", "tiled"])
+def test_crest_mode_level2_bitwise(gpu, impl):
     # coarse fidelity level (FaceMode::Crest, terrain.rs:12-18), which the reference GPU path rejects
     sc = valley_scene(5.0)
     from itr_gpu.terrain import TerrainBase
@@ -192,12 +210,24 @@ def test_crest_mode_level2_bitwise(gpu):
     p.duration_s = 600.0
     t = PreparedTerrain(base2)
     mon = MonitorSet(np.arange(0, base2.nx * base2.ny, 7))
-    r = gpu.run_batch(p, [t], mon, want_peak=True)[0]
+    gpu.set_option("impl", IMPL[impl])
+    try:
+        r = gpu.run_batch(p, [t], mon, want_peak=True)[0]
+    finally:
+        gpu.set_option("impl", 0)
     o = orc.flat_run(base_arrays(base2), design_dict(t), p, mon, want_peak=True)
-    compare_run(r, o, "crest level 2")
+    compare_run(r, o, f"crest level 2 ({impl})")
 
 
-def test_guard_and_incumbent_aborts_identical(gpu):
+@pytest.fixture(params=["batched", "tiled"])
+def impl_gpu(gpu, request):
+    gpu.set_option("impl", IMPL[request.param])
+    yield gpu
+    gpu.set_option("impl", 0)
+
+
+def test_guard_and_incumbent_aborts_identical(impl_gpu):
+    gpu = impl_gpu
     sc = small_valley(1200.0)
     designs = sc.designs(6)
     terrs = [t for _, _, t in designs]
