@@ -185,6 +185,25 @@ int itr_gpu_last_timing(itr_ctx* ctx, double* kernel_ms, double* total_ms, uint6
  * results kept on the device; for timing the kernel over resident inputs. */
 int itr_gpu_rerun_resident(itr_ctx* ctx);
 
+/* Vector-Jacobian product of the forward (the north star's adjoint; the reference has none,
+ * its optimisers are derivative-free, crates/itr-opt/src/cmaes.rs). For every design it gives
+ * dJ/d(face jump) of the asset term J = sum_k w_k tau softplus((P_k - eta_k) / tau)
+ * (objective.rs:95-128; the earthwork term does not depend on the jumps):
+ *   dj_ddzx  n_designs * ny * (nx+1), same layout as itr_design.dzx
+ *   dj_ddzy  n_designs * (ny+1) * nx, same layout as itr_design.dzy
+ * The forward runs to completion on the tiled path (aborts off), keeping the state every
+ * checkpoint_interval steps; the backward recomputes each segment and steps the discrete
+ * adjoint back through it with the recorded dt sequence held fixed. results are the
+ * forward's, as itr_gpu_run_batch gives them. Signed face mode only (ITR_UNSUPPORTED
+ * otherwise); obj must have at least one asset. Device memory: checkpoints of 12 B per cell
+ * per design per interval, a tape of checkpoint_interval states. */
+int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n_designs, const itr_design* designs,
+                const uint32_t* monitors, int32_t n_mon, const itr_objective* obj, int32_t checkpoint_interval,
+                itr_result* results, double* dj_ddzx, double* dj_ddzy);
+
+/* Device time of the last itr_gpu_vjp: taped forward (kernels and checkpoints) and backward. */
+int itr_gpu_last_vjp_timing(itr_ctx* ctx, double* forward_ms, double* backward_ms);
+
 /* ---- Allocation-free plain forward. No reference counterpart. ----
  * For callers that cannot allocate device memory when they run a design: a process that
  * has committed the whole device to its own pool, a caller whose other streams must not be

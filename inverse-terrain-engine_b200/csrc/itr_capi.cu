@@ -20,6 +20,7 @@
 #include "itr_device.cuh"
 #include "itr_batched.cuh"
 #include "itr_plain.cuh"
+#include "itr_adjoint.cuh"
 
 using namespace itr;
 
@@ -84,6 +85,12 @@ struct itr_ctx {
   DevBuf pH, pQX, pQY, pPK, ppart, pctl;
   // tiled batched path: state planes, tile partials, control blocks of all designs
   DevBuf tH, tQX, tQY, tpart, tctl;
+  // adjoint: argmax states, (dt, rain) ring, checkpoints, tape, adjoint state, gradients
+  DevBuf aTpk, aRing, aTape, aLA, aLB, aGx, aGy, aSeg, aNst, aSeedC, aSeedS, aSeedW, aSeedN, aTmon;
+  HostBuf aRingH;
+  std::vector<DevBuf> aCkpt;
+  struct Vjp* vjp = nullptr;
+  double vjp_fwd_ms = 0, vjp_bwd_ms = 0;
   HostBuf stage, hout;
   // last run
   double kernel_ms = 0, total_ms = 0;
@@ -379,8 +386,12 @@ void itr_gpu_destroy(itr_ctx* ctx) {
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   for (DevBuf* b : {&ctx->wet, &ctx->gn2, &ctx->bc, &ctx->dzx, &ctx->dzy, &ctx->dzx2, &ctx->dzy2, &ctx->h0, &ctx->cut, &ctx->fill,
                     &ctx->mon, &ctx->obj_i, &ctx->obj_d, &ctx->peak, &ctx->depth, &ctx->ledger, &ctx->out, &ctx->mmax,
-                    &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl})
+                    &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
+                    &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy,
+                    &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon})
     b->release();
+  for (DevBuf& b : ctx->aCkpt) b.release();
+  ctx->aRingH.release();
   ctx->stage.release();
   ctx->hout.release();
   for (int i = 0; i < 4; ++i) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -455,14 +466,26 @@ static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid,
 // per step, driven entirely by the control blocks on the device, so a block of
 // steps_per_submit steps is captured once in a CUDA graph and replayed until every design
 // is done (the host reads the control blocks between replays).
+// Adjoint request: while set, run_batch takes the tiled path and records a tape.
+struct Vjp {
+  int K;                                  // checkpoint interval (steps)
+  std::vector<std::vector<double>> dt;    // per design: (dt, rain) of every step taken
+  uint64_t blocks = 0;                    // checkpoints written (one per block of K steps)
+  double* gx;                             // host outputs
+  double* gy;
+};
+
 static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* launches) {
   const int nb = (int)(tgrid.x * tgrid.y);
   const dim3 grid(tgrid.x, tgrid.y, (unsigned)n);
   const cudaStream_t st = ctx->stream;
+  Vjp* tape = ctx->vjp;
+  const size_t N = (size_t)A.nx * A.ny;
   k_plain_init<<<n, 1024, 0, st>>>(A);
   k_plain_finalize<<<n, 32, 0, st>>>(A, nb, 1);
   *launches += 2;
-  const int K = ctx->steps_per_submit;
+  const int K = tape ? tape->K : ctx->steps_per_submit;
+  if (tape) { tape->dt.assign(n, std::vector<double>()); tape->blocks = 0; }
   auto block = [&]() {
     for (int s = 0; s < K; ++s) {
       if (A.mode == 1) k_plain_update<true><<<grid, 256, 0, st>>>(A);
@@ -483,12 +506,32 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
   PlainCtl* hc = ctx->hout.as<PlainCtl>();
   int rc = ITR_OK;
   for (uint64_t polls = 0;; ++polls) {
+    if (tape) {   // checkpoint: the state at the start of this block
+      if (ctx->aCkpt.size() <= polls) ctx->aCkpt.emplace_back();
+      cudaError_t e = ctx->aCkpt[polls].ensure((size_t)n * 3 * N * 4);
+      if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "checkpoint %llu: %s", (unsigned long long)polls, cudaGetErrorString(e)); break; }
+      k_adj_ckpt<<<dim3(64, (unsigned)n), 256, 0, st>>>(A, ctx->aCkpt[polls].as<float>());
+      *launches += 1;
+      tape->blocks = polls + 1;
+    }
     if (ge) { const cudaError_t e = cudaGraphLaunch(ge, st); if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "cudaGraphLaunch: %s", cudaGetErrorString(e)); break; } }
     else block();
     *launches += 2 * K;
     cudaError_t e = cudaMemcpyAsync(hc, A.ctl, (size_t)n * sizeof(PlainCtl), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "tiled run: %s", cudaGetErrorString(e)); break; }
+    if (tape) {   // (dt, rain) of this block's steps, from the ring of 2K slots
+      double* ring = ctx->aRingH.as<double>();
+      e = cudaMemcpy(ring, A.dt_log, (size_t)n * 2 * K * 2 * 8, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "tape: %s", cudaGetErrorString(e)); break; }
+      const uint64_t s0 = polls * (uint64_t)K;
+      for (int d = 0; d < n; ++d)
+        for (uint64_t s = s0; s < s0 + K && s < hc[d].step; ++s) {
+          const double* q = ring + ((size_t)d * 2 * K + (size_t)(s % (2 * K))) * 2;
+          tape->dt[d].push_back(q[0]);
+          tape->dt[d].push_back(q[1]);
+        }
+    }
     bool all = true;
     for (int d = 0; d < n; ++d) all = all && hc[d].done;
     if (all) break;
@@ -496,6 +539,107 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
   }
   if (ge) cudaGraphExecDestroy(ge);
   return rc;
+}
+
+// ------------------------------------------------------------------ adjoint ----------
+// Backward sweep after a taped tiled forward (itr_adjoint.cuh): seeds from the monitor
+// maxima and their argmax states, then segment by segment (last first) replay K steps from
+// the checkpoint and step the adjoint back through them.
+static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* ob, int n, const uint32_t* mon, int n_mon,
+                        const float* hmm, const DesignOut* hdo) {
+  Vjp* V = ctx->vjp;
+  const int nx = F.nx, ny = F.ny, K = V->K;
+  const size_t N = (size_t)nx * ny, SX = (size_t)ny * (nx + 1), SY = (size_t)(ny + 1) * nx;
+  const cudaStream_t st = ctx->stream;
+  // argmax states of the monitored cells
+  CU(ctx->aTmon.ensure((size_t)n * (n_mon > 0 ? n_mon : 1) * 4));
+  std::vector<unsigned> tmon((size_t)n * (n_mon > 0 ? n_mon : 1), 0u);
+  if (n_mon > 0) {
+    k_gather_u32<<<(n * n_mon + 255) / 256, 256, 0, st>>>(ctx->aTpk.as<unsigned>(), F.mon_cells, n_mon, N, n, ctx->aTmon.as<unsigned>());
+    CU(cudaMemcpyAsync(tmon.data(), ctx->aTmon.p, (size_t)n * n_mon * 4, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+  }
+  // seeds: for each asset, its argmax cell (first on ties) at the state that set the max,
+  // weighted by dJ/dP_k = w_k sigmoid((P_k - eta_k) / tau)
+  const int ms = ob->n_assets > 0 ? ob->n_assets : 1;
+  std::vector<unsigned> sc((size_t)n * ms, 0u), ss((size_t)n * ms, 0u);
+  std::vector<float> sw((size_t)n * ms, 0.0f);
+  std::vector<int> sn(n, 0);
+  for (int d = 0; d < n; ++d)
+    for (int a = 0; a < ob->n_assets; ++a) {
+      double best = 0.0;
+      int bp = -1;
+      for (int m = ob->asset_off[a]; m < ob->asset_off[a + 1]; ++m) {
+        const double v = (double)hmm[(size_t)d * n_mon + ob->asset_pos[m]];
+        if (bp < 0 || v > best) { best = v; bp = ob->asset_pos[m]; }
+      }
+      if (bp < 0) continue;
+      const unsigned state = tmon[(size_t)d * n_mon + bp];
+      if (state == 0u) continue;   // never raised above 0: no dependence
+      const double x = (best - ob->asset_threshold[a]) / ob->tau;
+      const size_t q = (size_t)d * ms + sn[d]++;
+      sc[q] = mon[bp]; ss[q] = state; sw[q] = (float)(ob->asset_weight[a] / (1.0 + std::exp(-x)));
+    }
+  std::vector<unsigned long long> nst(n);
+  unsigned long long nmax = 0;
+  for (int d = 0; d < n; ++d) { nst[d] = hdo[d].steps; nmax = nst[d] > nmax ? nst[d] : nmax; }
+  const uint64_t nblocks = (nmax + K - 1) / K;
+  if (nblocks > V->blocks) return fail(ctx, ITR_DEVICE_ERROR, "adjoint: %llu segments but %llu checkpoints",
+                                       (unsigned long long)nblocks, (unsigned long long)V->blocks);
+  CU(ctx->aSeedC.ensure(sc.size() * 4)); CU(ctx->aSeedS.ensure(ss.size() * 4)); CU(ctx->aSeedW.ensure(sw.size() * 4));
+  CU(ctx->aSeedN.ensure((size_t)n * 4)); CU(ctx->aNst.ensure((size_t)n * 8));
+  CU(cudaMemcpyAsync(ctx->aSeedC.p, sc.data(), sc.size() * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ctx->aSeedS.p, ss.data(), ss.size() * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ctx->aSeedW.p, sw.data(), sw.size() * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ctx->aSeedN.p, sn.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ctx->aNst.p, nst.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st));
+  const size_t S3 = (size_t)n * 3 * N;
+  CU(ctx->aTape.ensure((size_t)K * S3 * 4));
+  CU(ctx->aLA.ensure(S3 * 4)); CU(ctx->aLB.ensure(S3 * 4));
+  CU(ctx->aGx.ensure((size_t)n * SX * 8)); CU(ctx->aGy.ensure((size_t)n * SY * 8));
+  CU(ctx->aSeg.ensure((size_t)n * K * 2 * 8));
+  CU(ctx->aRingH.ensure((size_t)n * K * 2 * 8));
+  CU(cudaMemsetAsync(ctx->aLA.p, 0, S3 * 4, st));
+  CU(cudaMemsetAsync(ctx->aGx.p, 0, (size_t)n * SX * 8, st));
+  CU(cudaMemsetAsync(ctx->aGy.p, 0, (size_t)n * SY * 8, st));
+  AdjArgs A;
+  memset(&A, 0, sizeof(A));
+  A.P = F.P; A.nx = nx; A.ny = ny; A.n_designs = n;
+  A.wet = F.wet; A.gn2 = F.gn2; A.bc = F.bc; A.dzx = F.dzx; A.dzy = F.dzy;
+  A.n_steps = ctx->aNst.as<unsigned long long>();
+  A.seg = ctx->aSeg.as<double>(); A.K = K;
+  A.tape = ctx->aTape.as<float>();
+  A.gdzx = ctx->aGx.as<double>(); A.gdzy = ctx->aGy.as<double>();
+  A.seed_cell = ctx->aSeedC.as<unsigned>(); A.seed_state = ctx->aSeedS.as<unsigned>(); A.seed_w = ctx->aSeedW.as<float>();
+  A.seed_n = ctx->aSeedN.as<int>(); A.max_seeds = ms;
+  const dim3 grid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile, (unsigned)n);
+  float* lin = ctx->aLA.as<float>();
+  float* lout = ctx->aLB.as<float>();
+  double* segh = ctx->aRingH.as<double>();
+  for (uint64_t b = nblocks; b-- > 0;) {
+    CU(cudaStreamSynchronize(st));   // the previous segment's upload has left the host buffer
+    for (int d = 0; d < n; ++d)
+      for (int j = 0; j < K; ++j) {
+        const uint64_t s = b * K + j;
+        const bool have = s < nst[d];
+        segh[((size_t)d * K + j) * 2] = have ? V->dt[d][2 * s] : 0.0;
+        segh[((size_t)d * K + j) * 2 + 1] = have ? V->dt[d][2 * s + 1] : 0.0;
+      }
+    CU(cudaMemcpyAsync(ctx->aSeg.p, segh, (size_t)n * K * 2 * 8, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctx->aTape.p, ctx->aCkpt[b].p, S3 * 4, cudaMemcpyDeviceToDevice, st));
+    A.step0 = b * K;
+    for (int j = 0; j + 1 < K; ++j) k_adj_replay<<<grid, 256, 0, st>>>(A, j);
+    for (int j = K - 1; j >= 0; --j) {
+      A.lin = lin; A.lout = lout;
+      k_adj_step<<<grid, 256, 0, st>>>(A, j);
+      std::swap(lin, lout);
+    }
+    CU(cudaGetLastError());
+  }
+  CU(cudaMemcpyAsync(V->gx, ctx->aGx.p, (size_t)n * SX * 8, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(V->gy, ctx->aGy.p, (size_t)n * SY * 8, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  return ITR_OK;
 }
 
 // ------------------------------------------------------------------ run_batch -------
@@ -596,8 +740,8 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   const unsigned long long max_steps = 2000000000ull;
 
   // impl 2, or a grid no cluster shape can hold: the tiled batched path (state in HBM)
-  bool tiled = ctx->impl == 2;
-  if (ctx->impl == 0) {
+  bool tiled = ctx->impl == 2 || ctx->vjp != nullptr;
+  if (ctx->impl == 0 && !tiled) {
     BatchArgs A;
     memset(&A, 0, sizeof(A));
     A.P = P; A.nx = nx; A.ny = ny; A.mode = g->mode; A.n_designs = n;
@@ -685,6 +829,15 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.ledger = max_rows > 0 ? ctx->ledger.as<double>() : nullptr;
     A.max_rows = max_rows;
     A.max_steps = max_steps;
+    if (ctx->vjp) {
+      const int K = ctx->vjp->K;
+      CU(ctx->aTpk.ensure((size_t)n * N * 4));
+      CU(ctx->aRing.ensure((size_t)n * 2 * K * 2 * 8));
+      CU(ctx->aRingH.ensure((size_t)n * 2 * K * 2 * 8));
+      A.tpk = ctx->aTpk.as<unsigned>();
+      A.dt_log = ctx->aRing.as<double>();
+      A.max_log = 2 * K;
+    }
     CU(cudaEventRecord(ctx->ev[1], ctx->stream));
     rc = run_tiled_batch(ctx, A, n, tgrid, &launches);
     if (rc != ITR_OK) return rc;
@@ -820,6 +973,43 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     }
   }
   ctx->cell_updates = cu;
+  if (ctx->vjp) {
+    CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+    rc = vjp_backward(ctx, ctx->last_tiled, ob, n, mon, n_mon, hmm, hdo);
+    if (rc != ITR_OK) return rc;
+    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+    CU(cudaEventSynchronize(ctx->ev[2]));
+    float b_ms = 0;
+    cudaEventElapsedTime(&b_ms, ctx->ev[1], ctx->ev[2]);
+    ctx->vjp_fwd_ms = ctx->kernel_ms;
+    ctx->vjp_bwd_ms = b_ms;
+  }
+  return ITR_OK;
+}
+
+extern "C" int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
+                           const uint32_t* mon, int32_t n_mon, const itr_objective* ob, int32_t checkpoint_interval,
+                           itr_result* res, double* dj_ddzx, double* dj_ddzy) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (!ob || ob->n_assets < 1) return fail(ctx, ITR_INVALID_ARG, "the adjoint needs an objective with assets");
+  if (!g || g->mode != ITR_FACE_SIGNED) return fail(ctx, ITR_UNSUPPORTED, "the adjoint supports signed face jumps only");
+  if (checkpoint_interval < 1 || checkpoint_interval > 65536) return fail(ctx, ITR_INVALID_ARG, "checkpoint interval out of range");
+  if (n > 0 && (!dj_ddzx || !dj_ddzy)) return fail(ctx, ITR_INVALID_ARG, "gradient outputs are NULL");
+  itr_objective o = *ob;          // the taped forward runs every design to its end
+  o.guard_abort = 0;
+  o.has_incumbent = 0;
+  Vjp V;
+  V.K = checkpoint_interval; V.gx = dj_ddzx; V.gy = dj_ddzy;
+  ctx->vjp = &V;
+  const int rc = itr_gpu_run_batch(ctx, p, g, n, ds, mon, n_mon, &o, res);
+  ctx->vjp = nullptr;
+  return rc;
+}
+
+extern "C" int itr_gpu_last_vjp_timing(itr_ctx* ctx, double* forward_ms, double* backward_ms) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (forward_ms) *forward_ms = ctx->vjp_fwd_ms;
+  if (backward_ms) *backward_ms = ctx->vjp_bwd_ms;
   return ITR_OK;
 }
 

@@ -63,7 +63,7 @@ struct PlainArgs {
   int max_rows;
   unsigned long long max_steps;
   unsigned* tpk;      // optional, per design nx*ny: index of the state that last raised PK
-  double* dt_log;     // optional, per design max_log x (dt, rain) of every step
+  double* dt_log;     // optional, per design a ring of max_log (dt, rain): slot step % max_log
   int max_log;
 };
 
@@ -286,7 +286,10 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
     if (!(c.t < P.duration && c.sync_index < P.n_sync)) { c.done = 1; return; }
     if (c.step >= A.max_steps) { c.status = 4; c.done = 1; return; }
     c.pl = plan_step(P, c.t, c.sync_index, c.dt_cfl);
-    if (D.dt_log && c.step < (unsigned long long)A.max_log) { D.dt_log[2 * c.step] = c.pl.dt; D.dt_log[2 * c.step + 1] = c.pl.rain; }
+    if (D.dt_log) {   // ring of max_log entries, slot step mod max_log
+      const size_t slot = (size_t)(c.step % (unsigned long long)A.max_log);
+      D.dt_log[2 * slot] = c.pl.dt; D.dt_log[2 * slot + 1] = c.pl.rain;
+    }
     c.k = step_consts(P, c.pl.dt, c.pl.rain);
   }
 }

@@ -82,6 +82,9 @@ SIGNATURES = {
     "itr_gpu_set_option": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64]),
     "itr_gpu_last_timing": (C.c_int, [C.c_void_p, _dp, _dp, C.POINTER(C.c_uint64), _i32p]),
     "itr_gpu_rerun_resident": (C.c_int, [C.c_void_p]),
+    "itr_gpu_vjp": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.c_int32, C.POINTER(Design), _u32p,
+                              C.c_int32, C.POINTER(Objective), C.c_int32, C.POINTER(Result), _dp, _dp]),
+    "itr_gpu_last_vjp_timing": (C.c_int, [C.c_void_p, _dp, _dp]),
     "itr_gpu_run_plain_static": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(Grid), C.POINTER(Design), _u32p,
                                            C.c_int32, C.POINTER(Result), C.c_char_p, C.c_size_t]),
 }

@@ -185,6 +185,8 @@ class GpuRun:
     sync_count: int = 0
     rel_residual: float = 0.0
     cell_updates: int = 0
+    dj_ddzx: np.ndarray | None = None   # itr_gpu_vjp: dJ/d(x-face jump), (ny, nx+1)
+    dj_ddzy: np.ndarray | None = None   # itr_gpu_vjp: dJ/d(y-face jump), (ny+1, nx)
 
 
 @dataclass
@@ -260,9 +262,26 @@ class GpuSolver:
                                [(t.cut_m3, t.fill_m3) for t in terrains], monitors, objective, baseline_max, guard_abort,
                                incumbent, want_peak, want_depth, ledger_rows)
 
+    def vjp(self, p: SolverParams, terrains: list[PreparedTerrain], monitors: MonitorSet, objective: Objective,
+            checkpoint_interval: int = 128, want_peak: bool = False) -> list[GpuRun]:
+        """Forward runs plus dJ/d(face jump) per design (itr_gpu_vjp)."""
+        base: TerrainBase = terrains[0].base
+        return self.run_arrays(p, base, [t.dzx for t in terrains], [t.dzy for t in terrains],
+                               [t.dzx2 for t in terrains], [t.dzy2 for t in terrains],
+                               [t.initial_depth(p.initial_depth, p.initial_stage) if p.initial_stage is not None else None for t in terrains],
+                               [(t.cut_m3, t.fill_m3) for t in terrains], monitors, objective, want_peak=want_peak,
+                               want_depth=True, vjp_interval=checkpoint_interval)
+
+    def last_vjp_timing(self) -> dict:
+        f, b = C.c_double(), C.c_double()
+        self.lib.itr_gpu_last_vjp_timing(self.ctx, C.byref(f), C.byref(b))
+        return {"forward_ms": f.value, "backward_ms": b.value}
+
     def run_arrays(self, p: SolverParams, base, dzx, dzy, dzx2, dzy2, h0, vols, monitors: MonitorSet, objective=None,
-                   baseline_max=None, guard_abort=False, incumbent=None, want_peak=False, want_depth=True, ledger_rows=0):
-        """run_batch on packed per-design arrays (the C ABI's own view)."""
+                   baseline_max=None, guard_abort=False, incumbent=None, want_peak=False, want_depth=True, ledger_rows=0,
+                   vjp_interval: int | None = None):
+        """run_batch on packed per-design arrays (the C ABI's own view); with vjp_interval,
+        itr_gpu_vjp instead (the runs then carry dj_ddzx / dj_ddzy)."""
         n = len(dzx)
         nx, ny = base.nx, base.ny
         keep = []   # keep numpy buffers alive for the call
@@ -319,8 +338,16 @@ class GpuSolver:
             R[i].depth = _ptr(dp, C.c_float)
             R[i].ledger = _ptr(lg, C.c_double)
             R[i].max_rows = ledger_rows
-        rc = self.lib.itr_gpu_run_batch(self.ctx, C.byref(P), C.byref(Gd), n, D, _ptr(mon, C.c_uint32), nm,
-                                        C.byref(O) if O is not None else None, R)
+        if vjp_interval:
+            if O is None:
+                raise ValueError("the adjoint needs an objective")
+            gx = np.zeros((n, ny, nx + 1), dtype=np.float64)
+            gy = np.zeros((n, ny + 1, nx), dtype=np.float64)
+            rc = self.lib.itr_gpu_vjp(self.ctx, C.byref(P), C.byref(Gd), n, D, _ptr(mon, C.c_uint32), nm, C.byref(O),
+                                      int(vjp_interval), R, _ptr(gx, C.c_double), _ptr(gy, C.c_double))
+        else:
+            rc = self.lib.itr_gpu_run_batch(self.ctx, C.byref(P), C.byref(Gd), n, D, _ptr(mon, C.c_uint32), nm,
+                                            C.byref(O) if O is not None else None, R)
         if rc == _lib.ITR_UNSUPPORTED:
             raise UnsupportedError(self.lib.itr_gpu_last_error(self.ctx).decode())
         if rc != _lib.ITR_OK:
@@ -339,7 +366,8 @@ class GpuSolver:
                                ledger=lg[:r.n_rows].copy() if lg is not None else None, breach_cell=int(r.breach_cell),
                                breach_sync=int(r.breach_sync), violation=float(r.violation), lower_bound=float(r.lower_bound),
                                j=float(r.j), feasible=bool(r.feasible), sync_count=int(r.sync_count),
-                               rel_residual=float(r.rel_residual), cell_updates=int(r.cell_updates)))
+                               rel_residual=float(r.rel_residual), cell_updates=int(r.cell_updates),
+                               dj_ddzx=gx[i] if vjp_interval else None, dj_ddzy=gy[i] if vjp_interval else None))
             total += int(r.cell_updates)
         self.last_cell_updates = total
         return runs

@@ -254,31 +254,33 @@ extern "C" void orc_scene_run(void* h, int prec, int kernel, const int64_t* bbox
 // ------------------------------------------------------------------ flat (f32) -----
 // A terrain described only by the packed arrays of the GPU ABI. Stage/inflow ghosts are
 // not representable here (walls and transmissive only), matching the GPU path's scope.
-struct Flat {
+template <class T> struct FlatT {
   FineTerrain fine;  // only z_ref (0) and nothing else is read
-  TerrainBase<float> tb;
-  PreparedTerrain<float> pt;
+  TerrainBase<T> tb;
+  PreparedTerrain<T> pt;
 };
+using Flat = FlatT<float>;
 
-static void flat_build(Flat& F, int64_t nx, int64_t ny, double dx, double dy, int mode, const float* wet,
-                       const float* gn2, const uint8_t* bc, const float* dzx, const float* dzy,
-                       const float* dzx2, const float* dzy2) {
-  TerrainBase<float>& tb = F.tb;
+template <class T, class W>
+static void flat_build(FlatT<T>& F, int64_t nx, int64_t ny, double dx, double dy, int mode, const W* wet,
+                       const W* gn2, const uint8_t* bc, const W* dzx, const W* dzy,
+                       const W* dzx2, const W* dzy2) {
+  TerrainBase<T>& tb = F.tb;
   tb.fine = &F.fine; tb.level = 1; tb.dx = dx; tb.dy = dy; tb.g = G_ACC;
   tb.layout = Layout((size_t)nx, (size_t)ny);
   tb.mode = mode == 1 ? CREST : SIGNED;
   const Layout& L = tb.layout;
   size_t len = L.len();
-  tb.fx0.assign(len, 0.f); tb.fx1.assign(len, 0.f); tb.fy0.assign(len, 0.f); tb.fy1.assign(len, 0.f);
-  tb.wet.assign(len, 0.f); tb.gn2.assign(len, 0.f);
+  tb.fx0.assign(len, T(0)); tb.fx1.assign(len, T(0)); tb.fy0.assign(len, T(0)); tb.fy1.assign(len, T(0));
+  tb.wet.assign(len, T(0)); tb.gn2.assign(len, T(0));
   tb.z.assign((size_t)(nx * ny), 0.0); tb.wall.assign((size_t)(nx * ny), 0);
   tb.wet_count = 0;
   for (int64_t r = 0; r < ny; ++r)
     for (int64_t c = 0; c < nx; ++c) {
       size_t k = (size_t)(r * nx + c);
-      tb.wet[L.at(c + 1, r + 1)] = wet[k]; tb.gn2[L.at(c + 1, r + 1)] = gn2[k];
-      tb.wall[k] = !(wet[k] != 0.0f);
-      tb.wet_count += wet[k] != 0.0f;
+      tb.wet[L.at(c + 1, r + 1)] = (T)wet[k]; tb.gn2[L.at(c + 1, r + 1)] = (T)gn2[k];
+      tb.wall[k] = !(wet[k] != W(0));
+      tb.wet_count += wet[k] != W(0);
     }
   tb.bnd.north.assign(nx, Ghost{}); tb.bnd.south.assign(nx, Ghost{});
   tb.bnd.west.assign(ny, Ghost{}); tb.bnd.east.assign(ny, Ghost{});
@@ -289,13 +291,13 @@ static void flat_build(Flat& F, int64_t nx, int64_t ny, double dx, double dy, in
   F.pt.fx0 = tb.fx0; F.pt.fx1 = tb.fx1; F.pt.fy0 = tb.fy0; F.pt.fy1 = tb.fy1;
   for (int64_t r = 0; r < ny; ++r)
     for (int64_t f = 0; f <= nx; ++f) {
-      F.pt.fx0[L.at(f, r + 1)] = dzx[r * (nx + 1) + f];
-      if (dzx2) F.pt.fx1[L.at(f, r + 1)] = dzx2[r * (nx + 1) + f];
+      F.pt.fx0[L.at(f, r + 1)] = (T)dzx[r * (nx + 1) + f];
+      if (dzx2) F.pt.fx1[L.at(f, r + 1)] = (T)dzx2[r * (nx + 1) + f];
     }
   for (int64_t f = 0; f <= ny; ++f)
     for (int64_t c = 0; c < nx; ++c) {
-      F.pt.fy0[L.at(c + 1, f)] = dzy[f * nx + c];
-      if (dzy2) F.pt.fy1[L.at(c + 1, f)] = dzy2[f * nx + c];
+      F.pt.fy0[L.at(c + 1, f)] = (T)dzy[f * nx + c];
+      if (dzy2) F.pt.fy1[L.at(c + 1, f)] = (T)dzy2[f * nx + c];
     }
 }
 
@@ -317,6 +319,26 @@ extern "C" void orc_flat_run(int kernel, int64_t nx, int64_t ny, double dx, doub
   write_result(R, S, out_s, mon_max, mon_tmax, ledger, max_rows, h_out, qx_out, qy_out, peak, peak_step);
 }
 
+// The same run in f64 from f64 arrays (the f64 scalar oracle on the GPU ABI's packed view):
+// the reference for central finite differences of J with respect to single face jumps.
+extern "C" void orc_flat_run64(int kernel, int64_t nx, int64_t ny, double dx, double dy, int mode, const double* wet,
+                  const double* gn2, const uint8_t* bc, const double* dzx, const double* dzy, const double* dzx2,
+                  const double* dzy2, const double* h0, const double* pv, const double* rain_t, const double* rain_r,
+                  int n_rain, int n_mon, const uint32_t* mon, int n_guard, const int64_t* guard_pos, const double* baseline,
+                  int n_assets, const int64_t* asset_off, const int64_t* asset_pos, const double* asset_thr,
+                  const double* asset_w, const double* obj_f, int want_peak,
+                  double* out_s, double* mon_max, double* mon_tmax, double* ledger, int max_rows,
+                  double* h_out, double* qx_out, double* qy_out, double* peak, double* peak_step) {
+  FlatT<double> F;
+  flat_build(F, nx, ny, dx, dy, mode, wet, gn2, bc, dzx, dzy, dzx2, dzy2);
+  ObjIn oi; ObjIn* op = nullptr;
+  if (obj_f) { make_obj(oi, n_mon, mon, n_guard, guard_pos, baseline, n_assets, asset_off, asset_pos, asset_thr, asset_w, obj_f); op = &oi; }
+  Solver<double> S; S.p = make_params(pv, rain_t, rain_r, n_rain);
+  std::vector<uint32_t> mcells(mon, mon + n_mon);
+  RunResult R = S.run(F.pt, mcells, kernel == 0 ? K_ORACLE : K_FUSED, op ? &op->cfg : nullptr, h0, want_peak != 0);
+  write_result(R, S, out_s, mon_max, mon_tmax, ledger, max_rows, h_out, qx_out, qy_out, peak, peak_step);
+}
+
 // Candidate-parallel f32 fused runs (one design per thread, the reference's default search
 // mode, crates/itr-opt/src/evaluator.rs:337-352), for the timed CPU baseline. Face arrays are
 // per design (n_designs * ny*(nx+1) and n_designs * (ny+1)*nx). Returns wall seconds; steps
@@ -332,7 +354,7 @@ extern "C" double orc_flat_batch(int threads, int n_designs, int64_t nx, int64_t
       int d = next.fetch_add(1);
       if (d >= n_designs) break;
       Flat F;
-      flat_build(F, nx, ny, dx, dy, 0, wet, gn2, bc, dzx + (size_t)d * ny * (nx + 1), dzy + (size_t)d * (ny + 1) * nx, nullptr, nullptr);
+      flat_build(F, nx, ny, dx, dy, 0, wet, gn2, bc, dzx + (size_t)d * ny * (nx + 1), dzy + (size_t)d * (ny + 1) * nx, (const float*)nullptr, (const float*)nullptr);
       Solver<float> S; S.p = make_params(pv, rain_t, rain_r, n_rain);
       std::vector<uint32_t> mcells(mon, mon + n_mon);
       RunResult R = S.run(F.pt, mcells, K_FUSED, nullptr, h0 ? h0 + (size_t)d * nx * ny : nullptr, false);

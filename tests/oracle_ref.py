@@ -63,6 +63,8 @@ def lib():
     L.orc_scene_run.argtypes = [C.c_void_p, C.c_int, C.c_int, _i64, _d, C.c_double, C.c_double] + run_args + [_d] + out_args
     L.orc_flat_run.argtypes = ([C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int, _f, _f, _u8, _f, _f, _f, _f, _f]
                                + run_args + out_args)
+    L.orc_flat_run64.argtypes = ([C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int, _d, _d, _u8, _d, _d, _d, _d, _d]
+                                 + run_args + out_args)
     L.orc_flat_batch.restype = C.c_double
     L.orc_flat_batch.argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, _f, _f, _u8, _f, _f, _f, _d, _d,
                                  _d, C.c_int, C.c_int, _u32, _d, _d]
@@ -218,6 +220,28 @@ def flat_run(base_arrays, design, params, monitors, kernel=1, objective=None, ba
                                               P(bc, C.c_uint8), P(dzx, C.c_float), P(dzy, C.c_float), P(dzx2, C.c_float),
                                               P(dzy2, C.c_float), P(h0, C.c_float), *a),
                 nx, ny, params, monitors, objective, baseline, incumbent, cut, fill, None, want_peak, max_rows, scene=False)
+
+
+def flat_run64(base_arrays, design, params, monitors, kernel=1, objective=None, want_peak=False, max_rows=256):
+    """The f64 scalar oracle on the same packed arrays (face jumps taken as f64)."""
+    nx, ny, dx, dy, mode, wet, gn2, bc = base_arrays
+    keep = []
+
+    def f64(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return a
+
+    wet, gn2 = f64(wet), f64(gn2)
+    bc = np.ascontiguousarray(bc, dtype=np.uint8)
+    dzx, dzy, dzx2, dzy2, h0 = (f64(design.get(k)) for k in ("dzx", "dzy", "dzx2", "dzy2", "h0"))
+    cut, fill = design.get("cut", 0.0), design.get("fill", 0.0)
+    return _run(lambda *a: lib().orc_flat_run64(kernel, nx, ny, dx, dy, mode, P(wet, C.c_double), P(gn2, C.c_double),
+                                                P(bc, C.c_uint8), P(dzx, C.c_double), P(dzy, C.c_double), P(dzx2, C.c_double),
+                                                P(dzy2, C.c_double), P(h0, C.c_double), *a),
+                nx, ny, params, monitors, objective, None, None, cut, fill, None, want_peak, max_rows, scene=False)
 
 
 def flat_batch(threads, base_arrays, dzx_all, dzy_all, h0_all, params, monitors):
