@@ -62,6 +62,7 @@ struct LaunchCfg {
   int C = 1, T = 512, W = 1, S = 1;
   size_t smem = 0;
   bool ok = false;
+  bool tiled = false;   // the measured choice was the tiled HBM path
 };
 
 }  // namespace
@@ -741,6 +742,36 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
 
   // impl 2, or a grid no cluster shape can hold: the tiled batched path (state in HBM)
   bool tiled = ctx->impl == 2 || ctx->vjp != nullptr;
+  const dim3 tgrid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile);
+  const int n_tiles = (int)(tgrid.x * tgrid.y);
+  auto tiled_args = [&](PlainArgs& A) -> cudaError_t {
+    cudaError_t e = ctx->tH.ensure((size_t)n * 2 * N * 4);
+    if (e == cudaSuccess) e = ctx->tQX.ensure((size_t)n * 2 * N * 4);
+    if (e == cudaSuccess) e = ctx->tQY.ensure((size_t)n * 2 * N * 4);
+    if (e == cudaSuccess) e = ctx->tpart.ensure((size_t)n * n_tiles * 5 * 8);
+    if (e == cudaSuccess) e = ctx->tctl.ensure((size_t)n * sizeof(PlainCtl));
+    memset(&A, 0, sizeof(A));
+    A.P = P; A.nx = nx; A.ny = ny; A.mode = g->mode; A.n_designs = n;
+    A.wet = reinterpret_cast<const float*>(dv + o_wet);
+    A.gn2 = reinterpret_cast<const float*>(dv + o_gn2);
+    A.bc = reinterpret_cast<const uint8_t*>(dv + o_bc);
+    A.dzx = reinterpret_cast<const float*>(dv + o_dzx);
+    A.dzy = reinterpret_cast<const float*>(dv + o_dzy);
+    A.dzx2 = crest ? reinterpret_cast<const float*>(dv + o_dzx2) : nullptr;
+    A.dzy2 = crest ? reinterpret_cast<const float*>(dv + o_dzy2) : nullptr;
+    A.h0 = reinterpret_cast<const float*>(dv + o_h0);
+    A.cut_d = reinterpret_cast<const double*>(dv + o_cut);
+    A.fill_d = reinterpret_cast<const double*>(dv + o_fill);
+    A.n_mon = n_mon; A.mon_cells = reinterpret_cast<const unsigned*>(dv + o_mon);
+    A.obj = DO;
+    A.H = ctx->tH.as<float>(); A.QX = ctx->tQX.as<float>(); A.QY = ctx->tQY.as<float>();
+    A.PK = ctx->peak.as<float>();
+    A.part = ctx->tpart.as<double>(); A.ctl = ctx->tctl.as<PlainCtl>();
+    A.ledger = max_rows > 0 ? ctx->ledger.as<double>() : nullptr;
+    A.max_rows = max_rows;
+    A.max_steps = max_steps;
+    return e;
+  };
   if (ctx->impl == 0 && !tiled) {
     BatchArgs A;
     memset(&A, 0, sizeof(A));
@@ -773,6 +804,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
       if (!cfg.ok) return fail(ctx, ITR_UNSUPPORTED, "cluster=%d threads=%d does not fit a %dx%d grid in shared memory", ctx->cluster, ctx->threads, nx, ny);
     } else if (ctx->tuned.count(key)) {
       cfg = ctx->tuned[key];
+      tiled = cfg.tiled;
     } else {
       std::vector<LaunchCfg> cands = candidates(ctx, nx, ny, n, crest);
       if (cands.empty()) {
@@ -781,11 +813,32 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
         // Measured autotuning: time a short probe (the first steps of this very batch) of
         // the best few shapes by the model and keep the fastest for this (grid, population).
         cfg = cands[0];
-        if (ctx->autotune && cands.size() > 1) {
+        if (ctx->autotune) {   // (a single candidate is timed too: the tiled path is compared with it)
           rc = autotune(ctx, A, cands, n, &cfg);
           if (rc != ITR_OK) return rc;
         }
+        if (ctx->autotune) {
+          // the tiled HBM path as one more candidate, timed over the same probe steps
+          PlainArgs T;
+          CU(tiled_args(T));
+          T.max_steps = (unsigned long long)ctx->probe_steps;
+          T.obj.enabled = 0; T.ledger = nullptr; T.max_rows = 0;
+          int dummy = 0;
+          float t_ms = 0.0f;
+          // direct launches and one poll: no graph build or host round trips in the timing
+          const int g0 = ctx->graph, k0 = ctx->steps_per_submit;
+          ctx->graph = 0; ctx->steps_per_submit = ctx->probe_steps;
+          CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+          rc = run_tiled_batch(ctx, T, n, tgrid, &dummy);
+          ctx->graph = g0; ctx->steps_per_submit = k0;
+          if (rc != ITR_OK) return rc;
+          CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+          CU(cudaEventSynchronize(ctx->ev[2]));
+          CU(cudaEventElapsedTime(&t_ms, ctx->ev[1], ctx->ev[2]));
+          if (t_ms < ctx->tune_ms) { cfg.tiled = true; ctx->tune_ms = t_ms; }
+        }
         ctx->tuned[key] = cfg;
+        tiled = cfg.tiled;
       }
     }
     if (!tiled) {
@@ -803,32 +856,9 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     }
   }
   if (tiled) {
-    const dim3 tgrid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile);
-    const int nb = (int)(tgrid.x * tgrid.y);
-    CU(ctx->tH.ensure((size_t)n * 2 * N * 4)); CU(ctx->tQX.ensure((size_t)n * 2 * N * 4)); CU(ctx->tQY.ensure((size_t)n * 2 * N * 4));
-    CU(ctx->tpart.ensure((size_t)n * nb * 5 * 8));
-    CU(ctx->tctl.ensure((size_t)n * sizeof(PlainCtl)));
+    const int nb = n_tiles;
     PlainArgs A;
-    memset(&A, 0, sizeof(A));
-    A.P = P; A.nx = nx; A.ny = ny; A.mode = g->mode; A.n_designs = n;
-    A.wet = reinterpret_cast<const float*>(dv + o_wet);
-    A.gn2 = reinterpret_cast<const float*>(dv + o_gn2);
-    A.bc = reinterpret_cast<const uint8_t*>(dv + o_bc);
-    A.dzx = reinterpret_cast<const float*>(dv + o_dzx);
-    A.dzy = reinterpret_cast<const float*>(dv + o_dzy);
-    A.dzx2 = crest ? reinterpret_cast<const float*>(dv + o_dzx2) : nullptr;
-    A.dzy2 = crest ? reinterpret_cast<const float*>(dv + o_dzy2) : nullptr;
-    A.h0 = reinterpret_cast<const float*>(dv + o_h0);
-    A.cut_d = reinterpret_cast<const double*>(dv + o_cut);
-    A.fill_d = reinterpret_cast<const double*>(dv + o_fill);
-    A.n_mon = n_mon; A.mon_cells = reinterpret_cast<const unsigned*>(dv + o_mon);
-    A.obj = DO;
-    A.H = ctx->tH.as<float>(); A.QX = ctx->tQX.as<float>(); A.QY = ctx->tQY.as<float>();
-    A.PK = ctx->peak.as<float>();
-    A.part = ctx->tpart.as<double>(); A.ctl = ctx->tctl.as<PlainCtl>();
-    A.ledger = max_rows > 0 ? ctx->ledger.as<double>() : nullptr;
-    A.max_rows = max_rows;
-    A.max_steps = max_steps;
+    CU(tiled_args(A));
     if (ctx->vjp) {
       const int K = ctx->vjp->K;
       CU(ctx->aTpk.ensure((size_t)n * N * 4));
