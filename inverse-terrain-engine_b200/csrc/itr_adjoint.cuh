@@ -64,7 +64,7 @@ ITR_DEV void adj_load(const AdjArgs& A, const float* X, int gx, int gy, float& h
 }
 
 // ---- forward replay: x_{n+1} = F(x_n) with the recorded (dt, rain) ----
-__global__ void __launch_bounds__(256) k_adj_replay(const AdjArgs A, int j) {
+__global__ void __launch_bounds__(kTileThreads) k_adj_replay(const AdjArgs A, int j) {
   __shared__ float sh[18 * 18], su[18 * 18], sv[18 * 18], sc[18 * 18], sqx[18 * 18], sqy[18 * 18];
   __shared__ FaceF fx[16 * 17], fy[17 * 16];
   const int d = blockIdx.z;
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) k_adj_replay(const AdjArgs A, int j) {
   const float* dzy = A.dzy + d * SY;
   const int gx0 = blockIdx.x * kTile, gy0 = blockIdx.y * kTile;
   const int li = threadIdx.x;
-  for (int e = li; e < 324; e += 256) {
+  for (int e = li; e < 324; e += kTileThreads) {
     const int hx = e % 18, hy = e / 18;
     float h, qx, qy, u, v, c;
     adj_load(A, X, gx0 - 1 + hx, gy0 - 1 + hy, h, qx, qy);
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(256) k_adj_replay(const AdjArgs A, int j) {
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
   }
   __syncthreads();
-  for (int e = li; e < 272; e += 256) {
+  for (int e = li; e < 272; e += kTileThreads) {
     {
       const int fyr = e / 17, fxc = e % 17, row = gy0 + fyr, f = gx0 + fxc;
       if (row < ny && f <= nx) {
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(256) k_adj_replay(const AdjArgs A, int j) {
   }
   __syncthreads();
   const int lx = li % 16, ly = li / 16, gx = gx0 + lx, gy = gy0 + ly;
-  if (gx < nx && gy < ny) {
+  if (li < 256 && gx < nx && gy < ny) {
     const int a = (ly + 1) * 18 + lx + 1;
     const size_t gi = (size_t)gy * nx + gx;
     const CellNew o = update_cell(sh[a], sqx[a], sqy[a], fx[ly * 17 + lx], fx[ly * 17 + lx + 1], fy[ly * 16 + lx],
@@ -245,7 +245,7 @@ ITR_DEV void sources_bwd(float h, float qx, float qy, const FaceF& w, const Face
 // four faces' input adjoints (ghost sides folded back onto the interior cell).
 constexpr int kR = 20, kQ = 18;
 
-__global__ void __launch_bounds__(256) k_adj_step(const AdjArgs A, int j) {
+__global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int j) {
   __shared__ float sh[kR * kR], sqx[kR * kR], sqy[kR * kR], su[kR * kR], sv[kR * kR], sc[kR * kR];
   __shared__ FaceF fx[kQ * 19], fy[19 * kQ];           // forward faces of the 18x18 cells
   __shared__ float l1[3][kQ * kQ];                      // adjoint of (h1, qx1, qy1)
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(256) k_adj_step(const AdjArgs A, int j) {
   const int li = threadIdx.x;
   if (n >= A.n_steps[d]) {   // the design stopped before this step: the adjoint passes through
     const int gx = gx0 + li % 16, gy = gy0 + li / 16;
-    if (gx < nx && gy < ny) {
+    if (li < 256 && gx < nx && gy < ny) {
       const size_t gi = (size_t)gy * nx + gx;
       LO[gi] = LI[gi]; LO[N + gi] = LI[N + gi]; LO[2 * N + gi] = LI[2 * N + gi];
     }
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(256) k_adj_step(const AdjArgs A, int j) {
   const float* dzx = A.dzx + d * SX;
   const float* dzy = A.dzy + d * SY;
   // 1. state and velocities of the 20x20 region
-  for (int e = li; e < kR * kR; e += 256) {
+  for (int e = li; e < kR * kR; e += kTileThreads) {
     const int ix = e % kR, iy = e / kR;
     float h, qx, qy, u, v, c;
     adj_load(A, X, gx0 - 2 + ix, gy0 - 2 + iy, h, qx, qy);
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(256) k_adj_step(const AdjArgs A, int j) {
   __syncthreads();
   // 2. forward faces of the 18x18 cells: x-face (jr, fi) joins region cells (fi, jr+1) and
   //    (fi+1, jr+1); y-face (fr, ic) joins (ic+1, fr) and (ic+1, fr+1)
-  for (int e = li; e < kQ * 19; e += 256) {
+  for (int e = li; e < kQ * 19; e += kTileThreads) {
     {
       const int jr = e / 19, fi = e % 19;
       const int row = gy0 - 1 + jr, f = gx0 - 1 + fi;
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(256) k_adj_step(const AdjArgs A, int j) {
   __syncthreads();
   // 3. adjoint through the sources of every in-domain cell of the 18x18 region
   const int* sn = A.seed_n;
-  for (int e = li; e < kQ * kQ; e += 256) {
+  for (int e = li; e < kQ * kQ; e += kTileThreads) {
     const int ic = e % kQ, jr = e / kQ;
     const int gx = gx0 - 1 + ic, gy = gy0 - 1 + jr;
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(256) k_adj_step(const AdjArgs A, int j) {
   // 4. face adjoints and their input adjoints, for every face touching a tile cell
   double* gx_d = A.gdzx + d * SX;
   double* gy_d = A.gdzy + d * SY;
-  for (int e = li; e < 16 * 17; e += 256) {
+  for (int e = li; e < 16 * 17; e += kTileThreads) {
     {  // x-face between tile-row cells (xl-1, yr) and (xl, yr) of the 18x18 region, xl = 1..17
       const int yr = e / 17 + 1, xl = e % 17 + 1;
       const int row = gy0 - 1 + yr, f = gx0 - 1 + xl;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(256) k_adj_step(const AdjArgs A, int j) {
   //    the identity part of the flux update
   {
     const int lx = li % 16, ly = li / 16, gx = gx0 + lx, gy = gy0 + ly;
-    if (gx < nx && gy < ny) {
+    if (li < 256 && gx < nx && gy < ny) {
       const float* W = bx[ly * 17 + lx];        // west face: this cell is its R side
       const float* E = bx[ly * 17 + lx + 1];    // east face: L side
       const float* Nf = by[ly * 16 + lx];       // north face: B side

@@ -448,8 +448,8 @@ static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid,
   PlainCtl* hctl = ctx->hout.as<PlainCtl>();
   for (uint64_t guard = 0;; ++guard) {
     for (int s = 0; s < ctx->steps_per_submit; ++s) {
-      if (A.mode == 1) k_plain_update<true><<<grid, 256, 0, ctx->stream>>>(A);
-      else k_plain_update<false><<<grid, 256, 0, ctx->stream>>>(A);
+      if (A.mode == 1) k_plain_update<true><<<grid, kTileThreads, 0, ctx->stream>>>(A);
+      else k_plain_update<false><<<grid, kTileThreads, 0, ctx->stream>>>(A);
       k_plain_finalize<<<1, 32, 0, ctx->stream>>>(A, n_blocks, 0);
       *launches += 2;
     }
@@ -489,8 +489,8 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
   if (tape) { tape->dt.assign(n, std::vector<double>()); tape->blocks = 0; }
   auto block = [&]() {
     for (int s = 0; s < K; ++s) {
-      if (A.mode == 1) k_plain_update<true><<<grid, 256, 0, st>>>(A);
-      else k_plain_update<false><<<grid, 256, 0, st>>>(A);
+      if (A.mode == 1) k_plain_update<true><<<grid, kTileThreads, 0, st>>>(A);
+      else k_plain_update<false><<<grid, kTileThreads, 0, st>>>(A);
       k_plain_finalize<<<n, 32, 0, st>>>(A, nb, 0);
     }
   };
@@ -629,10 +629,10 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
     CU(cudaMemcpyAsync(ctx->aSeg.p, segh, (size_t)n * K * 2 * 8, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(ctx->aTape.p, ctx->aCkpt[b].p, S3 * 4, cudaMemcpyDeviceToDevice, st));
     A.step0 = b * K;
-    for (int j = 0; j + 1 < K; ++j) k_adj_replay<<<grid, 256, 0, st>>>(A, j);
+    for (int j = 0; j + 1 < K; ++j) k_adj_replay<<<grid, kTileThreads, 0, st>>>(A, j);
     for (int j = K - 1; j >= 0; --j) {
       A.lin = lin; A.lout = lout;
-      k_adj_step<<<grid, 256, 0, st>>>(A, j);
+      k_adj_step<<<grid, kTileThreads, 0, st>>>(A, j);
       std::swap(lin, lout);
     }
     CU(cudaGetLastError());

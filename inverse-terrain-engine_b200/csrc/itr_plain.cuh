@@ -18,6 +18,10 @@
 namespace itr {
 
 constexpr int kTile = 16;
+// Threads of the tiled kernels: 9 warps, so the 272 x-faces and 272 y-faces of a 16x16 tile
+// take one pass (with 256 threads a second pass would run 16 faces on a full block); the
+// 256 cells of the tile use the first 8 warps.
+constexpr int kTileThreads = 288;
 
 // Device-side integrator state of one design (the reference's Ctl words, in f64).
 struct PlainCtl {
@@ -111,12 +115,12 @@ ITR_DEV void plain_load(const PlainArgs& A, const PlainDesign& D, int par, int g
 }
 
 template <bool CREST>
-__global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
+__global__ void __launch_bounds__(kTileThreads) k_plain_update(const PlainArgs A) {
   __shared__ float sh[18 * 18], su[18 * 18], sv[18 * 18], sc[18 * 18], sqx[18 * 18], sqy[18 * 18];
   __shared__ FaceF fx[16 * 17], fy[17 * 16];
-  __shared__ float wmax[8];
-  __shared__ unsigned wbad[8];
-  __shared__ double wsum[8][5];
+  __shared__ float wmax[kTileThreads / 32];
+  __shared__ unsigned wbad[kTileThreads / 32];
+  __shared__ double wsum[kTileThreads / 32][5];
   const PlainDesign D = plain_design(A, blockIdx.z, gridDim.x * gridDim.y);
   const PlainCtl& cl = *D.ctl;
   if (cl.done) return;
@@ -127,7 +131,7 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
   const int nx = A.nx, ny = A.ny;
   const int gx0 = blockIdx.x * kTile, gy0 = blockIdx.y * kTile;
   const int li = threadIdx.x;
-  for (int e = li; e < 324; e += 256) {
+  for (int e = li; e < 324; e += kTileThreads) {
     int hx = e % 18, hy = e / 18;
     float h, qx, qy;
     plain_load(A, D, par, gx0 - 1 + hx, gy0 - 1 + hy, h, qx, qy);
@@ -136,7 +140,7 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
   }
   __syncthreads();
-  for (int e = li; e < 272; e += 256) {
+  for (int e = li; e < 272; e += kTileThreads) {
     {  // x-faces: 16 rows x 17
       int fyr = e / 17, fxc = e % 17;
       int row = gy0 + fyr, f = gx0 + fxc;
@@ -164,7 +168,7 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
   double acc[5] = {0, 0, 0, 0, 0};
   const int lx = li % 16, ly = li / 16;
   const int gx = gx0 + lx, gy = gy0 + ly;
-  if (gx < nx && gy < ny) {
+  if (li < 256 && gx < nx && gy < ny) {
     const FaceF w = fx[ly * 17 + lx], e = fx[ly * 17 + lx + 1];
     const FaceF n = fy[ly * 16 + lx], s = fy[(ly + 1) * 16 + lx];
     const int a = (ly + 1) * 18 + lx + 1;
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(256) k_plain_update(const PlainArgs A) {
   __syncthreads();
   if (li == 0) {
     float mm = 0.0f; unsigned bb = 0u; double ss[5] = {0, 0, 0, 0, 0};
-    for (int w = 0; w < 8; ++w) { mm = rmax(mm, wmax[w]); bb |= wbad[w]; for (int j = 0; j < 5; ++j) ss[j] += wsum[w][j]; }
+    for (int w = 0; w < kTileThreads / 32; ++w) { mm = rmax(mm, wmax[w]); bb |= wbad[w]; for (int j = 0; j < 5; ++j) ss[j] += wsum[w][j]; }
     if (mm > 0.0f) atomicMax(&D.ctl->smax_bits, __float_as_uint(mm));
     if (bb) atomicOr(&D.ctl->bad, 1u);
     double* p = D.part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 5;

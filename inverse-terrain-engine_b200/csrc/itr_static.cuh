@@ -243,8 +243,8 @@ extern "C" int itr_gpu_run_plain_static(int device, const itr_params* p, const i
   PlainCtl hc;
   for (uint64_t polls = 0;; ++polls) {
     for (int s = 0; s < kStepsPerPoll; ++s) {
-      if (crest) k_plain_update<true><<<grid, 256, 0, st>>>(A);
-      else k_plain_update<false><<<grid, 256, 0, st>>>(A);
+      if (crest) k_plain_update<true><<<grid, kTileThreads, 0, st>>>(A);
+      else k_plain_update<false><<<grid, kTileThreads, 0, st>>>(A);
       k_plain_finalize<<<1, 32, 0, st>>>(A, nb, 0);
     }
     SCU(cudaGetLastError());
