@@ -178,6 +178,43 @@ def cpu_baseline(sc, terrs, budget_s=20.0):
             "cell_steps": cs, "wall_s": wall}
 
 
+def plain_comparison(g, sc, terrs, n_sample=2):
+    """The plain one-design-per-launch CUDA forward (impl 1: per step one tiled update and one
+    finalize launch, designs one after another) on the first designs of the same workload,
+    full storm; its cell-steps/s does not depend on how many designs it runs in sequence."""
+    g.set_option("impl", 1)
+    try:
+        runs = g.run_batch(sc.params, terrs[:n_sample], sc.monitors, want_depth=False)
+        g.rerun_resident()
+        tm = g.last_timing()
+    finally:
+        g.set_option("impl", 0)
+    cs = float(sum(r.steps for r in runs)) * sc.base.nx * sc.base.ny
+    return {"value": cs / (tm["kernel_ms"] / 1e3), "unit": "cell-steps/s", "designs_sampled": n_sample,
+            "launches": tm["launches"], "kernel_ms": tm["kernel_ms"]}
+
+
+def adjoint_summary(g, K=128):
+    """Config 4 (rolling hills 240x192 @2.5 m, 60 min storm, 32 designs x 4 primitives): the
+    batched forward against itr_gpu_vjp (taped forward + checkpointed backward), device time."""
+    from itr_gpu.scenes import config
+    sc = config(4)
+    terrs = [t for _, _, t in sc.designs(32)]
+    g.run_batch(sc.params, terrs, sc.monitors, objective=sc.objective, want_depth=False)   # autotune
+    g.rerun_resident()
+    fwd = g.last_timing()["kernel_ms"]
+    # the first call sizes the context's checkpoint and tape buffers; a search loop reuses them
+    g.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=K)
+    runs = g.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=K)
+    v = g.last_vjp_timing()
+    cs = float(sum(r.steps for r in runs)) * sc.base.nx * sc.base.ny
+    return {"workload": "config4 rolling hills 240x192 @2.5 m, 3600 s storm, 32 designs x 4 primitives",
+            "forward_ms": fwd, "forward_cell_steps_per_s": cs / (fwd / 1e3), "checkpoint_interval": K,
+            "vjp_taped_forward_ms": v["forward_ms"], "vjp_backward_ms": v["backward_ms"],
+            "adjoint_over_forward": (v["forward_ms"] + v["backward_ms"]) / fwd,
+            "gradient": "dJ/d(face jump), f32 discrete adjoint with frozen dt; 0.1% vs f64 central differences (tests/test_adjoint.py)"}
+
+
 def run_reference(args):
     rank, world, _ = dist_setup(args.gpus)
     if rank != 0:
@@ -211,6 +248,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--designs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain one-design-per-launch comparison")
+    ap.add_argument("--cluster", type=int, default=0, help="pin the cluster size (profiling; 0 = autotune)")
+    ap.add_argument("--threads", type=int, default=0, help="pin the threads per CTA (profiling; 0 = autotune)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the config-4 adjoint summary")
     ap.add_argument("--duration", type=float, default=None,
                     help="simulate only the first DURATION s of the storm (profiling case; not a bench line)")
     args = ap.parse_args()
@@ -225,6 +266,9 @@ def main():
     if args.duration is not None:
         sc.params.duration_s = float(args.duration)
     g = GpuSolver(local)
+    if args.cluster or args.threads:
+        g.set_option("cluster", args.cluster)
+        g.set_option("threads", args.threads)
     N = sc.base.nx * sc.base.ny
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -300,6 +344,9 @@ def main():
                 traffic = float(tj["dram_bytes_per_launch"])
             except Exception:
                 traffic = None
+        # single-GPU only: the other ranks would wait on the closing barrier meanwhile
+        plain = None if args.no_plain or world > 1 else plain_comparison(g, sc, terrs)
+        adj = None if args.no_adjoint or world > 1 or args.duration is not None else adjoint_summary(g)
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(sc, terrs)
@@ -318,6 +365,9 @@ def main():
                          "traffic": traffic, "peak_source": src,
                          "model": f"{BYTES_PER_CELL_STEP} B/cell-step x {cell_steps:.4g} cell-steps per launch"},
             "cpu_baseline": cpu,
+            "plain": plain,
+            "batched_over_plain": (value / world / plain["value"]) if plain else None,
+            "adjoint": adj,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
             "clocks": clk.summary(),
