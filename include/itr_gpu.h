@@ -185,6 +185,23 @@ int itr_gpu_last_timing(itr_ctx* ctx, double* kernel_ms, double* total_ms, uint6
  * results kept on the device; for timing the kernel over resident inputs. */
 int itr_gpu_rerun_resident(itr_ctx* ctx);
 
+/* Uneven batch (the fidelity ladder: coarse, native and half-cell grids of one scene,
+ * evaluator.rs:218-266 runs one batch per level). Each group is one grid with its designs,
+ * monitors and objective, exactly the arguments of itr_gpu_run_batch; every group's
+ * persistent cluster kernel runs as one branch of a single CUDA graph launch, each with
+ * the launch shape autotuned for its grid, per-design adaptive dt and per-design aborts.
+ * results holds sum(n_designs) entries in group order. */
+typedef struct itr_group {
+  const itr_grid* grid;
+  int32_t n_designs;
+  const itr_design* designs;
+  const uint32_t* monitors;
+  int32_t n_mon;
+  const itr_objective* obj;    /* may be NULL */
+} itr_group;
+
+int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_groups, const itr_group* groups, itr_result* results);
+
 /* Vector-Jacobian product of the forward (the north star's adjoint; the reference has none,
  * its optimisers are derivative-free, crates/itr-opt/src/cmaes.rs). For every design it gives
  * dJ/d(face jump) of the asset term J = sum_k w_k tau softplus((P_k - eta_k) / tau)

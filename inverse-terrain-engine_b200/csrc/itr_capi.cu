@@ -67,6 +67,18 @@ struct LaunchCfg {
 
 }  // namespace
 
+// What the results phase of a batch needs (kept by a deferred ladder group until its launch).
+struct Collect {
+  int n = 0, n_mon = 0, max_rows = 0;
+  size_t N = 0;
+  const itr_design* ds = nullptr;
+  itr_result* res = nullptr;
+  const itr_objective* ob = nullptr;
+  const uint32_t* mon = nullptr;     // host monitor list
+  const unsigned* dmon = nullptr;    // its device copy
+  int launches = 0;
+};
+
 struct itr_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -91,6 +103,12 @@ struct itr_ctx {
   HostBuf aRingH;
   std::vector<DevBuf> aCkpt;
   struct Vjp* vjp = nullptr;
+  // ladder: one child context per grid group; a deferred run stops before its launch
+  std::vector<itr_ctx*> children;
+  bool defer = false;
+  bool pending_ok = false;
+  Collect pending;
+  cudaEvent_t ev_fork = nullptr;
   double vjp_fwd_ms = 0, vjp_bwd_ms = 0;
   HostBuf stage, hout;
   // last run
@@ -163,10 +181,10 @@ static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_targe
   return c;
 }
 
-static int launch_batched(itr_ctx* ctx, const BatchArgs& A, const LaunchCfg& cfg, int n_designs) {
+static int launch_batched(itr_ctx* ctx, const BatchArgs& A, const LaunchCfg& cfg, int n_designs, bool set_attr = true) {
   const bool crest = A.mode == 1, clustered = cfg.C > 1;
   BatchedFn fn = batched_fn(crest, clustered, maxt_bucket(cfg.T));
-  CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+  if (set_attr) CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   cudaLaunchConfig_t lc;
   memset(&lc, 0, sizeof(lc));
   lc.gridDim = dim3((unsigned)(n_designs * cfg.C), 1, 1);
@@ -392,6 +410,8 @@ void itr_gpu_destroy(itr_ctx* ctx) {
                     &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon})
     b->release();
   for (DevBuf& b : ctx->aCkpt) b.release();
+  for (itr_ctx* c : ctx->children) itr_gpu_destroy(c);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   ctx->aRingH.release();
   ctx->stage.release();
   ctx->hout.release();
@@ -643,6 +663,101 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   return ITR_OK;
 }
 
+// Results of a finished batch: per-design outcomes, monitor maxima, ledgers, J (host), and
+// for an adjoint request the backward sweep.
+static int collect_results(itr_ctx* ctx, const Collect& c) {
+  const int n = c.n, n_mon = c.n_mon, max_rows = c.max_rows;
+  const size_t N = c.N;
+  const itr_design* ds = c.ds;
+  itr_result* res = c.res;
+  const itr_objective* ob = c.ob;
+  const uint32_t* mon = c.mon;
+  int launches = c.launches;
+  int rc = ITR_OK;
+  // ---- results back ----
+  unsigned char* ho = ctx->hout.as<unsigned char>();
+  size_t hoff = 0;
+  DesignOut* hdo = reinterpret_cast<DesignOut*>(ho);
+  hoff = align_up((size_t)n * sizeof(DesignOut), 256);
+  float* hmm = reinterpret_cast<float*>(ho + hoff);
+  hoff = align_up(hoff + (size_t)n * (n_mon > 0 ? n_mon : 1) * 4, 256);
+  double* hled = reinterpret_cast<double*>(ho + hoff);
+  hoff = align_up(hoff + (size_t)n * (max_rows > 0 ? max_rows : 1) * 64, 256);
+  CU(cudaMemcpyAsync(hdo, ctx->out.p, (size_t)n * sizeof(DesignOut), cudaMemcpyDeviceToHost, ctx->stream));
+  if (n_mon > 0) {
+    int tot = n_mon * n;
+    k_gather_monitors<<<(tot + 255) / 256, 256, 0, ctx->stream>>>(ctx->peak.as<float>(), c.dmon, n_mon, N, n,
+                                                                   ctx->mmax.as<float>());
+    launches += 1;
+    CU(cudaMemcpyAsync(hmm, ctx->mmax.p, (size_t)tot * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (max_rows > 0) CU(cudaMemcpyAsync(hled, ctx->ledger.p, (size_t)n * max_rows * 64, cudaMemcpyDeviceToHost, ctx->stream));
+  for (int d = 0; d < n; ++d) {
+    if (res[d].peak) CU(cudaMemcpyAsync(res[d].peak, ctx->peak.as<float>() + d * N, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (res[d].depth) CU(cudaMemcpyAsync(res[d].depth, ctx->depth.as<float>() + d * N, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CU(cudaEventRecord(ctx->ev[3], ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+#ifdef ITR_CHECKED
+  {
+    unsigned long long e[4];
+    CU(cudaMemcpyFromSymbol(e, g_itr_err, sizeof(e)));
+    if (e[0]) return fail(ctx, ITR_DEVICE_ERROR, "checked build: bounds violation code %llu index %lld block %llu thread %llu",
+                          e[0], (long long)e[1], e[2], e[3]);
+  }
+#endif
+  float k_ms = 0, t_ms = 0;
+  cudaEventElapsedTime(&k_ms, ctx->ev[1], ctx->ev[2]);
+  cudaEventElapsedTime(&t_ms, ctx->ev[0], ctx->ev[3]);
+  ctx->kernel_ms = k_ms; ctx->total_ms = t_ms; ctx->launches = launches;
+  uint64_t cu = 0;
+  for (int d = 0; d < n; ++d) {
+    const DesignOut& o = hdo[d];
+    itr_result& r = res[d];
+    if (o.status >= 4) return fail(ctx, ITR_DEVICE_TIMEOUT, "design %d: run exceeded its step or wait limit (status %d)", d, o.status);
+    r.steps = o.steps;
+    r.cell_updates = o.steps * (uint64_t)N;
+    cu += r.cell_updates;
+    r.t_end = o.t_end;
+    r.sync_count = o.sync_count;
+    r.status = o.status;
+    r.breach_cell = o.breach_cell;
+    r.breach_sync = o.breach_sync;
+    r.lower_bound = o.lower_bound;
+    r.n_rows = o.n_rows < r.max_rows ? o.n_rows : r.max_rows;
+    r.volume_m3 = o.volume;
+    r.rel_residual = o.rel_residual;
+    if (r.monitor_max) for (int k = 0; k < n_mon; ++k) r.monitor_max[k] = (double)hmm[(size_t)d * n_mon + k];
+    if (r.ledger && r.max_rows > 0) memcpy(r.ledger, hled + (size_t)d * max_rows * 8, (size_t)r.n_rows * 64);
+    r.j = 0.0; r.feasible = 1; r.violation = 0.0;
+    if (ob) {
+      std::vector<double> mm(n_mon > 0 ? n_mon : 1);
+      for (int k = 0; k < n_mon; ++k) mm[k] = (double)hmm[(size_t)d * n_mon + k];
+      double j, worst;
+      host_objective(ob, mm.data(), ds[d].cut_m3, ds[d].fill_m3, j, worst);
+      r.j = j;
+      if (ob->require_no_worsening && ob->baseline_max && worst > ob->guard_tolerance) r.violation = worst - ob->guard_tolerance;
+      if (o.status == ITR_RUN_GUARD_ABORT) r.violation = o.violation;
+      r.feasible = (r.violation == 0.0 && o.status != ITR_RUN_GUARD_ABORT && o.status != ITR_RUN_UNHEALTHY) ? 1 : 0;
+    } else if (o.status == ITR_RUN_UNHEALTHY) {
+      r.feasible = 0;
+    }
+  }
+  ctx->cell_updates = cu;
+  if (ctx->vjp) {
+    CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+    rc = vjp_backward(ctx, ctx->last_tiled, ob, n, mon, n_mon, hmm, hdo);
+    if (rc != ITR_OK) return rc;
+    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+    CU(cudaEventSynchronize(ctx->ev[2]));
+    float b_ms = 0;
+    cudaEventElapsedTime(&b_ms, ctx->ev[1], ctx->ev[2]);
+    ctx->vjp_fwd_ms = ctx->kernel_ms;
+    ctx->vjp_bwd_ms = b_ms;
+  }
+  return ITR_OK;
+}
+
 // ------------------------------------------------------------------ run_batch -------
 extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
                                  const uint32_t* mon, int32_t n_mon, const itr_objective* ob, itr_result* res) {
@@ -843,6 +958,17 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     }
     if (!tiled) {
       A.C = cfg.C; A.W = cfg.W; A.S = cfg.S;
+      if (ctx->defer) {   // ladder group: the launch goes into the ladder's graph
+        BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T));
+        CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+        ctx->last_args = A; ctx->last_cfg = cfg; ctx->have_last = true;
+        ctx->last_was_plain = false; ctx->last_was_tiled = false;
+        Collect& c = ctx->pending;
+        c.n = n; c.n_mon = n_mon; c.max_rows = max_rows; c.N = N; c.ds = ds; c.res = res; c.ob = ob;
+        c.mon = mon; c.dmon = reinterpret_cast<const unsigned*>(dv + o_mon); c.launches = launches;
+        ctx->pending_ok = true;
+        return ITR_OK;
+      }
       CU(cudaEventRecord(ctx->ev[1], ctx->stream));
       rc = launch_batched(ctx, A, cfg, n);
       if (rc != ITR_OK) return rc;
@@ -933,87 +1059,91 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   }
   CU(cudaGetLastError());
 
-  // ---- results back ----
-  unsigned char* ho = ctx->hout.as<unsigned char>();
-  size_t hoff = 0;
-  DesignOut* hdo = reinterpret_cast<DesignOut*>(ho);
-  hoff = align_up((size_t)n * sizeof(DesignOut), 256);
-  float* hmm = reinterpret_cast<float*>(ho + hoff);
-  hoff = align_up(hoff + (size_t)n * (n_mon > 0 ? n_mon : 1) * 4, 256);
-  double* hled = reinterpret_cast<double*>(ho + hoff);
-  hoff = align_up(hoff + (size_t)n * (max_rows > 0 ? max_rows : 1) * 64, 256);
-  CU(cudaMemcpyAsync(hdo, ctx->out.p, (size_t)n * sizeof(DesignOut), cudaMemcpyDeviceToHost, ctx->stream));
-  if (n_mon > 0) {
-    int tot = n_mon * n;
-    k_gather_monitors<<<(tot + 255) / 256, 256, 0, ctx->stream>>>(ctx->peak.as<float>(), reinterpret_cast<const unsigned*>(dv + o_mon), n_mon, N, n,
-                                                                   ctx->mmax.as<float>());
-    launches += 1;
-    CU(cudaMemcpyAsync(hmm, ctx->mmax.p, (size_t)tot * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  Collect col;
+  col.n = n; col.n_mon = n_mon; col.max_rows = max_rows; col.N = N; col.ds = ds; col.res = res; col.ob = ob;
+  col.mon = mon; col.dmon = reinterpret_cast<const unsigned*>(dv + o_mon); col.launches = launches;
+  return collect_results(ctx, col);
+}
+
+// Uneven batch: several grid groups (the fidelity ladder's coarse, native and half-cell
+// grids) in one CUDA graph launch. Each group is prepared on its own child context (inputs
+// uploaded, launch shape autotuned for its grid) and its persistent cluster kernel becomes
+// one parallel branch of the graph; a group whose grid needs the tiled path runs on its own
+// before the graph. Results come back per group, in group order.
+extern "C" int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_groups, const itr_group* groups,
+                                  itr_result* results) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (n_groups < 1 || !groups || !results || !p) return fail(ctx, ITR_INVALID_ARG, "ladder: groups, params and results are required");
+  CU(cudaSetDevice(ctx->device));
+  while ((int)ctx->children.size() < n_groups) {
+    char err[256] = {0};
+    itr_ctx* c = itr_gpu_create(ctx->device, err, sizeof(err));
+    if (!c) return fail(ctx, ITR_DEVICE_ERROR, "ladder group context: %s", err);
+    ctx->children.push_back(c);
   }
-  if (max_rows > 0) CU(cudaMemcpyAsync(hled, ctx->ledger.p, (size_t)n * max_rows * 64, cudaMemcpyDeviceToHost, ctx->stream));
-  for (int d = 0; d < n; ++d) {
-    if (res[d].peak) CU(cudaMemcpyAsync(res[d].peak, ctx->peak.as<float>() + d * N, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    if (res[d].depth) CU(cudaMemcpyAsync(res[d].depth, ctx->depth.as<float>() + d * N, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!ctx->ev_fork) CU(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  size_t off = 0;
+  for (int gi = 0; gi < n_groups; ++gi) {
+    itr_ctx* c = ctx->children[gi];
+    c->impl = ctx->impl; c->threads = ctx->threads; c->cluster = ctx->cluster; c->graph = ctx->graph;
+    c->steps_per_submit = ctx->steps_per_submit; c->autotune = ctx->autotune; c->autotune_top = ctx->autotune_top;
+    c->probe_steps = ctx->probe_steps; c->exact_special = ctx->exact_special;
+    if (!c->ev_fork) CU(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    c->defer = true;
+    c->pending_ok = false;
+    const itr_group& G = groups[gi];
+    const int rc = itr_gpu_run_batch(c, p, G.grid, G.n_designs, G.designs, G.monitors, G.n_mon, G.obj, results + off);
+    c->defer = false;
+    if (rc != ITR_OK) return fail(ctx, rc, "ladder group %d: %s", gi, c->err.c_str());
+    CU(cudaStreamSynchronize(c->stream));   // its inputs are on the device before the graph runs
+    off += (size_t)(G.n_designs > 0 ? G.n_designs : 0);
   }
-  CU(cudaEventRecord(ctx->ev[3], ctx->stream));
-  CU(cudaStreamSynchronize(ctx->stream));
-#ifdef ITR_CHECKED
-  {
-    unsigned long long e[4];
-    CU(cudaMemcpyFromSymbol(e, g_itr_err, sizeof(e)));
-    if (e[0]) return fail(ctx, ITR_DEVICE_ERROR, "checked build: bounds violation code %llu index %lld block %llu thread %llu",
-                          e[0], (long long)e[1], e[2], e[3]);
+  // one graph: fork from the context stream into every deferred group's stream, join back
+  cudaGraph_t gr = nullptr;
+  CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = cudaEventRecord(ctx->ev_fork, ctx->stream);
+  for (int gi = 0; gi < n_groups && ce == cudaSuccess; ++gi) {
+    itr_ctx* c = ctx->children[gi];
+    if (!c->pending_ok) continue;
+    ce = cudaStreamWaitEvent(c->stream, ctx->ev_fork, 0);
+    if (ce == cudaSuccess && launch_batched(c, c->last_args, c->last_cfg, c->pending.n, false) != ITR_OK) ce = cudaErrorLaunchFailure;
+    if (ce == cudaSuccess) ce = cudaEventRecord(c->ev_fork, c->stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(ctx->stream, c->ev_fork, 0);
   }
-#endif
-  float k_ms = 0, t_ms = 0;
-  cudaEventElapsedTime(&k_ms, ctx->ev[1], ctx->ev[2]);
-  cudaEventElapsedTime(&t_ms, ctx->ev[0], ctx->ev[3]);
-  ctx->kernel_ms = k_ms; ctx->total_ms = t_ms; ctx->launches = launches;
+  const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &gr);
+  if (ce != cudaSuccess || ee != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    return fail(ctx, ITR_DEVICE_ERROR, "ladder graph capture: %s", cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+  }
+  cudaGraphExec_t ge = nullptr;
+  ce = cudaGraphInstantiate(&ge, gr, 0);
+  cudaGraphDestroy(gr);
+  CU(ce);
+  CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+  ce = cudaGraphLaunch(ge, ctx->stream);
+  if (ce == cudaSuccess) ce = cudaEventRecord(ctx->ev[2], ctx->stream);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+  cudaGraphExecDestroy(ge);
+  CU(ce);
+  float k_ms = 0.0f;
+  CU(cudaEventElapsedTime(&k_ms, ctx->ev[1], ctx->ev[2]));
   uint64_t cu = 0;
-  for (int d = 0; d < n; ++d) {
-    const DesignOut& o = hdo[d];
-    itr_result& r = res[d];
-    if (o.status >= 4) return fail(ctx, ITR_DEVICE_TIMEOUT, "design %d: run exceeded its step or wait limit (status %d)", d, o.status);
-    r.steps = o.steps;
-    r.cell_updates = o.steps * (uint64_t)N;
-    cu += r.cell_updates;
-    r.t_end = o.t_end;
-    r.sync_count = o.sync_count;
-    r.status = o.status;
-    r.breach_cell = o.breach_cell;
-    r.breach_sync = o.breach_sync;
-    r.lower_bound = o.lower_bound;
-    r.n_rows = o.n_rows < r.max_rows ? o.n_rows : r.max_rows;
-    r.volume_m3 = o.volume;
-    r.rel_residual = o.rel_residual;
-    if (r.monitor_max) for (int k = 0; k < n_mon; ++k) r.monitor_max[k] = (double)hmm[(size_t)d * n_mon + k];
-    if (r.ledger && r.max_rows > 0) memcpy(r.ledger, hled + (size_t)d * max_rows * 8, (size_t)r.n_rows * 64);
-    r.j = 0.0; r.feasible = 1; r.violation = 0.0;
-    if (ob) {
-      std::vector<double> mm(n_mon > 0 ? n_mon : 1);
-      for (int k = 0; k < n_mon; ++k) mm[k] = (double)hmm[(size_t)d * n_mon + k];
-      double j, worst;
-      host_objective(ob, mm.data(), ds[d].cut_m3, ds[d].fill_m3, j, worst);
-      r.j = j;
-      if (ob->require_no_worsening && ob->baseline_max && worst > ob->guard_tolerance) r.violation = worst - ob->guard_tolerance;
-      if (o.status == ITR_RUN_GUARD_ABORT) r.violation = o.violation;
-      r.feasible = (r.violation == 0.0 && o.status != ITR_RUN_GUARD_ABORT && o.status != ITR_RUN_UNHEALTHY) ? 1 : 0;
-    } else if (o.status == ITR_RUN_UNHEALTHY) {
-      r.feasible = 0;
+  int launches = 1;
+  for (int gi = 0; gi < n_groups; ++gi) {
+    itr_ctx* c = ctx->children[gi];
+    if (c->pending_ok) {
+      c->pending_ok = false;
+      const int rc = collect_results(c, c->pending);
+      if (rc != ITR_OK) return fail(ctx, rc, "ladder group %d: %s", gi, c->err.c_str());
     }
+    cu += c->cell_updates;
+    launches += c->launches;
   }
+  ctx->kernel_ms = k_ms;
+  ctx->total_ms = k_ms;
   ctx->cell_updates = cu;
-  if (ctx->vjp) {
-    CU(cudaEventRecord(ctx->ev[1], ctx->stream));
-    rc = vjp_backward(ctx, ctx->last_tiled, ob, n, mon, n_mon, hmm, hdo);
-    if (rc != ITR_OK) return rc;
-    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
-    CU(cudaEventSynchronize(ctx->ev[2]));
-    float b_ms = 0;
-    cudaEventElapsedTime(&b_ms, ctx->ev[1], ctx->ev[2]);
-    ctx->vjp_fwd_ms = ctx->kernel_ms;
-    ctx->vjp_bwd_ms = b_ms;
-  }
+  ctx->launches = launches;
+  ctx->have_last = false;
   return ITR_OK;
 }
 

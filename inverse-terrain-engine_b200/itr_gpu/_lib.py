@@ -71,6 +71,13 @@ class Result(C.Structure):
     ]
 
 
+class Group(C.Structure):
+    _fields_ = [
+        ("grid", C.POINTER(Grid)), ("n_designs", C.c_int32), ("designs", C.POINTER(Design)),
+        ("monitors", C.POINTER(C.c_uint32)), ("n_mon", C.c_int32), ("obj", C.POINTER(Objective)),
+    ]
+
+
 # Every symbol the header declares, with its signature.
 SIGNATURES = {
     "itr_gpu_create": (C.c_void_p, [C.c_int, C.c_char_p, C.c_size_t]),
@@ -82,6 +89,7 @@ SIGNATURES = {
     "itr_gpu_set_option": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64]),
     "itr_gpu_last_timing": (C.c_int, [C.c_void_p, _dp, _dp, C.POINTER(C.c_uint64), _i32p]),
     "itr_gpu_rerun_resident": (C.c_int, [C.c_void_p]),
+    "itr_gpu_run_ladder": (C.c_int, [C.c_void_p, C.POINTER(Params), C.c_int32, C.POINTER(Group), C.POINTER(Result)]),
     "itr_gpu_vjp": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.c_int32, C.POINTER(Design), _u32p,
                               C.c_int32, C.POINTER(Objective), C.c_int32, C.POINTER(Result), _dp, _dp]),
     "itr_gpu_last_vjp_timing": (C.c_int, [C.c_void_p, _dp, _dp]),

@@ -277,29 +277,29 @@ class GpuSolver:
         self.lib.itr_gpu_last_vjp_timing(self.ctx, C.byref(f), C.byref(b))
         return {"forward_ms": f.value, "backward_ms": b.value}
 
-    def run_arrays(self, p: SolverParams, base, dzx, dzy, dzx2, dzy2, h0, vols, monitors: MonitorSet, objective=None,
-                   baseline_max=None, guard_abort=False, incumbent=None, want_peak=False, want_depth=True, ledger_rows=0,
-                   vjp_interval: int | None = None):
-        """run_batch on packed per-design arrays (the C ABI's own view); with vjp_interval,
-        itr_gpu_vjp instead (the runs then carry dj_ddzx / dj_ddzy)."""
+    def _params(self, p: SolverParams, keep: list):
+        rain_t = np.ascontiguousarray([q[0] for q in p.rain.pts] or [0.0], dtype=np.float64)
+        rain_r = np.ascontiguousarray([q[1] for q in p.rain.pts] or [0.0], dtype=np.float64)
+        keep += [rain_t, rain_r]
+        return _lib.Params(p.duration_s, p.sync_interval_s, p.cfl, p.dt_max_s, p.h_dry, p.h_eps,
+                           _ptr(rain_t, C.c_double), _ptr(rain_r, C.c_double), len(p.rain.pts), p.infil_capacity,
+                           p.initial_depth, 1 if p.skip_dry else 0, p.inflow_scale)
+
+    def _pack(self, base, dzx, dzy, dzx2, dzy2, h0, vols, monitors: MonitorSet, objective, baseline_max, guard_abort,
+              incumbent, want_peak, want_depth, ledger_rows, keep: list) -> dict:
+        """ctypes views of one batch (grid, designs, monitors, objective, result slots)."""
         n = len(dzx)
         nx, ny = base.nx, base.ny
-        keep = []   # keep numpy buffers alive for the call
 
         def arr(a, dt):
             a = np.ascontiguousarray(a, dtype=dt)
             keep.append(a)
             return a
 
-        rain_t = arr([q[0] for q in p.rain.pts] or [0.0], np.float64)
-        rain_r = arr([q[1] for q in p.rain.pts] or [0.0], np.float64)
-        P = _lib.Params(p.duration_s, p.sync_interval_s, p.cfl, p.dt_max_s, p.h_dry, p.h_eps,
-                        _ptr(rain_t, C.c_double), _ptr(rain_r, C.c_double), len(p.rain.pts), p.infil_capacity,
-                        p.initial_depth, 1 if p.skip_dry else 0, p.inflow_scale)
         wet, gn2, bc = arr(base.wet, np.float32), arr(base.gn2, np.float32), arr(base.bc, np.uint8)
         Gd = _lib.Grid(nx, ny, base.dx, base.dy, base.g, base.mode, _ptr(wet, C.c_float), _ptr(gn2, C.c_float),
                        _ptr(bc, C.c_uint8), base.wet_count)
-        D = (_lib.Design * n)()
+        D = (_lib.Design * max(n, 1))()
         for i in range(n):
             a = arr(dzx[i], np.float32)
             b = arr(dzy[i], np.float32)
@@ -325,7 +325,8 @@ class GpuSolver:
                                d.guard_tolerance_m, d.tau_m, d.cut_cost, d.fill_cost, d.earth_weight,
                                1 if d.require_no_offsite_worsening else 0, 1 if guard_abort else 0,
                                1 if incumbent is not None else 0, float(incumbent or 0.0))
-        R = (_lib.Result * n)()
+            keep.append(O)
+        R = (_lib.Result * max(n, 1))()
         outs = []
         for i in range(n):
             mm = np.zeros(max(nm, 1), dtype=np.float64)
@@ -338,25 +339,22 @@ class GpuSolver:
             R[i].depth = _ptr(dp, C.c_float)
             R[i].ledger = _ptr(lg, C.c_double)
             R[i].max_rows = ledger_rows
-        if vjp_interval:
-            if O is None:
-                raise ValueError("the adjoint needs an objective")
-            gx = np.zeros((n, ny, nx + 1), dtype=np.float64)
-            gy = np.zeros((n, ny + 1, nx), dtype=np.float64)
-            rc = self.lib.itr_gpu_vjp(self.ctx, C.byref(P), C.byref(Gd), n, D, _ptr(mon, C.c_uint32), nm, C.byref(O),
-                                      int(vjp_interval), R, _ptr(gx, C.c_double), _ptr(gy, C.c_double))
-        else:
-            rc = self.lib.itr_gpu_run_batch(self.ctx, C.byref(P), C.byref(Gd), n, D, _ptr(mon, C.c_uint32), nm,
-                                            C.byref(O) if O is not None else None, R)
+        keep += [Gd, D, R]
+        return dict(n=n, nx=nx, ny=ny, base=base, Gd=Gd, D=D, mon=mon, nm=nm, O=O, R=R, outs=outs)
+
+    def _check(self, rc, what):
         if rc == _lib.ITR_UNSUPPORTED:
             raise UnsupportedError(self.lib.itr_gpu_last_error(self.ctx).decode())
         if rc != _lib.ITR_OK:
-            raise DeviceError(f"itr_gpu_run_batch failed ({rc}): {self.lib.itr_gpu_last_error(self.ctx).decode()}")
-        runs = []
+            raise DeviceError(f"{what} failed ({rc}): {self.lib.itr_gpu_last_error(self.ctx).decode()}")
+
+    @staticmethod
+    def _unpack(b: dict, R, gx=None, gy=None) -> list[GpuRun]:
+        n, nx, ny, nm, base = b["n"], b["nx"], b["ny"], b["nm"], b["base"]
         area = base.dx * base.dy
-        total = 0
+        runs = []
         for i in range(n):
-            mm, pk, dp, lg = outs[i]
+            mm, pk, dp, lg = b["outs"][i]
             r = R[i]
             depth = dp.reshape(ny, nx) if dp is not None else None
             runs.append(GpuRun(monitor_max=mm[:nm].copy(), steps=int(r.steps), t_end=float(r.t_end),
@@ -367,10 +365,67 @@ class GpuSolver:
                                breach_sync=int(r.breach_sync), violation=float(r.violation), lower_bound=float(r.lower_bound),
                                j=float(r.j), feasible=bool(r.feasible), sync_count=int(r.sync_count),
                                rel_residual=float(r.rel_residual), cell_updates=int(r.cell_updates),
-                               dj_ddzx=gx[i] if vjp_interval else None, dj_ddzy=gy[i] if vjp_interval else None))
-            total += int(r.cell_updates)
-        self.last_cell_updates = total
+                               dj_ddzx=gx[i] if gx is not None else None, dj_ddzy=gy[i] if gy is not None else None))
         return runs
+
+    def run_arrays(self, p: SolverParams, base, dzx, dzy, dzx2, dzy2, h0, vols, monitors: MonitorSet, objective=None,
+                   baseline_max=None, guard_abort=False, incumbent=None, want_peak=False, want_depth=True, ledger_rows=0,
+                   vjp_interval: int | None = None):
+        """run_batch on packed per-design arrays (the C ABI's own view); with vjp_interval,
+        itr_gpu_vjp instead (the runs then carry dj_ddzx / dj_ddzy)."""
+        keep = []   # keep numpy buffers alive for the call
+        P = self._params(p, keep)
+        b = self._pack(base, dzx, dzy, dzx2, dzy2, h0, vols, monitors, objective, baseline_max, guard_abort, incumbent,
+                       want_peak, want_depth, ledger_rows, keep)
+        n, nx, ny, O, R = b["n"], b["nx"], b["ny"], b["O"], b["R"]
+        gx = gy = None
+        if vjp_interval:
+            if O is None:
+                raise ValueError("the adjoint needs an objective")
+            gx = np.zeros((n, ny, nx + 1), dtype=np.float64)
+            gy = np.zeros((n, ny + 1, nx), dtype=np.float64)
+            rc = self.lib.itr_gpu_vjp(self.ctx, C.byref(P), C.byref(b["Gd"]), n, b["D"], _ptr(b["mon"], C.c_uint32), b["nm"],
+                                      C.byref(O), int(vjp_interval), R, _ptr(gx, C.c_double), _ptr(gy, C.c_double))
+        else:
+            rc = self.lib.itr_gpu_run_batch(self.ctx, C.byref(P), C.byref(b["Gd"]), n, b["D"], _ptr(b["mon"], C.c_uint32),
+                                            b["nm"], C.byref(O) if O is not None else None, R)
+        self._check(rc, "itr_gpu_run_batch")
+        runs = self._unpack(b, R, gx, gy)
+        self.last_cell_updates = sum(r.cell_updates for r in runs)
+        return runs
+
+    def run_ladder(self, p: SolverParams, groups: list[dict], want_peak=False, want_depth=False) -> list[list[GpuRun]]:
+        """itr_gpu_run_ladder: several grid groups (each a dict with terrains, monitors and
+        optionally objective, baseline_max, guard_abort, incumbent) in one graph launch."""
+        keep = []
+        P = self._params(p, keep)
+        packs = []
+        for g in groups:
+            ts = g["terrains"]
+            base = ts[0].base
+            packs.append(self._pack(base, [t.dzx for t in ts], [t.dzy for t in ts], [t.dzx2 for t in ts], [t.dzy2 for t in ts],
+                                    [t.initial_depth(p.initial_depth, p.initial_stage) if p.initial_stage is not None else None for t in ts],
+                                    [(t.cut_m3, t.fill_m3) for t in ts], g["monitors"], g.get("objective"), g.get("baseline_max"),
+                                    g.get("guard_abort", False), g.get("incumbent"), want_peak, want_depth, 0, keep))
+        total = sum(b["n"] for b in packs)
+        R = (_lib.Result * total)()
+        k = 0
+        for b in packs:                       # the result slots of each group, contiguous
+            for i in range(b["n"]):
+                R[k + i] = b["R"][i]
+            k += b["n"]
+        G = (_lib.Group * len(packs))()
+        for gi, b in enumerate(packs):
+            G[gi] = _lib.Group(C.pointer(b["Gd"]), b["n"], b["D"], _ptr(b["mon"], C.c_uint32), b["nm"],
+                               C.pointer(b["O"]) if b["O"] is not None else None)
+        rc = self.lib.itr_gpu_run_ladder(self.ctx, C.byref(P), len(packs), G, R)
+        self._check(rc, "itr_gpu_run_ladder")
+        out, k = [], 0
+        for b in packs:
+            out.append(self._unpack(b, R[k:k + b["n"]]))
+            k += b["n"]
+        self.last_cell_updates = sum(r.cell_updates for g in out for r in g)
+        return out
 
 
 class GpuBackend:
