@@ -215,6 +215,35 @@ def adjoint_summary(g, K=128):
             "gradient": "dJ/d(face jump), f32 discrete adjoint with frozen dt; 0.1% vs f64 central differences (tests/test_adjoint.py)"}
 
 
+def ladder_summary(g):
+    """Config 3 (uneven batching with early abort): the valley scene at 10, 5 and 2.5 m
+    (45x35, 90x70, 180x140), 40 min storm, 3 primitives per design, 256 designs split
+    128 / 96 / 32, guard and incumbent abort live (incumbent = best J of the previous batch,
+    frozen for this one), all groups in one CUDA graph launch (itr_gpu_run_ladder)."""
+    from itr_gpu import PreparedTerrain
+    from itr_gpu.scenes import valley_scene
+    spec, p = [], None
+    for cell, n in ((10.0, 128), (5.0, 96), (2.5, 32)):
+        sc = valley_scene(cell, n_prims=3)
+        sc.params.duration_s = 2400.0
+        p = sc.params
+        ts = [t for _, _, t in sc.designs(n)]
+        prev = [t for _, _, t in sc.designs(n, seed=sc.design_seed + 500)]   # the previous batch
+        base = g.run_batch(p, [PreparedTerrain(sc.base)], sc.monitors)[0]
+        inc = min(r.j for r in g.run_batch(p, prev, sc.monitors, objective=sc.objective, want_depth=False))
+        spec.append(dict(terrains=ts, monitors=sc.monitors, objective=sc.objective, baseline_max=base.monitor_max,
+                         guard_abort=True, incumbent=inc))
+    g.run_ladder(p, spec)                                        # autotunes each group's shape
+    out = g.run_ladder(p, spec)
+    t = g.last_timing()
+    cs = sum(r.cell_updates for o in out for r in o)
+    st = [r.status for o in out for r in o]
+    return {"workload": "config3 valley ladder 45x35/90x70/180x140, 2400 s storm, 128/96/32 designs x 3 primitives, aborts live",
+            "ms": t["kernel_ms"], "cell_steps_per_s": cs / (t["kernel_ms"] / 1e3), "designs_per_s": len(st) / (t["kernel_ms"] / 1e3),
+            "status_counts": {"ok": st.count(0), "guard_abort": st.count(1), "incumbent_abort": st.count(2), "unhealthy": st.count(3)},
+            "launch": "one CUDA graph, one persistent cluster kernel per grid as parallel branches"}
+
+
 def run_reference(args):
     rank, world, _ = dist_setup(args.gpus)
     if rank != 0:
@@ -252,6 +281,7 @@ def main():
     ap.add_argument("--cluster", type=int, default=0, help="pin the cluster size (profiling; 0 = autotune)")
     ap.add_argument("--threads", type=int, default=0, help="pin the threads per CTA (profiling; 0 = autotune)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the config-4 adjoint summary")
+    ap.add_argument("--no-ladder", action="store_true", help="skip the config-3 uneven-batch summary")
     ap.add_argument("--duration", type=float, default=None,
                     help="simulate only the first DURATION s of the storm (profiling case; not a bench line)")
     args = ap.parse_args()
@@ -347,6 +377,7 @@ def main():
         # single-GPU only: the other ranks would wait on the closing barrier meanwhile
         plain = None if args.no_plain or world > 1 else plain_comparison(g, sc, terrs)
         adj = None if args.no_adjoint or world > 1 or args.duration is not None else adjoint_summary(g)
+        lad = None if args.no_ladder or world > 1 or args.duration is not None else ladder_summary(g)
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(sc, terrs)
@@ -368,6 +399,7 @@ def main():
             "plain": plain,
             "batched_over_plain": (value / world / plain["value"]) if plain else None,
             "adjoint": adj,
+            "ladder": lad,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
             "clocks": clk.summary(),
