@@ -142,9 +142,9 @@ def sum_over_ranks(x, world):
     return float(t.item())
 
 
-def workload(rank=0, n_designs=64):
+def workload(rank=0, n_designs=64, which=2):
     from itr_gpu.scenes import config
-    sc = config(2)
+    sc = config(which)
     ds = sc.designs(n_designs, seed=sc.design_seed + 1000 * rank)
     return sc, [t for _, _, t in ds]
 
@@ -194,11 +194,13 @@ def plain_comparison(g, sc, terrs, n_sample=2):
             "launches": tm["launches"], "kernel_ms": tm["kernel_ms"]}
 
 
-def adjoint_summary(g, K=128):
+def adjoint_summary(g, K=128, duration=None):
     """Config 4 (rolling hills 240x192 @2.5 m, 60 min storm, 32 designs x 4 primitives): the
     batched forward against itr_gpu_vjp (taped forward + checkpointed backward), device time."""
     from itr_gpu.scenes import config
     sc = config(4)
+    if duration is not None:
+        sc.params.duration_s = float(duration)
     terrs = [t for _, _, t in sc.designs(32)]
     g.run_batch(sc.params, terrs, sc.monitors, objective=sc.objective, want_depth=False)   # autotune
     g.rerun_resident()
@@ -208,7 +210,7 @@ def adjoint_summary(g, K=128):
     runs = g.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=K)
     v = g.last_vjp_timing()
     cs = float(sum(r.steps for r in runs)) * sc.base.nx * sc.base.ny
-    return {"workload": "config4 rolling hills 240x192 @2.5 m, 3600 s storm, 32 designs x 4 primitives",
+    return {"workload": f"config4 rolling hills 240x192 @2.5 m, {sc.params.duration_s:.0f} s storm, 32 designs x 4 primitives",
             "forward_ms": fwd, "forward_cell_steps_per_s": cs / (fwd / 1e3), "checkpoint_interval": K,
             "vjp_taped_forward_ms": v["forward_ms"], "vjp_backward_ms": v["backward_ms"],
             "adjoint_over_forward": (v["forward_ms"] + v["backward_ms"]) / fwd,
@@ -282,6 +284,12 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="pin the threads per CTA (profiling; 0 = autotune)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the config-4 adjoint summary")
     ap.add_argument("--no-ladder", action="store_true", help="skip the config-3 uneven-batch summary")
+    ap.add_argument("--workload", type=int, default=2, choices=[2, 5],
+                    help="2: the bench workload; 5: the 1024x1024 scene (16 designs; measurement / profiling only)")
+    ap.add_argument("--impl-path", default="auto", choices=["auto", "tiled", "plain"],
+                    help="profiling: run the main workload on the tiled or plain path instead of the autotuned one")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="profiling: only the config-4 adjoint (forward + VJP) for --duration seconds of storm; prints its summary")
     ap.add_argument("--duration", type=float, default=None,
                     help="simulate only the first DURATION s of the storm (profiling case; not a bench line)")
     args = ap.parse_args()
@@ -292,13 +300,20 @@ def main():
     import torch
     torch.cuda.set_device(local)
     from itr_gpu import GpuSolver
-    sc, terrs = workload(rank, args.designs)
+    if args.adjoint_only:
+        g = GpuSolver(local)
+        print(json.dumps({"adjoint": adjoint_summary(g, duration=args.duration)}))
+        g.close()
+        return 0
+    sc, terrs = workload(rank, args.designs if args.workload == 2 else 16, args.workload)
     if args.duration is not None:
         sc.params.duration_s = float(args.duration)
     g = GpuSolver(local)
     if args.cluster or args.threads:
         g.set_option("cluster", args.cluster)
         g.set_option("threads", args.threads)
+    if args.impl_path != "auto":
+        g.set_option("impl", 2 if args.impl_path == "tiled" else 1)
     N = sc.base.nx * sc.base.ny
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -386,8 +401,11 @@ def main():
             "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": k_total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes and designs)",
-            "config": {"workload": "config2: rolling hills 120x96 @5 m, 60 min storm (100 mm/h peak at 20 min), "
-                                   f"{len(terrs)} designs x 4 primitives per GPU, run to completion",
+            "config": {"workload": ("config2: rolling hills 120x96 @5 m, 60 min storm (100 mm/h peak at 20 min), "
+                                    f"{len(terrs)} designs x 4 primitives per GPU, run to completion") if args.workload == 2 else
+                                   (f"config5: fractal 1024x1024 @2 m, {sc.params.duration_s:.0f} s of the 90 min double-peak storm, "
+                                    f"{len(terrs)} designs x 6 primitives"),
+                       "path": args.impl_path,
                        "designs_per_gpu": len(terrs), "cells": N, "steps_per_design_mean": sum(steps_per_design) / len(steps_per_design),
                        "parallelism": f"designs sharded over {world} GPU(s), 1 design per thread-block cluster",
                        "l2": "flushed between timed iterations (256 MB write)"},

@@ -64,7 +64,7 @@ ITR_DEV void adj_load(const AdjArgs& A, const float* X, int gx, int gy, float& h
 }
 
 // ---- forward replay: x_{n+1} = F(x_n) with the recorded (dt, rain) ----
-__global__ void __launch_bounds__(kTileThreads) k_adj_replay(const AdjArgs A, int j) {
+__global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A, int j) {
   __shared__ float sh[18 * 18], su[18 * 18], sv[18 * 18], sc[18 * 18], sqx[18 * 18], sqy[18 * 18];
   __shared__ FaceF fx[16 * 17], fy[17 * 16];
   const int d = blockIdx.z;
