@@ -202,7 +202,7 @@ typedef struct itr_group {
 
 int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_groups, const itr_group* groups, itr_result* results);
 
-/* Vector-Jacobian product of the forward (the north star's adjoint; the reference has none,
+/* Vector-Jacobian product of the forward (an addition: the reference has no adjoint,
  * its optimisers are derivative-free, crates/itr-opt/src/cmaes.rs). For every design it gives
  * dJ/d(face jump) of the asset term J = sum_k w_k tau softplus((P_k - eta_k) / tau)
  * (objective.rs:95-128; the earthwork term does not depend on the jumps):

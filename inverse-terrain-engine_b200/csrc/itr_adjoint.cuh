@@ -1,6 +1,6 @@
 // itr_adjoint.cuh — reverse-mode derivative (vector-Jacobian product) of the forward step.
 //
-// The reference has no adjoint; this is the north-star addition. For J = sum_k w_k tau
+// The reference has no adjoint (its optimisers are derivative-free). For J = sum_k w_k tau
 // softplus((P_k - eta_k)/tau) (objective.rs:95-128), with P_k the largest running-max depth
 // over asset k's monitored cells, it gives dJ/d(face jump) for every x- and y-face of every
 // design: dJ/ddzx[r][f] and dJ/ddzy[f][c] (the arrays the forward takes, shader.wgsl:25-26).

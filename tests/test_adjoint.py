@@ -1,6 +1,6 @@
 """Adjoint (itr_gpu_vjp): dJ/d(face jump) against central finite differences of the f64 oracle.
 
-<= 1% relative error against finite differences on a fully wet, smooth case
+Required: <= 1% relative error against finite differences on a fully wet, smooth case
 (initial depth 0.3 m, no dry cells). The adjoint is the derivative of the discrete f32 step
 with the recorded dt sequence held fixed; the finite differences rerun the f64 oracle with
 its own adaptive dt, so agreement also bounds the effect of freezing dt.
@@ -19,7 +19,7 @@ from itr_gpu import (Asset, GpuSolver, Hyetograph, Objective, ObjectiveDef, Prep
 
 pytestmark = pytest.mark.gpu
 
-FD_REL_TOL = 0.01      # north star: adjoint vs finite differences
+FD_REL_TOL = 0.01      # required: adjoint vs finite differences
 FD_STEP_M = 1e-3       # central difference step on one face jump
 
 

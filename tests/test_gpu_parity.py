@@ -2,7 +2,7 @@
 
 The oracle restates the reference's f32 fused kernel; with IEEE arithmetic and no FMA on
 both sides the results are expected bit for bit: same step count and end time, same final
-depth and same per-cell peak depth. The north-star tolerances (<= 1e-4 m peak depth,
+depth and same per-cell peak depth. The required tolerances (<= 1e-4 m peak depth,
 <= 1e-5 relative J) are asserted too, so a failure says which bar broke.
 Mirrors crates/itr-gpu/tests/gpu.rs (lake at rest, rain volume, CPU comparison, batch vs
 single, unsupported inputs rejected).
@@ -22,8 +22,8 @@ from itr_gpu.scenes import valley_scene
 
 pytestmark = pytest.mark.gpu
 
-PEAK_TOL_M = 1e-4      # north star: per-cell peak depth vs the reference's f32 kernel
-J_REL_TOL = 1e-5       # north star: relative J
+PEAK_TOL_M = 1e-4      # required: per-cell peak depth vs the reference's f32 kernel
+J_REL_TOL = 1e-5       # required: relative J
 
 
 @pytest.fixture(scope="module")
