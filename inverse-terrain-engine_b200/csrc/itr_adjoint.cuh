@@ -79,6 +79,17 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A,
   const float* dzy = A.dzy + d * SY;
   const int gx0 = blockIdx.x * kTile, gy0 = blockIdx.y * kTile;
   const int li = threadIdx.x;
+  // global loads first (face jumps, wet / g n^2, halo), as k_plain_update
+  const int fxr = li / 17, fxcol = li % 17, fyr_ = li / 16, fycol = li % 16;
+  const bool xv = li < 272 && gy0 + fxr < ny && gx0 + fxcol <= nx;
+  const bool yv = li < 272 && gx0 + fycol < nx && gy0 + fyr_ <= ny;
+  const size_t xo = (size_t)(gy0 + fxr) * (nx + 1) + gx0 + fxcol;
+  const size_t yo = (size_t)(gy0 + fyr_) * nx + gx0 + fycol;
+  const float xd = xv ? dzx[xo] : 0.0f, yd = yv ? dzy[yo] : 0.0f;
+  const int lx = li % 16, ly = li / 16, gx = gx0 + lx, gy = gy0 + ly;
+  const bool cv = li < 256 && gx < nx && gy < ny;
+  const size_t gi = (size_t)gy * nx + gx;
+  const float wet_c = cv ? A.wet[gi] : 0.0f, gn2_c = cv ? A.gn2[gi] : 0.0f;
   for (int e = li; e < 324; e += kTileThreads) {
     const int hx = e % 18, hy = e / 18;
     float h, qx, qy, u, v, c;
@@ -87,30 +98,19 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A,
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
   }
   __syncthreads();
-  for (int e = li; e < 272; e += kTileThreads) {
-    {
-      const int fyr = e / 17, fxc = e % 17, row = gy0 + fyr, f = gx0 + fxc;
-      if (row < ny && f <= nx) {
-        const int a = (fyr + 1) * 18 + fxc;
-        fx[e] = face<true, false>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1],
-                                  dzx[(size_t)row * (nx + 1) + f], 0.0f, k);
-      }
-    }
-    {
-      const int fyr = e / 16, fxc = e % 16, c = gx0 + fxc, f = gy0 + fyr;
-      if (c < nx && f <= ny) {
-        const int a = fyr * 18 + fxc + 1, b = a + 18;
-        fy[e] = face<false, false>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], dzy[(size_t)f * nx + c], 0.0f, k);
-      }
-    }
+  if (xv) {
+    const int a = (fxr + 1) * 18 + fxcol;
+    fx[li] = face<true, false>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], xd, 0.0f, k);
+  }
+  if (yv) {
+    const int a = fyr_ * 18 + fycol + 1, b = a + 18;
+    fy[li] = face<false, false>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], yd, 0.0f, k);
   }
   __syncthreads();
-  const int lx = li % 16, ly = li / 16, gx = gx0 + lx, gy = gy0 + ly;
-  if (li < 256 && gx < nx && gy < ny) {
+  if (cv) {
     const int a = (ly + 1) * 18 + lx + 1;
-    const size_t gi = (size_t)gy * nx + gx;
     const CellNew o = update_cell(sh[a], sqx[a], sqy[a], fx[ly * 17 + lx], fx[ly * 17 + lx + 1], fy[ly * 16 + lx],
-                                  fy[(ly + 1) * 16 + lx], A.wet[gi], A.gn2[gi], k);
+                                  fy[(ly + 1) * 16 + lx], wet_c, gn2_c, k);
     Y[gi] = o.h; Y[N + gi] = o.qx; Y[2 * N + gi] = o.qy;
   }
 }
@@ -248,6 +248,7 @@ constexpr int kR = 20, kQ = 18;
 __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int j) {
   __shared__ float sh[kR * kR], sqx[kR * kR], sqy[kR * kR], su[kR * kR], sv[kR * kR], sc[kR * kR];
   __shared__ FaceF fx[kQ * 19], fy[19 * kQ];           // forward faces of the 18x18 cells
+  __shared__ float jx[kQ * 19], jy[19 * kQ];            // their jumps
   __shared__ float l1[3][kQ * kQ];                      // adjoint of (h1, qx1, qy1)
   __shared__ float bx[16 * 17][8], by[17 * 16][8];      // face input adjoints: L (h,u,v,c), R (h,u,v,c)
   const int d = blockIdx.z;
@@ -271,7 +272,28 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
   const StepK k = step_consts(A.P, sg[0], sg[1]);
   const float* dzx = A.dzx + d * SX;
   const float* dzy = A.dzy + d * SY;
-  // 1. state and velocities of the 20x20 region
+  // 1. state and velocities of the 20x20 region; the face jumps and this thread's old
+  //    gradient sums are loaded first, so all these loads are in flight together
+  float jxa = 0.0f, jxb = 0.0f, jya = 0.0f, jyb = 0.0f;
+  const int e2 = li + kTileThreads;
+  auto xjump = [&](int e) -> float {
+    const int jr = e / 19, fi = e % 19, row = gy0 - 1 + jr, f = gx0 - 1 + fi;
+    return (row >= 0 && row < ny && f >= 0 && f <= nx) ? dzx[(size_t)row * (nx + 1) + f] : 0.0f;
+  };
+  auto yjump = [&](int e) -> float {
+    const int fr = e / kQ, ic = e % kQ, col = gx0 - 1 + ic, f = gy0 - 1 + fr;
+    return (col >= 0 && col < nx && f >= 0 && f <= ny) ? dzy[(size_t)f * nx + col] : 0.0f;
+  };
+  jxa = xjump(li); jya = yjump(li);
+  if (e2 < kQ * 19) { jxb = xjump(e2); jyb = yjump(e2); }
+  // the faces this thread differentiates in step 4 and whether its tile owns them
+  const int yr4 = li / 17 + 1, xl4 = li % 17 + 1, yt4 = li / 16 + 1, xc4 = li % 16 + 1;
+  const int row4 = gy0 - 1 + yr4, fx4 = gx0 - 1 + xl4, col4 = gx0 - 1 + xc4, fy4 = gy0 - 1 + yt4;
+  const bool xown = li < 272 && row4 < ny && fx4 <= nx && (fx4 < gx0 + kTile || fx4 == nx);
+  const bool yown = li < 272 && col4 < nx && fy4 <= ny && (fy4 < gy0 + kTile || fy4 == ny);
+  double* gxp = A.gdzx + d * SX + (size_t)row4 * (nx + 1) + fx4;
+  double* gyp = A.gdzy + d * SY + (size_t)fy4 * nx + col4;
+  const double gx_old = xown ? *gxp : 0.0, gy_old = yown ? *gyp : 0.0;
   for (int e = li; e < kR * kR; e += kTileThreads) {
     const int ix = e % kR, iy = e / kR;
     float h, qx, qy, u, v, c;
@@ -279,6 +301,8 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
     cell_vel(h, qx, qy, k.g, k.heps2, u, v, c);
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
   }
+  jx[li] = jxa; jy[li] = jya;
+  if (e2 < kQ * 19) { jx[e2] = jxb; jy[e2] = jyb; }
   __syncthreads();
   // 2. forward faces of the 18x18 cells: x-face (jr, fi) joins region cells (fi, jr+1) and
   //    (fi+1, jr+1); y-face (fr, ic) joins (ic+1, fr) and (ic+1, fr+1)
@@ -289,8 +313,7 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
       FaceF o{};
       if (row >= 0 && row < ny && f >= 0 && f <= nx) {
         const int a = (jr + 1) * kR + fi;
-        o = face<true, false>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1],
-                              dzx[(size_t)row * (nx + 1) + f], 0.0f, k);
+        o = face<true, false>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], jx[e], 0.0f, k);
       }
       fx[e] = o;
     }
@@ -300,7 +323,7 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
       FaceF o{};
       if (col >= 0 && col < nx && f >= 0 && f <= ny) {
         const int a = fr * kR + ic + 1, b = a + kR;
-        o = face<false, false>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], dzy[(size_t)f * nx + col], 0.0f, k);
+        o = face<false, false>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], jy[e], 0.0f, k);
       }
       fy[e] = o;
     }
@@ -328,8 +351,6 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
   }
   __syncthreads();
   // 4. face adjoints and their input adjoints, for every face touching a tile cell
-  double* gx_d = A.gdzx + d * SX;
-  double* gy_d = A.gdzy + d * SY;
   for (int e = li; e < 16 * 17; e += kTileThreads) {
     {  // x-face between tile-row cells (xl-1, yr) and (xl, yr) of the 18x18 region, xl = 1..17
       const int yr = e / 17 + 1, xl = e % 17 + 1;
@@ -342,11 +363,11 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
         const float lnl = -k.dtdx * l1[1][L], lnr = k.dtdx * l1[1][R];
         const float lt = -k.dtdx * l1[2][L] + k.dtdx * l1[2][R];
         const int a = (yr + 1) * kR + xl;   // region cell of L
-        const float dz = dzx[(size_t)row * (nx + 1) + f];
+        const float dz = jx[yr * 19 + xl];
         const FaceBwd b = face_bwd<true>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], dz, k,
                                          lm, lnl, lnr, lt);
         o[0] = b.hl; o[1] = b.ul; o[2] = b.vl; o[3] = b.cl; o[4] = b.hr; o[5] = b.ur; o[6] = b.vr; o[7] = b.cr;
-        if (f < gx0 + kTile || f == nx) gx_d[(size_t)row * (nx + 1) + f] += (double)b.dz;
+        if (xown) *gxp = gx_old + (double)b.dz;
       }
     }
     {  // y-face between (xc, yt-1) and (xc, yt) of the 18x18 region, yt = 1..17
@@ -360,11 +381,11 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
         const float lt = -k.dtdy * l1[1][T] + k.dtdy * l1[1][B];
         const float lnl = -k.dtdy * l1[2][T], lnr = k.dtdy * l1[2][B];
         const int a = yt * kR + xc + 1;      // region cell of T
-        const float dz = dzy[(size_t)f * nx + col];
+        const float dz = jy[yt * kQ + xc];
         const FaceBwd b = face_bwd<false>(sh[a], su[a], sv[a], sc[a], sh[a + kR], su[a + kR], sv[a + kR], sc[a + kR], dz,
                                           k, lm, lnl, lnr, lt);
         o[0] = b.hl; o[1] = b.ul; o[2] = b.vl; o[3] = b.cl; o[4] = b.hr; o[5] = b.ur; o[6] = b.vr; o[7] = b.cr;
-        if (f < gy0 + kTile || f == ny) gy_d[(size_t)f * nx + col] += (double)b.dz;
+        if (yown) *gyp = gy_old + (double)b.dz;
       }
     }
   }

@@ -373,6 +373,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   const size_t ox0 = (size_t)d * ny * nxp1 + cc0, ox1 = (size_t)d * ny * nxp1 + cc1;
   const size_t oy0 = (size_t)d * (ny + 1) * nx + oc0, oy1 = (size_t)d * (ny + 1) * nx + oc1;
   const int bc_w = 2 * nx, bc_e = 2 * nx + ny, bc_n = 0, bc_s = nx, nbc = 2 * nx + 2 * ny;
+  (void)nbc;   // used by the checked build's index checks
 
   // Prefetch ring: row r's operands for this thread's two columns are copied one row ahead.
   constexpr int K = CREST ? 6 : 4;

@@ -618,8 +618,10 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   CU(ctx->aTape.ensure((size_t)K * S3 * 4));
   CU(ctx->aLA.ensure(S3 * 4)); CU(ctx->aLB.ensure(S3 * 4));
   CU(ctx->aGx.ensure((size_t)n * SX * 8)); CU(ctx->aGy.ensure((size_t)n * SY * 8));
-  CU(ctx->aSeg.ensure((size_t)n * K * 2 * 8));
-  CU(ctx->aRingH.ensure((size_t)n * K * 2 * 8));
+  // (dt, rain) of every segment, laid out [segment][design][K][2], uploaded once
+  const size_t seg_elems = (size_t)n * K * 2;
+  CU(ctx->aSeg.ensure(nblocks * seg_elems * 8));
+  CU(ctx->aRingH.ensure(nblocks * seg_elems * 8));
   CU(cudaMemsetAsync(ctx->aLA.p, 0, S3 * 4, st));
   CU(cudaMemsetAsync(ctx->aGx.p, 0, (size_t)n * SX * 8, st));
   CU(cudaMemsetAsync(ctx->aGy.p, 0, (size_t)n * SY * 8, st));
@@ -637,18 +639,20 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   float* lin = ctx->aLA.as<float>();
   float* lout = ctx->aLB.as<float>();
   double* segh = ctx->aRingH.as<double>();
-  for (uint64_t b = nblocks; b-- > 0;) {
-    CU(cudaStreamSynchronize(st));   // the previous segment's upload has left the host buffer
+  for (uint64_t b = 0; b < nblocks; ++b)
     for (int d = 0; d < n; ++d)
       for (int j = 0; j < K; ++j) {
         const uint64_t s = b * K + j;
         const bool have = s < nst[d];
-        segh[((size_t)d * K + j) * 2] = have ? V->dt[d][2 * s] : 0.0;
-        segh[((size_t)d * K + j) * 2 + 1] = have ? V->dt[d][2 * s + 1] : 0.0;
+        double* q = segh + b * seg_elems + ((size_t)d * K + j) * 2;
+        q[0] = have ? V->dt[d][2 * s] : 0.0;
+        q[1] = have ? V->dt[d][2 * s + 1] : 0.0;
       }
-    CU(cudaMemcpyAsync(ctx->aSeg.p, segh, (size_t)n * K * 2 * 8, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ctx->aSeg.p, segh, nblocks * seg_elems * 8, cudaMemcpyHostToDevice, st));
+  for (uint64_t b = nblocks; b-- > 0;) {   // no host round trip between segments
     CU(cudaMemcpyAsync(ctx->aTape.p, ctx->aCkpt[b].p, S3 * 4, cudaMemcpyDeviceToDevice, st));
     A.step0 = b * K;
+    A.seg = ctx->aSeg.as<double>() + b * seg_elems;
     for (int j = 0; j + 1 < K; ++j) k_adj_replay<<<grid, kTileThreads, 0, st>>>(A, j);
     for (int j = K - 1; j >= 0; --j) {
       A.lin = lin; A.lout = lout;

@@ -22,6 +22,7 @@ constexpr int kTile = 16;
 // take one pass (with 256 threads a second pass would run 16 faces on a full block); the
 // 256 cells of the tile use the first 8 warps.
 constexpr int kTileThreads = 288;
+static_assert(kTileThreads >= 17 * 16, "one x-face and one y-face per thread");
 // The update kernels ask for 6 resident blocks per SM (32 registers a thread): with the
 // 18x18 halo loads waiting on HBM, more resident warps beat fewer registers (measured +10%).
 
@@ -133,6 +134,21 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArg
   const int nx = A.nx, ny = A.ny;
   const int gx0 = blockIdx.x * kTile, gy0 = blockIdx.y * kTile;
   const int li = threadIdx.x;
+  // Every global load of this thread is issued first, so their latencies overlap: the
+  // jumps of its x- and y-face (thread e computes x-face e and y-face e), its cell's wet,
+  // g n^2 and running peak, then its halo cells.
+  const int fxr = li / 17, fxcol = li % 17, fyr_ = li / 16, fycol = li % 16;
+  const bool xv = li < 272 && gy0 + fxr < ny && gx0 + fxcol <= nx;
+  const bool yv = li < 272 && gx0 + fycol < nx && gy0 + fyr_ <= ny;
+  const size_t xo = (size_t)(gy0 + fxr) * (nx + 1) + gx0 + fxcol;
+  const size_t yo = (size_t)(gy0 + fyr_) * nx + gx0 + fycol;
+  const float xd0 = xv ? D.dzx[xo] : 0.0f, xd1 = (CREST && xv) ? D.dzx2[xo] : 0.0f;
+  const float yd0 = yv ? D.dzy[yo] : 0.0f, yd1 = (CREST && yv) ? D.dzy2[yo] : 0.0f;
+  const int lx = li % 16, ly = li / 16;
+  const int gx = gx0 + lx, gy = gy0 + ly;
+  const bool cv = li < 256 && gx < nx && gy < ny;
+  const size_t gi = (size_t)gy * nx + gx;
+  const float wet_c = cv ? A.wet[gi] : 0.0f, gn2_c = cv ? A.gn2[gi] : 0.0f, pk_c = cv ? D.PK[gi] : 0.0f;
   for (int e = li; e < 324; e += kTileThreads) {
     int hx = e % 18, hy = e / 18;
     float h, qx, qy;
@@ -142,43 +158,26 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArg
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
   }
   __syncthreads();
-  for (int e = li; e < 272; e += kTileThreads) {
-    {  // x-faces: 16 rows x 17
-      int fyr = e / 17, fxc = e % 17;
-      int row = gy0 + fyr, f = gx0 + fxc;
-      if (row < ny && f <= nx) {
-        int a = (fyr + 1) * 18 + fxc;
-        size_t o = (size_t)row * (nx + 1) + f;
-        float d0 = D.dzx[o], d1 = CREST ? D.dzx2[o] : 0.0f;
-        fx[e] = face<true, CREST>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], d0, d1, k);
-      }
-    }
-    {  // y-faces: 17 rows x 16
-      int fyr = e / 16, fxc = e % 16;
-      int c = gx0 + fxc, f = gy0 + fyr;
-      if (c < nx && f <= ny) {
-        int a = fyr * 18 + fxc + 1, b = a + 18;
-        size_t o = (size_t)f * nx + c;
-        float d0 = D.dzy[o], d1 = CREST ? D.dzy2[o] : 0.0f;
-        fy[e] = face<false, CREST>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], d0, d1, k);
-      }
-    }
+  if (xv) {  // x-faces: 16 rows x 17
+    const int a = (fxr + 1) * 18 + fxcol;
+    fx[li] = face<true, CREST>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], xd0, xd1, k);
+  }
+  if (yv) {  // y-faces: 17 rows x 16
+    const int a = fyr_ * 18 + fycol + 1, b = a + 18;
+    fy[li] = face<false, CREST>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], yd0, yd1, k);
   }
   __syncthreads();
   float smax = 0.0f;
   bool bad = false;
   double acc[5] = {0, 0, 0, 0, 0};
-  const int lx = li % 16, ly = li / 16;
-  const int gx = gx0 + lx, gy = gy0 + ly;
-  if (li < 256 && gx < nx && gy < ny) {
+  if (cv) {
     const FaceF w = fx[ly * 17 + lx], e = fx[ly * 17 + lx + 1];
     const FaceF n = fy[ly * 16 + lx], s = fy[(ly + 1) * 16 + lx];
     const int a = (ly + 1) * 18 + lx + 1;
-    const size_t gi = (size_t)gy * nx + gx;
-    CellNew o = update_cell(sh[a], sqx[a], sqy[a], w, e, n, s, A.wet[gi], A.gn2[gi], k);
+    CellNew o = update_cell(sh[a], sqx[a], sqy[a], w, e, n, s, wet_c, gn2_c, k);
     const size_t wo = (size_t)(par ^ 1) * nx * ny + gi;
     D.H[wo] = o.h; D.QX[wo] = o.qx; D.QY[wo] = o.qy;
-    if (o.h > D.PK[gi]) {
+    if (o.h > pk_c) {
       D.PK[gi] = o.h;
       if (D.tpk) D.tpk[gi] = (unsigned)(cl.step + 1);   // this step makes state step+1
     }
