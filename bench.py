@@ -194,14 +194,18 @@ def plain_comparison(g, sc, terrs, n_sample=2):
             "launches": tm["launches"], "kernel_ms": tm["kernel_ms"]}
 
 
-def adjoint_summary(g, K=128, duration=None):
-    """Config 4 (rolling hills 240x192 @2.5 m, 60 min storm, 32 designs x 4 primitives): the
+def adjoint_summary(g, K=128, duration=None, which=4):
+    """Config 4 (rolling hills 240x192 @2.5 m, 60 min storm, 32 designs x 4 primitives), or
+    config 5 (fractal 1024x1024 @2 m, 90 min storm, 16 designs x 6 primitives, K = 256): the
     batched forward against itr_gpu_vjp (taped forward + checkpointed backward), device time."""
     from itr_gpu.scenes import config
-    sc = config(4)
+    sc = config(which)
     if duration is not None:
         sc.params.duration_s = float(duration)
-    terrs = [t for _, _, t in sc.designs(32)]
+    n = 32 if which == 4 else 16
+    if which == 5:
+        K = 256
+    terrs = [t for _, _, t in sc.designs(n)]
     g.run_batch(sc.params, terrs, sc.monitors, objective=sc.objective, want_depth=False)   # autotune
     g.rerun_resident()
     fwd = g.last_timing()["kernel_ms"]
@@ -210,7 +214,8 @@ def adjoint_summary(g, K=128, duration=None):
     runs = g.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=K)
     v = g.last_vjp_timing()
     cs = float(sum(r.steps for r in runs)) * sc.base.nx * sc.base.ny
-    return {"workload": f"config4 rolling hills 240x192 @2.5 m, {sc.params.duration_s:.0f} s storm, 32 designs x 4 primitives",
+    label = ("config4 rolling hills 240x192 @2.5 m" if which == 4 else "config5 fractal 1024x1024 @2 m")
+    return {"workload": f"{label}, {sc.params.duration_s:.0f} s storm, {n} designs x {sc.n_prims} primitives",
             "forward_ms": fwd, "forward_cell_steps_per_s": cs / (fwd / 1e3), "checkpoint_interval": K,
             "vjp_taped_forward_ms": v["forward_ms"], "vjp_backward_ms": v["backward_ms"],
             "adjoint_over_forward": (v["forward_ms"] + v["backward_ms"]) / fwd,
@@ -302,7 +307,7 @@ def main():
     from itr_gpu import GpuSolver
     if args.adjoint_only:
         g = GpuSolver(local)
-        print(json.dumps({"adjoint": adjoint_summary(g, duration=args.duration)}))
+        print(json.dumps({"adjoint": adjoint_summary(g, duration=args.duration, which=4 if args.workload == 2 else 5)}))
         g.close()
         return 0
     sc, terrs = workload(rank, args.designs if args.workload == 2 else 16, args.workload)
