@@ -251,6 +251,26 @@ def ladder_summary(g):
             "launch": "one CUDA graph, one persistent cluster kernel per grid as parallel branches"}
 
 
+def boundary_summary(g):
+    """Stage and inflow ghosts (the boundaries the reference's GPU backend declined): the
+    inflow-driven valley at 5 m (90x70; inflow hydrographs on the west and south edges,
+    stage on the east and north), 40 min storm, 64 designs on the batched path, beside the
+    same designs on the valley with its plain transmissive outlet. Both run twice; the
+    second run (autotuned shape) is timed."""
+    from itr_gpu.scenes import inflow_valley_scene, valley_scene
+    out = {}
+    for name, sc in (("stage_inflow", inflow_valley_scene(5.0)), ("transmissive_only", valley_scene(5.0))):
+        ts = [t for _, _, t in sc.designs(64)]
+        g.run_batch(sc.params, ts, sc.monitors, want_depth=False)
+        runs = g.run_batch(sc.params, ts, sc.monitors, want_depth=False)
+        t = g.last_timing()
+        cs = sum(r.cell_updates for r in runs)
+        out[name] = {"ms": t["kernel_ms"], "cell_steps_per_s": cs / (t["kernel_ms"] / 1e3),
+                     "steps_per_design_mean": sum(r.steps for r in runs) / len(runs)}
+    out["workload"] = "valley 90x70 @5 m, 2400 s storm, 64 designs x 2 primitives, batched path"
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_setup(args.gpus)
     if rank != 0:
@@ -288,7 +308,7 @@ def main():
     ap.add_argument("--cluster", type=int, default=0, help="pin the cluster size (profiling; 0 = autotune)")
     ap.add_argument("--threads", type=int, default=0, help="pin the threads per CTA (profiling; 0 = autotune)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the config-4 adjoint summary")
-    ap.add_argument("--no-ladder", action="store_true", help="skip the config-3 uneven-batch summary")
+    ap.add_argument("--no-ladder", action="store_true", help="skip the config-3 uneven-batch and stage/inflow summaries")
     ap.add_argument("--workload", type=int, default=2, choices=[2, 5],
                     help="2: the bench workload; 5: the 1024x1024 scene (16 designs; measurement / profiling only)")
     ap.add_argument("--impl-path", default="auto", choices=["auto", "tiled", "plain"],
@@ -398,6 +418,7 @@ def main():
         plain = None if args.no_plain or world > 1 else plain_comparison(g, sc, terrs)
         adj = None if args.no_adjoint or world > 1 or args.duration is not None else adjoint_summary(g)
         lad = None if args.no_ladder or world > 1 or args.duration is not None else ladder_summary(g)
+        bnd = None if args.no_ladder or world > 1 or args.duration is not None else boundary_summary(g)
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(sc, terrs)
@@ -423,6 +444,7 @@ def main():
             "batched_over_plain": (value / world / plain["value"]) if plain else None,
             "adjoint": adj,
             "ladder": lad,
+            "boundaries": bnd,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
             "clocks": clk.summary(),

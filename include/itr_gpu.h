@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define ITR_GPU_ABI_VERSION 1
+#define ITR_GPU_ABI_VERSION 2
 
 typedef struct itr_ctx itr_ctx;
 
@@ -52,8 +52,9 @@ enum itr_run_status {
 };
 
 /* SolverParams (crates/itr-hydro/src/solver.rs:27-49). locked_dt and cfl_hard have no
- * counterpart here (baseline-locked dt is not part of the batch path); inflow_scale must
- * be 1, as the reference GPU backend requires (backend.rs:53-55). */
+ * counterpart here (baseline-locked dt is not part of the batch path). inflow_scale
+ * multiplies every inflow hydrograph as in fill_ghosts (boundary.rs:27); the reference GPU
+ * backend rejected values other than 1 (backend.rs:53-55), this one takes any. */
 typedef struct itr_params {
   double duration_s;
   double sync_interval_s;
@@ -67,7 +68,7 @@ typedef struct itr_params {
   double infil_capacity;    /* constant infiltration capacity [m/s]                      */
   double initial_depth;     /* used for designs whose h0 is NULL (init_state, solver.rs:287) */
   int32_t skip_dry;         /* dry-row skipping; bitwise-neutral (kernel.rs:605-612)     */
-  double inflow_scale;      /* must be 1.0                                               */
+  double inflow_scale;      /* factor on every inflow hydrograph (1.0 = as given)        */
 } itr_params;
 
 /* The shared TerrainBase<f32> of one call (terrain.rs:237-257): every design in a call
@@ -81,7 +82,22 @@ typedef struct itr_grid {
   const float* gn2;         /* nx*ny, g*n^2 (TerrainBase::gn2)                        */
   const uint8_t* bc;        /* 2*nx + 2*ny codes: north[nx], south[nx], west[ny], east[ny] */
   int64_t wet_count;        /* number of open cells (rain volume in the ledger)       */
+  /* Stage and inflow ghosts (Ghost::Stage / Ghost::Inflow, terrain.rs:121-129, filled by
+   * boundary.rs:43-50,66-71). Indexed like bc; read only at ITR_BC_STAGE / ITR_BC_INFLOW
+   * cells, so all may be NULL when bc has neither. Zero-initialise the struct otherwise. */
+  const double* bc_stage;   /* stage cells: water level above the terrain datum [m]   */
+  const int32_t* bc_hydro;  /* inflow cells: index of the cell's hydrograph           */
+  const double* bc_inv_len; /* inflow cells: 1 / length of the cell's segment [1/m]   */
+  int32_t n_hydro;          /* inflow hydrographs (Boundaries::hydrographs)           */
+  const int32_t* hydro_off; /* n_hydro+1 offsets into hydro_t / hydro_q               */
+  const double* hydro_t;    /* hydrograph points: time [s] (a Hyetograph, scenario.rs:526) */
+  const double* hydro_q;    /*                    discharge [m^3/s]                    */
 } itr_grid;
+
+/* Limits of the inflow tables: distinct (hydrograph, segment length) pairs over the inflow
+ * cells, and hydrograph points summed over those pairs. */
+#define ITR_MAX_INFLOW_GROUPS 8
+#define ITR_MAX_INFLOW_POINTS 64
 
 /* One candidate: the face jumps of its PreparedTerrain (lib.rs:177-194 packs the same
  * arrays). dzx[r*(nx+1) + f] is x-face f of row r (f = 0 and f = nx are the domain edges
@@ -94,6 +110,10 @@ typedef struct itr_design {
   const float* dzy2;        /* crest mode only, else NULL */
   const float* h0;          /* nx*ny initial depth, or NULL for params.initial_depth on open cells */
   double cut_m3, fill_m3;   /* earthwork volumes of the edit (J's earthwork term)      */
+  const double* z_edge;     /* 2*nx+2*ny, indexed like grid.bc: z level above the datum of the
+                               interior cell behind each boundary cell (PreparedTerrain::z_level,
+                               which the design's edit changes); required when grid.bc has
+                               stage cells (a stage ghost's depth is stage - z_edge), else NULL */
 } itr_design;
 
 /* Objective and abort rules (objective.rs:8-150, GuardObserver evaluator.rs:88-108).
@@ -212,7 +232,9 @@ int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_groups, cons
  * checkpoint_interval steps; the backward recomputes each segment and steps the discrete
  * adjoint back through it with the recorded dt sequence held fixed. results are the
  * forward's, as itr_gpu_run_batch gives them. Signed face mode only (ITR_UNSUPPORTED
- * otherwise); obj must have at least one asset. Device memory: checkpoints of 12 B per cell
+ * otherwise); obj must have at least one asset. With stage cells the stage ghosts' depths
+ * (stage - z_edge) are held fixed: the result is the derivative with respect to the face
+ * jumps alone. Device memory: checkpoints of 12 B per cell
  * per design per interval, a tape of checkpoint_interval states. */
 int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n_designs, const itr_design* designs,
                 const uint32_t* monitors, int32_t n_mon, const itr_objective* obj, int32_t checkpoint_interval,
@@ -229,8 +251,9 @@ int itr_gpu_last_vjp_timing(itr_ctx* ctx, double* forward_ms, double* backward_m
  * bits as itr_gpu_run_batch) for ONE design on scratch held in a static device array of
  * fixed size, reserved when the library's module loads; the call allocates nothing, on the
  * device or the host. Inputs and results are host buffers with run_batch's meaning;
- * there is no objective (j = 0, no aborts). Runs on the device's legacy default stream
- * and returns when the results are in the host buffers.
+ * there is no objective (j = 0, no aborts), and boundaries are walls or transmissive
+ * (stage and inflow cells, or inflow_scale other than 1, give ITR_UNSUPPORTED). Runs on
+ * the device's legacy default stream and returns when the results are in the host buffers.
  * Limits, rejected with ITR_INVALID_ARG and a message in err before any device work: */
 #define ITR_STATIC_MAX_POINTS 263169      /* (nx+1)*(ny+1), e.g. 512 x 512 cells      */
 #define ITR_STATIC_MAX_TILES 16384        /* ceil(nx/16) * ceil(ny/16)                 */

@@ -19,6 +19,11 @@
 //   * every branch (wet/dry, HLL upwinding, min/max of wave speeds, reconstruction clamps,
 //     infiltration cap, drying, q_min flush) takes the derivative of the side the forward
 //     took; sqrt(g h) has derivative 0 at h = 0; rcbrt(h) is differentiated as h^(-1/3).
+// Stage and inflow ghosts: the replay rebuilds them as the forward did (the step's start
+// time is on the tape); their adjoint folds back onto the interior cell through what the
+// ghost copies (a stage ghost's momentum, an inflow ghost's depth where it exceeds the
+// critical depth). The stage depths themselves (stage - z behind the edge) are held fixed:
+// the gradient is the one with respect to the face jumps alone.
 // Signed face mode (fidelity level 1) only.
 #pragma once
 #include "itr_plain.cuh"
@@ -30,11 +35,12 @@ struct AdjArgs {
   int nx, ny, n_designs;
   const float* wet;
   const float* gn2;
-  const uint8_t* bc;
+  const uint8_t* bc;                  // device codes (ghost_state)
+  const float* bh;                    // stage-ghost depths per design [2 nx + 2 ny], or NULL
   const float* dzx;                   // all designs, as the forward
   const float* dzy;
   const unsigned long long* n_steps;  // per design: steps of the forward run
-  const double* seg;                  // per design [K][2]: (dt, rain) of this segment's steps
+  const double* seg;                  // per design [K][3]: (dt, rain, t) of this segment's steps
   int K;
   unsigned long long step0;           // global index of the segment's first step
   const float* tape;                  // [K][n_designs][3][N]: state at step step0 + j
@@ -49,8 +55,11 @@ struct AdjArgs {
   int max_seeds;
 };
 
-// Padded cell (gx, gy) of a state [3][N] with ghost cells (boundary.rs:36-87), as plain_load.
-ITR_DEV void adj_load(const AdjArgs& A, const float* X, int gx, int gy, float& h, float& qx, float& qy) {
+// Padded cell (gx, gy) of a state [3][N] with ghost cells (boundary.rs:36-87), as plain_load:
+// bh = this design's stage depths, inf = the step's inflow group values (BND only).
+template <bool BND>
+ITR_DEV void adj_load(const AdjArgs& A, const float* X, int gx, int gy, float& h, float& qx, float& qy, const float* bh,
+                      const float2* inf) {
   const int nx = A.nx, ny = A.ny;
   const size_t N = (size_t)nx * ny;
   const bool ox = gx < 0 || gx >= nx, oy = gy < 0 || gy >= ny;
@@ -59,24 +68,65 @@ ITR_DEV void adj_load(const AdjArgs& A, const float* X, int gx, int gy, float& h
   const int sy = gy < 0 ? 0 : (gy >= ny ? ny - 1 : gy);
   const size_t i = (size_t)sy * nx + sx;
   h = X[i]; qx = X[N + i]; qy = X[2 * N + i];
-  if (ox) { const int code = gx < 0 ? A.bc[2 * nx + sy] : A.bc[2 * nx + ny + sy]; if (code == 0) qx = -qx; }
-  else if (oy) { const int code = gy < 0 ? A.bc[sx] : A.bc[nx + sx]; if (code == 0) qy = -qy; }
+  if (!BND) {
+    if (ox) { const int code = gx < 0 ? A.bc[2 * nx + sy] : A.bc[2 * nx + ny + sy]; if (code == 0) qx = -qx; }
+    else if (oy) { const int code = gy < 0 ? A.bc[sx] : A.bc[nx + sx]; if (code == 0) qy = -qy; }
+  } else if (ox || oy) {
+    const int p = ox ? (gx < 0 ? 2 * nx + sy : 2 * nx + ny + sy) : (gy < 0 ? sx : nx + sx);
+    const int code = A.bc[p];
+    const float hs = code == 2 ? bh[p] : 0.0f;
+    const float2 fi = code >= 3 ? inf[code - 3] : make_float2(0.0f, 0.0f);
+    if (ox) ghost_state<true>(code, h, qx, qy, hs, fi, gx < 0);
+    else ghost_state<false>(code, h, qx, qy, hs, fi, gy < 0);
+  }
+}
+
+// Inflow group values of a step at its start time t, into shared memory (BND only).
+template <bool BND>
+ITR_DEV void adj_inflow(const AdjArgs& A, double t, float2* inf) {
+  if (BND) {
+    if ((int)threadIdx.x < A.P.inflow.n) inf[threadIdx.x] = inflow_values(A.P.inflow, threadIdx.x, t, A.P.g);
+    __syncthreads();
+  }
+}
+
+// Adjoint of a stage or inflow ghost folded onto the interior cell behind it. (lh, lu, lv,
+// lc): adjoints of the ghost's (h, u, v, c) from its face; (hg, qxg, qyg, cg): the ghost's
+// state; hi: the interior depth; crit: the group's critical depth (inflow). A stage ghost
+// copies the momentum (u = qx t(hg), v = qy t(hg) with hg fixed); an inflow ghost's depth
+// max(hi, crit) follows hi where hi > crit, its discharge is fixed. Adds to the interior
+// cell's (h, qx, qy) adjoints.
+ITR_DEV void ghost_bwd(int code, float lh, float lu, float lv, float lc, float hg, float qxg, float qyg, float cg, float hi,
+                       float crit, float g, float heps2, float& ah, float& aqx, float& aqy) {
+  const float h2 = hg * hg, den = h2 + rmax(h2, heps2);
+  if (code == 2) {
+    const float t = (hg + hg) * rcp(den);
+    aqx += lu * t;
+    aqy += lv * t;
+  } else if (hi > crit) {
+    const float dtdh = h2 > heps2 ? -1.0f / h2 : 2.0f * (heps2 - h2) / (den * den);
+    ah += lh + (lu * qxg + lv * qyg) * dtdh + (cg > 0.0f ? lc * g * 0.5f / cg : 0.0f);
+  }
 }
 
 // ---- forward replay: x_{n+1} = F(x_n) with the recorded (dt, rain) ----
+template <bool BND>
 __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A, int j) {
   __shared__ float sh[18 * 18], su[18 * 18], sv[18 * 18], sc[18 * 18], sqx[18 * 18], sqy[18 * 18];
   __shared__ FaceF fx[16 * 17], fy[17 * 16];
+  __shared__ float2 sinf[kMaxInflow];
   const int d = blockIdx.z;
   if (A.step0 + j >= A.n_steps[d]) return;
   const int nx = A.nx, ny = A.ny;
   const size_t N = (size_t)nx * ny, SX = (size_t)ny * (nx + 1), SY = (size_t)(ny + 1) * nx;
   const float* X = A.tape + ((size_t)j * A.n_designs + d) * 3 * N;
   float* Y = const_cast<float*>(A.tape) + ((size_t)(j + 1) * A.n_designs + d) * 3 * N;
-  const double* sg = A.seg + ((size_t)d * A.K + j) * 2;
+  const double* sg = A.seg + ((size_t)d * A.K + j) * 3;
   const StepK k = step_consts(A.P, sg[0], sg[1]);
   const float* dzx = A.dzx + d * SX;
   const float* dzy = A.dzy + d * SY;
+  const float* bh = BND && A.bh ? A.bh + (size_t)d * (2 * nx + 2 * ny) : nullptr;
+  adj_inflow<BND>(A, sg[2], sinf);
   const int gx0 = blockIdx.x * kTile, gy0 = blockIdx.y * kTile;
   const int li = threadIdx.x;
   // global loads first (face jumps, wet / g n^2, halo), as k_plain_update
@@ -93,7 +143,7 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A,
   for (int e = li; e < 324; e += kTileThreads) {
     const int hx = e % 18, hy = e / 18;
     float h, qx, qy, u, v, c;
-    adj_load(A, X, gx0 - 1 + hx, gy0 - 1 + hy, h, qx, qy);
+    adj_load<BND>(A, X, gx0 - 1 + hx, gy0 - 1 + hy, h, qx, qy, bh, sinf);
     cell_vel(h, qx, qy, k.g, k.heps2, u, v, c);
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
   }
@@ -245,12 +295,14 @@ ITR_DEV void sources_bwd(float h, float qx, float qy, const FaceF& w, const Face
 // four faces' input adjoints (ghost sides folded back onto the interior cell).
 constexpr int kR = 20, kQ = 18;
 
+template <bool BND>
 __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int j) {
   __shared__ float sh[kR * kR], sqx[kR * kR], sqy[kR * kR], su[kR * kR], sv[kR * kR], sc[kR * kR];
   __shared__ FaceF fx[kQ * 19], fy[19 * kQ];           // forward faces of the 18x18 cells
   __shared__ float jx[kQ * 19], jy[19 * kQ];            // their jumps
   __shared__ float l1[3][kQ * kQ];                      // adjoint of (h1, qx1, qy1)
   __shared__ float bx[16 * 17][8], by[17 * 16][8];      // face input adjoints: L (h,u,v,c), R (h,u,v,c)
+  __shared__ float2 sinf[kMaxInflow];                   // the step's inflow group values
   const int d = blockIdx.z;
   const int nx = A.nx, ny = A.ny;
   const size_t N = (size_t)nx * ny, SX = (size_t)ny * (nx + 1), SY = (size_t)(ny + 1) * nx;
@@ -268,10 +320,12 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
     return;
   }
   const float* X = A.tape + ((size_t)j * A.n_designs + d) * 3 * N;
-  const double* sg = A.seg + ((size_t)d * A.K + j) * 2;
+  const double* sg = A.seg + ((size_t)d * A.K + j) * 3;
   const StepK k = step_consts(A.P, sg[0], sg[1]);
   const float* dzx = A.dzx + d * SX;
   const float* dzy = A.dzy + d * SY;
+  const float* bh = BND && A.bh ? A.bh + (size_t)d * (2 * nx + 2 * ny) : nullptr;
+  adj_inflow<BND>(A, sg[2], sinf);
   // 1. state and velocities of the 20x20 region; the face jumps and this thread's old
   //    gradient sums are loaded first, so all these loads are in flight together
   float jxa = 0.0f, jxb = 0.0f, jya = 0.0f, jyb = 0.0f;
@@ -297,7 +351,7 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
   for (int e = li; e < kR * kR; e += kTileThreads) {
     const int ix = e % kR, iy = e / kR;
     float h, qx, qy, u, v, c;
-    adj_load(A, X, gx0 - 2 + ix, gy0 - 2 + iy, h, qx, qy);
+    adj_load<BND>(A, X, gx0 - 2 + ix, gy0 - 2 + iy, h, qx, qy, bh, sinf);
     cell_vel(h, qx, qy, k.g, k.heps2, u, v, c);
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
   }
@@ -403,22 +457,47 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
       float lu = W[5] + E[1] + Nf[5] + Sf[1];
       float lv = W[6] + E[2] + Nf[6] + Sf[2];
       float lc = W[7] + E[3] + Nf[7] + Sf[3];
-      // ghosts: a wall mirrors the normal velocity, a transmissive edge copies the cell
-      if (gx == 0) { const float s = A.bc[2 * nx + gy] == 0 ? -1.0f : 1.0f; lh += W[0]; lu += s * W[1]; lv += W[2]; lc += W[3]; }
-      if (gx == nx - 1) { const float s = A.bc[2 * nx + ny + gy] == 0 ? -1.0f : 1.0f; lh += E[4]; lu += s * E[5]; lv += E[6]; lc += E[7]; }
-      if (gy == 0) { const float s = A.bc[gx] == 0 ? -1.0f : 1.0f; lh += Nf[0]; lu += Nf[1]; lv += s * Nf[2]; lc += Nf[3]; }
-      if (gy == ny - 1) { const float s = A.bc[nx + gx] == 0 ? -1.0f : 1.0f; lh += Sf[4]; lu += Sf[5]; lv += s * Sf[6]; lc += Sf[7]; }
-      // velocity map (numerics.rs:38-45): u = qx t(h), v = qy t(h), c = sqrt(g h)
+      // ghosts: a wall mirrors the normal velocity, a transmissive edge copies the cell; a
+      // stage or inflow ghost (BND) adds straight to the cell's (h, qx, qy) adjoints
       const int a = (ly + 2) * kR + lx + 2;
+      float gh = 0.0f, gqx = 0.0f, gqy = 0.0f;
+      auto fold = [&](int code, const float* L, int ga) {   // L: the ghost's (h, u, v, c) adjoints
+        const float crit = code >= 3 ? sinf[code - 3].y : 0.0f;
+        ghost_bwd(code, L[0], L[1], L[2], L[3], sh[ga], sqx[ga], sqy[ga], sc[ga], sh[a], crit, k.g, k.heps2, gh, gqx, gqy);
+      };
+      if (gx == 0) {
+        const int code = A.bc[2 * nx + gy];
+        if (BND && code >= 2) fold(code, W, a - 1);
+        else { const float s = code == 0 ? -1.0f : 1.0f; lh += W[0]; lu += s * W[1]; lv += W[2]; lc += W[3]; }
+      }
+      if (gx == nx - 1) {
+        const int code = A.bc[2 * nx + ny + gy];
+        if (BND && code >= 2) fold(code, E + 4, a + 1);
+        else { const float s = code == 0 ? -1.0f : 1.0f; lh += E[4]; lu += s * E[5]; lv += E[6]; lc += E[7]; }
+      }
+      if (gy == 0) {
+        const int code = A.bc[gx];
+        if (BND && code >= 2) fold(code, Nf, a - kR);
+        else { const float s = code == 0 ? -1.0f : 1.0f; lh += Nf[0]; lu += Nf[1]; lv += s * Nf[2]; lc += Nf[3]; }
+      }
+      if (gy == ny - 1) {
+        const int code = A.bc[nx + gx];
+        if (BND && code >= 2) fold(code, Sf + 4, a + kR);
+        else { const float s = code == 0 ? -1.0f : 1.0f; lh += Sf[4]; lu += Sf[5]; lv += s * Sf[6]; lc += Sf[7]; }
+      }
+      // velocity map (numerics.rs:38-45): u = qx t(h), v = qy t(h), c = sqrt(g h)
       const float h = sh[a], qx = sqx[a], qy = sqy[a], c = sc[a];
       const float h2 = h * h, den = h2 + rmax(h2, k.heps2);
       const float t = (h + h) * rcp(den);
       const float dtdh = h2 > k.heps2 ? -1.0f / h2 : 2.0f * (k.heps2 - h2) / (den * den);
       const int q = (ly + 1) * kQ + lx + 1;
       const size_t gi = (size_t)gy * nx + gx;
-      LO[gi] = lh + (lu * qx + lv * qy) * dtdh + (c > 0.0f ? lc * k.g * 0.5f / c : 0.0f) + l1[0][q];
-      LO[N + gi] = lu * t + l1[1][q];
-      LO[2 * N + gi] = lv * t + l1[2][q];
+      float oh = lh + (lu * qx + lv * qy) * dtdh + (c > 0.0f ? lc * k.g * 0.5f / c : 0.0f) + l1[0][q];
+      float oqx = lu * t + l1[1][q], oqy = lv * t + l1[2][q];
+      if (BND) { oh += gh; oqx += gqx; oqy += gqy; }
+      LO[gi] = oh;
+      LO[N + gi] = oqx;
+      LO[2 * N + gi] = oqy;
     }
   }
 }

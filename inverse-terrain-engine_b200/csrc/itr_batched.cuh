@@ -48,7 +48,8 @@ struct BatchArgs {
   int n_designs;
   const float* wet;   // nx*ny
   const float* gn2;   // nx*ny
-  const uint8_t* bc;  // north[nx], south[nx], west[ny], east[ny]
+  const uint8_t* bc;  // north[nx], south[nx], west[ny], east[ny]; device codes (ghost_state)
+  const float* bh;    // stage-ghost depths, n_designs * [2 nx + 2 ny] indexed like bc, or NULL
   const float* dzx;   // n_designs * ny*(nx+1)
   const float* dzy;   // n_designs * (ny+1)*nx
   const float* dzx2;  // crest only
@@ -75,14 +76,14 @@ ITR_DEV unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_sh
 // Shared-memory plan of one CTA. Every CTA of a cluster uses the plan of the largest band,
 // so an offset names the same array in every CTA (DSMEM maps local pointers to peers).
 struct SmemPlan {
-  size_t s4, s2, pk, bf, xb, bx, by, wsum, led, slot, red, mbar, pf, total;
+  size_t s4, s2, pk, bf, xb, bx, by, wsum, led, slot, red, mbar, inf, pf, total;
 };
 
 // Values staged per thread and row by the prefetch ring: south y-face jump, next row's
 // x-face jump, wet, g n^2 (+ the second jumps in crest mode).
 __host__ __device__ inline int prefetch_k(int crest) { return crest ? 6 : 4; }
 
-__host__ __device__ inline SmemPlan smem_plan(int nr_max, int nx, int S, int W, int nwarps, int crest = 0) {
+__host__ __device__ inline SmemPlan smem_plan(int nr_max, int nx, int S, int W, int nwarps, int crest = 0, int bnd = 0) {
   SmemPlan p;
   size_t n = (size_t)nr_max * nx, o = 0;
   p.s4 = o;   o += n * 16;                         // float4 h, qx, qy, u
@@ -101,14 +102,15 @@ __host__ __device__ inline SmemPlan smem_plan(int nr_max, int nx, int S, int W, 
   o = align_up(o, 16);
   p.red = o;  o += (size_t)nwarps * 8 * 8;         // f64 reductions at sync points
   p.mbar = o; o += 16;
+  p.inf = o;  o += bnd ? (size_t)2 * kMaxInflow * 8 : 0;   // float2 inflow values [2 parity][groups]
   o = align_up(o, 16);
   p.pf = o;   o += (size_t)2 * S * prefetch_k(crest) * 64 * W * 4;   // [2 slot][S][K][64W] floats
   p.total = align_up(o, 16);
   return p;
 }
 
-__host__ __device__ inline size_t batched_smem_bytes(int nr_max, int nx, int S, int W, int nwarps, int crest = 0) {
-  return smem_plan(nr_max, nx, S, W, nwarps, crest).total;
+__host__ __device__ inline size_t batched_smem_bytes(int nr_max, int nx, int S, int W, int nwarps, int crest = 0, int bnd = 0) {
+  return smem_plan(nr_max, nx, S, W, nwarps, crest, bnd).total;
 }
 
 // 4-byte asynchronous global->shared copy (cp.async, cached in L1), commit and wait.
@@ -180,6 +182,7 @@ struct Smem {
   unsigned* slot;  // [2] smax bits, [2] bad
   double* red;     // [nwarps][8]
   unsigned long long* mbar;
+  float2* INF;     // inflow group values [2 parity][kMaxInflow] (stage/inflow grids only)
   float* PF;       // prefetch ring, [2 slot][S][K][64W]
   int ncell, nbf, nxb;
 };
@@ -193,10 +196,27 @@ ITR_DEV Cell load_cell(const Smem& s, int idx) {
   return c;
 }
 
-// Ghost cells (boundary.rs:36-57): a wall mirrors the normal momentum (so the normal
-// velocity flips sign exactly), a transmissive edge copies the interior cell.
-ITR_DEV Cell ghost_x(Cell c, int code) { if (code == 0) { c.qx = -c.qx; c.u = -c.u; } return c; }
-ITR_DEV Cell ghost_y(Cell c, int code) { if (code == 0) { c.qy = -c.qy; c.v = -c.v; } return c; }
+// Ghost cells (boundary.rs:36-87) from the interior cell c behind them: a wall mirrors the
+// normal momentum (so the normal velocity flips sign exactly), a transmissive edge copies
+// the cell. BND (the grid has stage or inflow cells): a stage or inflow ghost takes its
+// state from ghost_state and its velocities and celerity from cell_vel, as every padded
+// cell's do in the reference's velocity pass. NX: across an x-normal face; pos: index in
+// bc / bh; inward_pos: west or north side.
+template <bool BND, bool NX>
+ITR_DEV Cell ghost_cell(Cell c, int code, const float* bh, int pos, const float2* inf, bool inward_pos, float g,
+                        float heps2) {
+  if (!BND || code < 2) {
+    if (code == 0) {
+      if (NX) { c.qx = -c.qx; c.u = -c.u; } else { c.qy = -c.qy; c.v = -c.v; }
+    }
+    return c;
+  }
+  const float hs = code == 2 ? bh[pos] : 0.0f;
+  const float2 fi = code >= 3 ? inf[code - 3] : make_float2(0.0f, 0.0f);
+  ghost_state<NX>(code, c.h, c.qx, c.qy, hs, fi, inward_pos);
+  cell_vel(c.h, c.qx, c.qy, g, heps2, c.u, c.v, c.c);
+  return c;
+}
 
 ITR_DEV Cell shfl_up_cell(Cell c) {
   Cell o;
@@ -320,7 +340,7 @@ ITR_DEV Face2 shfl_down_face2(const Face2& f) {
   return o;
 }
 
-template <bool CREST, bool CLUSTERED, int MAXT>
+template <bool CREST, bool CLUSTERED, int MAXT, bool BND>
 __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int C = A.C;
@@ -346,7 +366,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
 
   Smem sm;
   {
-    const SmemPlan pl = smem_plan(nr_max, nx, S, W, nwarps, CREST ? 1 : 0);
+    const SmemPlan pl = smem_plan(nr_max, nx, S, W, nwarps, CREST ? 1 : 0, BND ? 1 : 0);
     sm.S4 = reinterpret_cast<float4*>(smem_raw + pl.s4);
     sm.S2 = reinterpret_cast<float2*>(smem_raw + pl.s2);
     sm.PK = reinterpret_cast<float*>(smem_raw + pl.pk);
@@ -359,6 +379,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     sm.slot = reinterpret_cast<unsigned*>(smem_raw + pl.slot);
     sm.red = reinterpret_cast<double*>(smem_raw + pl.red);
     sm.mbar = reinterpret_cast<unsigned long long*>(smem_raw + pl.mbar);
+    sm.INF = reinterpret_cast<float2*>(smem_raw + pl.inf);
     sm.PF = reinterpret_cast<float*>(smem_raw + pl.pf);
     sm.ncell = nr_max * nx; sm.nbf = (S + 1) * nx; sm.nxb = 2 * S * W * 2;
   }
@@ -374,6 +395,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   const size_t oy0 = (size_t)d * (ny + 1) * nx + oc0, oy1 = (size_t)d * (ny + 1) * nx + oc1;
   const int bc_w = 2 * nx, bc_e = 2 * nx + ny, bc_n = 0, bc_s = nx, nbc = 2 * nx + 2 * ny;
   (void)nbc;   // used by the checked build's index checks
+  const float* const bh = BND ? A.bh + (size_t)d * nbc : nullptr;   // this design's stage depths
 
   // Prefetch ring: row r's operands for this thread's two columns are copied one row ahead.
   constexpr int K = CREST ? 6 : 4;
@@ -432,6 +454,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   for (int i = tid; i < 2 * S * K * vlanes; i += blockDim.x) sm.PF[i] = 0.0f;
   if (tid < 8) { sm.slot[tid] = 0u; sm.LED[tid] = 0.0; }
   if (tid == 0) mbar_init(sm.mbar, blockDim.x);
+  // inflow ghosts of step 0 (at t = 0); each later step's are written one step ahead
+  if (BND && wid == nwarps - 1 && lane < P.inflow.n) sm.INF[lane] = inflow_values(P.inflow, lane, 0.0, P.g);
   {
     double sw = s0_l;
 #pragma unroll
@@ -468,14 +492,21 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   const int xb_next = wis + 1 < W ? wis + 1 : 0;          // warp whose lane 0 holds col0 + 1 of lane 31
   const int xb_next_comp = wis + 1 < W ? 0 : 1;
 
+  const float2* inf_cur = sm.INF;   // this step's inflow group values (parity slot)
+  auto ghost_x = [&](const Cell& c, int pos, bool west) -> Cell {
+    return ghost_cell<BND, true>(c, A.bc[CK(pos, nbc, 13)], bh, pos, inf_cur, west, P.g_f, P.heps2_f);
+  };
+  auto ghost_y = [&](const Cell& c, int pos, bool north) -> Cell {
+    return ghost_cell<BND, false>(c, A.bc[CK(pos, nbc, 15)], bh, pos, inf_cur, north, P.g_f, P.heps2_f);
+  };
   // Loads the two cells of row lr (local) for this lane: interior cells, or the east ghost
   // for a lane whose column is nx (built from cell nx-1 and the east code of global row r).
   auto load_pair = [&](int lr, int r) -> Cell2 {
     Cell a{}, b{};
     if (cell0) a = load_cell(sm, lr * nx + col0);
-    else if (face0) a = ghost_x(load_cell(sm, lr * nx + nx - 1), A.bc[CK(bc_e + r, nbc, 13)]);
+    else if (face0) a = ghost_x(load_cell(sm, lr * nx + nx - 1), bc_e + r, false);
     if (cell1) b = load_cell(sm, lr * nx + col1);
-    else if (face1) b = ghost_x(load_cell(sm, lr * nx + nx - 1), A.bc[CK(bc_e + r, nbc, 13)]);
+    else if (face1) b = ghost_x(load_cell(sm, lr * nx + nx - 1), bc_e + r, false);
     return cell2_of(a, b);
   };
   // West neighbours of the lane's two cells in row lr: lane-1 by shuffle; lane 0 reads the
@@ -484,7 +515,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     Cell2 left = shfl_up_cell2(cur);
     if (lane == 0) {
       Cell a = cx(left), b = cy(left);
-      if (face0) a = col0 == 0 ? ghost_x(cx(cur), A.bc[CK(bc_w + r, nbc, 14)]) : load_cell(sm, lr * nx + col0 - 1);
+      if (face0) a = col0 == 0 ? ghost_x(cx(cur), bc_w + r, true) : load_cell(sm, lr * nx + col0 - 1);
       if (face1) b = load_cell(sm, lr * nx + col1 - 1);
       left = cell2_of(a, b);
     }
@@ -497,6 +528,12 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     StepK k = step_consts(P, pl.dt, pl.rain);
     k.exact = A.exact;
     const int sp = (int)(step & 1ull);
+    if (BND) {
+      inf_cur = sm.INF + sp * kMaxInflow;
+      // the next step's inflow ghosts, at its start time (slot read after this step's
+      // closing barrier; the other slot's readers finished before the previous one)
+      if (wid == nwarps - 1 && lane < P.inflow.n) sm.INF[(sp ^ 1) * kMaxInflow + lane] = inflow_values(P.inflow, lane, pl.t_new, P.g);
+    }
     float smax_l = 0.0f, infil_l = 0.0f, fix_l = 0.0f;
     bool bad_l = false;
     int par = 0;
@@ -517,8 +554,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       // the cells above the strip's first row: ghost, same CTA, or the CTA above
       Cell a0{}, a1{};
       if (top_dom) {
-        if (cell0) a0 = ghost_y(cx(cur), A.bc[CK(bc_n + col0, nbc, 15)]);
-        if (cell1) a1 = ghost_y(cy(cur), A.bc[CK(bc_n + col1, nbc, 15)]);
+        if (cell0) a0 = ghost_y(cx(cur), bc_n + col0, true);
+        if (cell1) a1 = ghost_y(cy(cur), bc_n + col1, true);
       } else if (r0 - 1 >= ra) {
         if (cell0) a0 = load_cell(sm, (lr0 - 1) * nx + col0);
         if (cell1) a1 = load_cell(sm, (lr0 - 1) * nx + col1);
@@ -600,8 +637,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
         fS_in = face2_of(sx, sy);
       } else {
         Cell b0{}, b1{};
-        if (cell0) b0 = ghost_y(cx(cur), A.bc[CK(bc_s + col0, nbc, 18)]);
-        if (cell1) b1 = ghost_y(cy(cur), A.bc[CK(bc_s + col1, nbc, 18)]);
+        if (cell0) b0 = ghost_y(cx(cur), bc_s + col0, false);
+        if (cell1) b1 = ghost_y(cy(cur), bc_s + col1, false);
         below = cell2_of(b0, b1);
       }
       // new faces and the cell update; every lane of the strip computes (lanes past the grid
@@ -698,16 +735,23 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
         const double ve = (double)sm.BX[(sp * 2 + 1) * nr_max + j] * dt_dy;   // east: outflow when m > 0
         if (ve > 0.0) dout += ve; else din -= ve;
       }
-      if (q == 0)
-        for (int j = lane; j < nx; j += 32) {
-          const double v = (double)sm.BY[(sp * 2 + 0) * nx + j] * dt_dx;
-          if (v > 0.0) din += v; else dout -= v;
+      // y_boundary (kernel.rs:452-472): a y-edge's mass fluxes are summed over the row first
+      // (FixedSum<f64>: lane (col + 1) & 15 in column order, then the pairwise tree, which
+      // the butterfly over lanes 0-15 reproduces), then split: the top edge is inflow when
+      // the net flux is > 0, the bottom edge outflow
+      for (int side = 0; side < 2; ++side) {
+        if (side == 0 ? q != 0 : q != C - 1) continue;
+        double acc16 = 0.0;
+        if (lane < 16)
+          for (int j = (lane + 15) & 15; j < nx; j += 16) acc16 += (double)sm.BY[(sp * 2 + side) * nx + j];
+#pragma unroll
+        for (int o = 1; o < 16; o <<= 1) acc16 += __shfl_xor_sync(0xffffffffu, acc16, o);
+        const double v = acc16 * dt_dx;
+        if (lane == 0) {
+          if (side == 0) { if (v > 0.0) din += v; else dout -= v; }
+          else { if (v > 0.0) dout += v; else din -= v; }
         }
-      if (q == C - 1)
-        for (int j = lane; j < nx; j += 32) {
-          const double v = (double)sm.BY[(sp * 2 + 1) * nx + j] * dt_dx;
-          if (v > 0.0) dout += v; else din -= v;
-        }
+      }
       di = warp_sum_d(di); df = warp_sum_d(df); din = warp_sum_d(din); dout = warp_sum_d(dout);
       if (lane == 0) { sm.LED[0] += di; sm.LED[1] += df; sm.LED[2] += din; sm.LED[3] += dout; }
     }

@@ -3,7 +3,9 @@
 //
 // Mirrors crates/itr-gpu/src/lib.rs: GpuSolver::new (:85) -> itr_gpu_create,
 // run_batch (:149) -> itr_gpu_run_batch, adapter_info (:126) -> itr_gpu_info, and the
-// rejections of unsupported inputs (:154-176, backend.rs:53-55) -> ITR_UNSUPPORTED.
+// input checks (:154-176) -> ITR_INVALID_ARG / ITR_UNSUPPORTED. The reference's rejections
+// of stage and inflow boundaries and of inflow_scale != 1 (:166-176, backend.rs:53-55) are
+// gone: build_boundaries and stage_depths pack them for the kernels.
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstring>
@@ -63,6 +65,7 @@ struct LaunchCfg {
   size_t smem = 0;
   bool ok = false;
   bool tiled = false;   // the measured choice was the tiled HBM path
+  bool bnd = false;     // the grid has stage or inflow cells (k_batched<..., BND>)
 };
 
 }  // namespace
@@ -149,23 +152,28 @@ static int fail(itr_ctx* c, int code, const char* fmt, ...) {
 // ------------------------------------------------------------------ kernels table ----
 typedef void (*BatchedFn)(const BatchArgs);
 
-static BatchedFn batched_fn(bool crest, bool clustered, int maxt) {
-#define PICK(CR, CL)                                                  \
-  if (maxt <= 256) return k_batched<CR, CL, 256>;                     \
-  if (maxt <= 512) return k_batched<CR, CL, 512>;                     \
-  if (maxt <= 768) return k_batched<CR, CL, 768>;                     \
-  return k_batched<CR, CL, 1024>;
-  if (crest) { if (clustered) { PICK(true, true) } else { PICK(true, false) } }
-  else { if (clustered) { PICK(false, true) } else { PICK(false, false) } }
+static BatchedFn batched_fn(bool crest, bool clustered, int maxt, bool bnd) {
+#define PICK(CR, CL, BD)                                              \
+  if (maxt <= 256) return k_batched<CR, CL, 256, BD>;                 \
+  if (maxt <= 512) return k_batched<CR, CL, 512, BD>;                 \
+  if (maxt <= 768) return k_batched<CR, CL, 768, BD>;                 \
+  return k_batched<CR, CL, 1024, BD>;
+  if (bnd) {
+    if (crest) { if (clustered) { PICK(true, true, true) } else { PICK(true, false, true) } }
+    else { if (clustered) { PICK(false, true, true) } else { PICK(false, false, true) } }
+  }
+  if (crest) { if (clustered) { PICK(true, true, false) } else { PICK(true, false, false) } }
+  else { if (clustered) { PICK(false, true, false) } else { PICK(false, false, false) } }
 #undef PICK
 }
 
 static int maxt_bucket(int T) { return T <= 256 ? 256 : T <= 512 ? 512 : T <= 768 ? 768 : 1024; }
 
 // Geometry of the batched kernel for (nx, ny) with C CTAs per design and about T threads.
-static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_target, bool crest) {
+static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_target, bool crest, bool bnd) {
   LaunchCfg c;
   c.C = C;
+  c.bnd = bnd;
   c.W = (nx + 1 + 63) / 64;   // warps per strip row; each lane holds two columns
   if (C < 1 || ny < C) return c;
   const int nr_min = ny / C, nr_max = (ny + C - 1) / C;
@@ -176,14 +184,14 @@ static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_targe
   c.S = S;
   c.T = S * 32 * c.W;
   if (c.T > 1024) return c;
-  c.smem = batched_smem_bytes(nr_max, nx, S, c.W, c.T / 32, crest ? 1 : 0);
+  c.smem = batched_smem_bytes(nr_max, nx, S, c.W, c.T / 32, crest ? 1 : 0, bnd ? 1 : 0);
   c.ok = c.smem <= ctx->smem_optin;
   return c;
 }
 
 static int launch_batched(itr_ctx* ctx, const BatchArgs& A, const LaunchCfg& cfg, int n_designs, bool set_attr = true) {
   const bool crest = A.mode == 1, clustered = cfg.C > 1;
-  BatchedFn fn = batched_fn(crest, clustered, maxt_bucket(cfg.T));
+  BatchedFn fn = batched_fn(crest, clustered, maxt_bucket(cfg.T), cfg.bnd);
   if (set_attr) CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   cudaLaunchConfig_t lc;
   memset(&lc, 0, sizeof(lc));
@@ -203,7 +211,7 @@ static int launch_batched(itr_ctx* ctx, const BatchArgs& A, const LaunchCfg& cfg
 }
 
 static int max_active_clusters(itr_ctx* ctx, const LaunchCfg& cfg, bool crest) {
-  BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T));
+  BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T), cfg.bnd);
   if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem) != cudaSuccess) return 0;
   cudaLaunchConfig_t lc;
   memset(&lc, 0, sizeof(lc));
@@ -223,11 +231,11 @@ static int max_active_clusters(itr_ctx* ctx, const LaunchCfg& cfg, bool crest) {
 }
 
 // Candidate configurations, best-first by a simple model: time ~ waves * work per CTA.
-static std::vector<LaunchCfg> candidates(itr_ctx* ctx, int nx, int ny, int n_designs, bool crest) {
+static std::vector<LaunchCfg> candidates(itr_ctx* ctx, int nx, int ny, int n_designs, bool crest, bool bnd) {
   std::vector<std::pair<double, LaunchCfg>> v;
   for (int C : {1, 2, 4, 8}) {
     for (int T : {256, 384, 512, 640, 768, 896, 1024}) {
-      LaunchCfg c = make_cfg(ctx, nx, ny, C, T, crest);
+      LaunchCfg c = make_cfg(ctx, nx, ny, C, T, crest, bnd);
       if (!c.ok) continue;
       bool dup = false;
       for (auto& e : v) if (e.second.C == c.C && e.second.T == c.T) dup = true;
@@ -287,12 +295,31 @@ static int check_inputs(itr_ctx* ctx, const itr_params* p, const itr_grid* g, in
   if (!(g->dx > 0.0) || !(g->dy > 0.0)) return fail(ctx, ITR_INVALID_ARG, "cell size must be positive");
   if (!g->wet || !g->gn2 || !g->bc) return fail(ctx, ITR_INVALID_ARG, "grid arrays wet, gn2, bc are required");
   if (g->mode != ITR_FACE_SIGNED && g->mode != ITR_FACE_CREST) return fail(ctx, ITR_INVALID_ARG, "unknown face mode %d", g->mode);
+  bool has_stage = false, has_inflow = false;
   for (int64_t i = 0; i < 2ll * g->nx + 2ll * g->ny; ++i) {
-    if (g->bc[i] == ITR_BC_STAGE) return fail(ctx, ITR_UNSUPPORTED, "Stage boundaries are not supported on the GPU backend");
-    if (g->bc[i] == ITR_BC_INFLOW) return fail(ctx, ITR_UNSUPPORTED, "Inflow boundaries are not supported on the GPU backend");
     if (g->bc[i] > ITR_BC_INFLOW) return fail(ctx, ITR_INVALID_ARG, "unknown boundary code %d", (int)g->bc[i]);
+    has_stage = has_stage || g->bc[i] == ITR_BC_STAGE;
+    has_inflow = has_inflow || g->bc[i] == ITR_BC_INFLOW;
   }
-  if (p->inflow_scale != 1.0) return fail(ctx, ITR_UNSUPPORTED, "inflow scaling is not supported on the GPU backend");
+  if (has_stage) {
+    if (!g->bc_stage) return fail(ctx, ITR_INVALID_ARG, "grid has stage cells but bc_stage is NULL");
+    for (int32_t d = 0; d < n; ++d)
+      if (!ds[d].z_edge) return fail(ctx, ITR_INVALID_ARG, "grid has stage cells but design %d has no z_edge", d);
+  }
+  if (has_inflow) {
+    if (!g->bc_hydro || !g->bc_inv_len || !g->hydro_off || g->n_hydro < 1)
+      return fail(ctx, ITR_INVALID_ARG, "grid has inflow cells but no inflow tables (bc_hydro, bc_inv_len, hydro_off, n_hydro)");
+    if (g->hydro_off[0] < 0) return fail(ctx, ITR_INVALID_ARG, "hydro_off[0] is negative");
+    for (int h = 0; h < g->n_hydro; ++h)
+      if (g->hydro_off[h + 1] < g->hydro_off[h]) return fail(ctx, ITR_INVALID_ARG, "hydro_off is not non-decreasing");
+    if (g->hydro_off[g->n_hydro] > 0 && (!g->hydro_t || !g->hydro_q)) return fail(ctx, ITR_INVALID_ARG, "hydrograph arrays are NULL");
+    for (int64_t i = 0; i < 2ll * g->nx + 2ll * g->ny; ++i) {
+      if (g->bc[i] != ITR_BC_INFLOW) continue;
+      if (g->bc_hydro[i] < 0 || g->bc_hydro[i] >= g->n_hydro) return fail(ctx, ITR_INVALID_ARG, "boundary cell %lld: hydrograph index %d out of range", (long long)i, g->bc_hydro[i]);
+      if (!(g->bc_inv_len[i] >= 0.0) || !std::isfinite(g->bc_inv_len[i])) return fail(ctx, ITR_INVALID_ARG, "boundary cell %lld: bad 1/length", (long long)i);
+    }
+    if (!std::isfinite(p->inflow_scale)) return fail(ctx, ITR_INVALID_ARG, "inflow_scale is not finite");
+  }
   if (!(p->duration_s >= 0.0) || !(p->sync_interval_s > 0.0) || !(p->cfl > 0.0) || !(p->dt_max_s > 0.0))
     return fail(ctx, ITR_INVALID_ARG, "duration, sync interval, cfl and dt_max must be positive");
   if (p->n_rain < 0 || p->n_rain > kMaxRain) return fail(ctx, ITR_INVALID_ARG, "hyetograph has %d points (max %d)", p->n_rain, kMaxRain);
@@ -335,7 +362,52 @@ static RunParams make_run_params(const itr_params* p, const itr_grid* g) {
   P.inv_dx_f = (float)(1.0 / g->dx); P.inv_dy_f = (float)(1.0 / g->dy);
   P.h_dry_f = (float)p->h_dry; P.heps2_f = (float)(p->h_eps * p->h_eps); P.q_min_f = (float)1e-30;
   P.nz = -0.0f;
+  P.inflow.n = 0;   // build_boundaries fills the groups
+  P.inflow.scale = p->inflow_scale;
   return P;
+}
+
+// Device boundary codes and inflow groups of a grid (boundary.rs:12-87): an inflow cell's
+// code becomes 3 + its group, a group being a distinct (hydrograph, 1 / segment length)
+// pair in boundary-cell order; other codes are copied. Stage depths are per design
+// (stage_depths).
+static int build_boundaries(itr_ctx* ctx, const itr_grid* g, Inflow& F, uint8_t* dbc) {
+  const int64_t nb = 2ll * g->nx + 2ll * g->ny;
+  int hyd[kMaxInflow];
+  int npts = 0;
+  F.n = 0;
+  F.off[0] = 0;
+  for (int64_t i = 0; i < nb; ++i) {
+    const uint8_t c = g->bc[i];
+    if (c != ITR_BC_INFLOW) { dbc[i] = c; continue; }
+    const int h = g->bc_hydro[i];
+    const double il = g->bc_inv_len[i];
+    int k = 0;
+    while (k < F.n && !(hyd[k] == h && F.inv_len[k] == il)) ++k;
+    if (k == F.n) {
+      if (F.n == kMaxInflow) return fail(ctx, ITR_UNSUPPORTED, "more than %d inflow groups (hydrograph, segment length)", kMaxInflow);
+      const int a = g->hydro_off[h], b = g->hydro_off[h + 1];
+      if (npts + (b - a) > kMaxInflowPts) return fail(ctx, ITR_UNSUPPORTED, "inflow hydrographs have more than %d points in all", kMaxInflowPts);
+      for (int j = a; j < b; ++j) { F.t[npts] = g->hydro_t[j]; F.q[npts] = g->hydro_q[j]; ++npts; }
+      hyd[k] = h;
+      F.inv_len[k] = il;
+      F.n += 1;
+      F.off[F.n] = npts;
+    }
+    dbc[i] = (uint8_t)(3 + k);
+  }
+  return ITR_OK;
+}
+
+// Stage-ghost depth of every boundary cell of one design, f32(max(stage - z, 0)) rounded
+// once from f64 (boundary.rs:45,68); 0 at other cells.
+static void stage_depths(const itr_grid* g, const double* z_edge, float* out) {
+  const int64_t nb = 2ll * g->nx + 2ll * g->ny;
+  for (int64_t i = 0; i < nb; ++i) {
+    if (g->bc[i] != ITR_BC_STAGE) { out[i] = 0.0f; continue; }
+    const double v = g->bc_stage[i] - z_edge[i];
+    out[i] = (float)(v > 0.0 ? v : 0.0);   // max(NaN, 0) is 0, as f64::max
+  }
 }
 
 // Host copy of the objective (objective.rs:94-128) for J and feasibility of a finished run.
@@ -460,6 +532,19 @@ int itr_gpu_last_timing(itr_ctx* ctx, double* kernel_ms, double* total_ms, uint6
 }  // extern "C"
 
 // ------------------------------------------------------------------ plain path ------
+// One step's update kernel of the tiled path: the ghost rule with stage and inflow cells
+// only where the grid has them.
+static void launch_update(const PlainArgs& A, dim3 grid, cudaStream_t st) {
+  const bool bnd = A.bh != nullptr || A.P.inflow.n > 0;
+  if (A.mode == 1) {
+    if (bnd) k_plain_update<true, true><<<grid, kTileThreads, 0, st>>>(A);
+    else k_plain_update<true, false><<<grid, kTileThreads, 0, st>>>(A);
+  } else {
+    if (bnd) k_plain_update<false, true><<<grid, kTileThreads, 0, st>>>(A);
+    else k_plain_update<false, false><<<grid, kTileThreads, 0, st>>>(A);
+  }
+}
+
 static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid, int* launches) {
   k_plain_init<<<1, 1024, 0, ctx->stream>>>(A);
   k_plain_finalize<<<1, 32, 0, ctx->stream>>>(A, n_blocks, 1);
@@ -468,8 +553,7 @@ static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid,
   PlainCtl* hctl = ctx->hout.as<PlainCtl>();
   for (uint64_t guard = 0;; ++guard) {
     for (int s = 0; s < ctx->steps_per_submit; ++s) {
-      if (A.mode == 1) k_plain_update<true><<<grid, kTileThreads, 0, ctx->stream>>>(A);
-      else k_plain_update<false><<<grid, kTileThreads, 0, ctx->stream>>>(A);
+      launch_update(A, grid, ctx->stream);
       k_plain_finalize<<<1, 32, 0, ctx->stream>>>(A, n_blocks, 0);
       *launches += 2;
     }
@@ -490,7 +574,7 @@ static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid,
 // Adjoint request: while set, run_batch takes the tiled path and records a tape.
 struct Vjp {
   int K;                                  // checkpoint interval (steps)
-  std::vector<std::vector<double>> dt;    // per design: (dt, rain) of every step taken
+  std::vector<std::vector<double>> dt;    // per design: (dt, rain, t) of every step taken
   uint64_t blocks = 0;                    // checkpoints written (one per block of K steps)
   double* gx;                             // host outputs
   double* gy;
@@ -509,8 +593,7 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
   if (tape) { tape->dt.assign(n, std::vector<double>()); tape->blocks = 0; }
   auto block = [&]() {
     for (int s = 0; s < K; ++s) {
-      if (A.mode == 1) k_plain_update<true><<<grid, kTileThreads, 0, st>>>(A);
-      else k_plain_update<false><<<grid, kTileThreads, 0, st>>>(A);
+      launch_update(A, grid, st);
       k_plain_finalize<<<n, 32, 0, st>>>(A, nb, 0);
     }
   };
@@ -541,16 +624,17 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
     cudaError_t e = cudaMemcpyAsync(hc, A.ctl, (size_t)n * sizeof(PlainCtl), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "tiled run: %s", cudaGetErrorString(e)); break; }
-    if (tape) {   // (dt, rain) of this block's steps, from the ring of 2K slots
+    if (tape) {   // (dt, rain, t) of this block's steps, from the ring of 2K slots
       double* ring = ctx->aRingH.as<double>();
-      e = cudaMemcpy(ring, A.dt_log, (size_t)n * 2 * K * 2 * 8, cudaMemcpyDeviceToHost);
+      e = cudaMemcpy(ring, A.dt_log, (size_t)n * 2 * K * 3 * 8, cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "tape: %s", cudaGetErrorString(e)); break; }
       const uint64_t s0 = polls * (uint64_t)K;
       for (int d = 0; d < n; ++d)
         for (uint64_t s = s0; s < s0 + K && s < hc[d].step; ++s) {
-          const double* q = ring + ((size_t)d * 2 * K + (size_t)(s % (2 * K))) * 2;
+          const double* q = ring + ((size_t)d * 2 * K + (size_t)(s % (2 * K))) * 3;
           tape->dt[d].push_back(q[0]);
           tape->dt[d].push_back(q[1]);
+          tape->dt[d].push_back(q[2]);
         }
     }
     bool all = true;
@@ -618,8 +702,8 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   CU(ctx->aTape.ensure((size_t)K * S3 * 4));
   CU(ctx->aLA.ensure(S3 * 4)); CU(ctx->aLB.ensure(S3 * 4));
   CU(ctx->aGx.ensure((size_t)n * SX * 8)); CU(ctx->aGy.ensure((size_t)n * SY * 8));
-  // (dt, rain) of every segment, laid out [segment][design][K][2], uploaded once
-  const size_t seg_elems = (size_t)n * K * 2;
+  // (dt, rain, t) of every segment, laid out [segment][design][K][3], uploaded once
+  const size_t seg_elems = (size_t)n * K * 3;
   CU(ctx->aSeg.ensure(nblocks * seg_elems * 8));
   CU(ctx->aRingH.ensure(nblocks * seg_elems * 8));
   CU(cudaMemsetAsync(ctx->aLA.p, 0, S3 * 4, st));
@@ -628,7 +712,7 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   AdjArgs A;
   memset(&A, 0, sizeof(A));
   A.P = F.P; A.nx = nx; A.ny = ny; A.n_designs = n;
-  A.wet = F.wet; A.gn2 = F.gn2; A.bc = F.bc; A.dzx = F.dzx; A.dzy = F.dzy;
+  A.wet = F.wet; A.gn2 = F.gn2; A.bc = F.bc; A.bh = F.bh; A.dzx = F.dzx; A.dzy = F.dzy;
   A.n_steps = ctx->aNst.as<unsigned long long>();
   A.seg = ctx->aSeg.as<double>(); A.K = K;
   A.tape = ctx->aTape.as<float>();
@@ -636,6 +720,7 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   A.seed_cell = ctx->aSeedC.as<unsigned>(); A.seed_state = ctx->aSeedS.as<unsigned>(); A.seed_w = ctx->aSeedW.as<float>();
   A.seed_n = ctx->aSeedN.as<int>(); A.max_seeds = ms;
   const dim3 grid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile, (unsigned)n);
+  const bool bnd = F.bh != nullptr || F.P.inflow.n > 0;   // stage or inflow ghosts
   float* lin = ctx->aLA.as<float>();
   float* lout = ctx->aLB.as<float>();
   double* segh = ctx->aRingH.as<double>();
@@ -644,19 +729,24 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
       for (int j = 0; j < K; ++j) {
         const uint64_t s = b * K + j;
         const bool have = s < nst[d];
-        double* q = segh + b * seg_elems + ((size_t)d * K + j) * 2;
-        q[0] = have ? V->dt[d][2 * s] : 0.0;
-        q[1] = have ? V->dt[d][2 * s + 1] : 0.0;
+        double* q = segh + b * seg_elems + ((size_t)d * K + j) * 3;
+        q[0] = have ? V->dt[d][3 * s] : 0.0;
+        q[1] = have ? V->dt[d][3 * s + 1] : 0.0;
+        q[2] = have ? V->dt[d][3 * s + 2] : 0.0;
       }
   CU(cudaMemcpyAsync(ctx->aSeg.p, segh, nblocks * seg_elems * 8, cudaMemcpyHostToDevice, st));
   for (uint64_t b = nblocks; b-- > 0;) {   // no host round trip between segments
     CU(cudaMemcpyAsync(ctx->aTape.p, ctx->aCkpt[b].p, S3 * 4, cudaMemcpyDeviceToDevice, st));
     A.step0 = b * K;
     A.seg = ctx->aSeg.as<double>() + b * seg_elems;
-    for (int j = 0; j + 1 < K; ++j) k_adj_replay<<<grid, kTileThreads, 0, st>>>(A, j);
+    for (int j = 0; j + 1 < K; ++j) {
+      if (bnd) k_adj_replay<true><<<grid, kTileThreads, 0, st>>>(A, j);
+      else k_adj_replay<false><<<grid, kTileThreads, 0, st>>>(A, j);
+    }
     for (int j = K - 1; j >= 0; --j) {
       A.lin = lin; A.lout = lout;
-      k_adj_step<<<grid, kTileThreads, 0, st>>>(A, j);
+      if (bnd) k_adj_step<true><<<grid, kTileThreads, 0, st>>>(A, j);
+      else k_adj_step<false><<<grid, kTileThreads, 0, st>>>(A, j);
       std::swap(lin, lout);
     }
     CU(cudaGetLastError());
@@ -778,11 +868,15 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   for (int d = 0; d < n; ++d) if (res[d].ledger && res[d].max_rows > max_rows) max_rows = res[d].max_rows;
   const int n_assets = ob ? ob->n_assets : 0, n_guard = ob ? ob->n_guard : 0;
   const int n_apos = ob && n_assets > 0 ? ob->asset_off[n_assets] : 0;
+  const size_t NB = 2 * (size_t)(nx + ny);   // boundary cells
+  bool has_stage = false;
+  for (size_t i = 0; i < NB; ++i) has_stage = has_stage || g->bc[i] == ITR_BC_STAGE;
 
   // ---- pack into pinned staging ----
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes, 256); return o; };
-  const size_t o_wet = take(N * 4), o_gn2 = take(N * 4), o_bc = take(2 * (size_t)(nx + ny));
+  const size_t o_wet = take(N * 4), o_gn2 = take(N * 4), o_bc = take(NB);
+  const size_t o_bh = has_stage ? take(n * NB * 4) : 0;
   const size_t o_dzx = take(n * SX * 4), o_dzy = take(n * SY * 4);
   const size_t o_dzx2 = crest ? take(n * SX * 4) : 0, o_dzy2 = crest ? take(n * SY * 4) : 0;
   const size_t o_h0 = take(n * N * 4), o_cut = take((size_t)n * 8), o_fill = take((size_t)n * 8);
@@ -794,7 +888,12 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   unsigned char* st = ctx->stage.as<unsigned char>();
   memcpy(st + o_wet, g->wet, N * 4);
   memcpy(st + o_gn2, g->gn2, N * 4);
-  memcpy(st + o_bc, g->bc, 2 * (size_t)(nx + ny));
+  RunParams P = make_run_params(p, g);
+  rc = build_boundaries(ctx, g, P.inflow, st + o_bc);
+  if (rc != ITR_OK) return rc;
+  const bool bnd = has_stage || P.inflow.n > 0;
+  if (has_stage)
+    for (int d = 0; d < n; ++d) stage_depths(g, ds[d].z_edge, reinterpret_cast<float*>(st + o_bh) + d * NB);
   const float hinit = (float)(p->initial_depth > 0.0 ? p->initial_depth : 0.0);
   for (int d = 0; d < n; ++d) {
     memcpy(st + o_dzx + d * SX * 4, ds[d].dzx, SX * 4);
@@ -830,7 +929,6 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   const size_t ctl_bytes = (size_t)n * sizeof(PlainCtl);
   CU(ctx->hout.ensure(out_bytes > ctl_bytes ? out_bytes : ctl_bytes));
 
-  RunParams P = make_run_params(p, g);
   DevObjective DO;
   memset(&DO, 0, sizeof(DO));
   if (ob) {
@@ -867,13 +965,14 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     cudaError_t e = ctx->tH.ensure((size_t)n * 2 * N * 4);
     if (e == cudaSuccess) e = ctx->tQX.ensure((size_t)n * 2 * N * 4);
     if (e == cudaSuccess) e = ctx->tQY.ensure((size_t)n * 2 * N * 4);
-    if (e == cudaSuccess) e = ctx->tpart.ensure((size_t)n * n_tiles * 5 * 8);
+    if (e == cudaSuccess) e = ctx->tpart.ensure((size_t)n * n_tiles * kPart * 8);
     if (e == cudaSuccess) e = ctx->tctl.ensure((size_t)n * sizeof(PlainCtl));
     memset(&A, 0, sizeof(A));
     A.P = P; A.nx = nx; A.ny = ny; A.mode = g->mode; A.n_designs = n;
     A.wet = reinterpret_cast<const float*>(dv + o_wet);
     A.gn2 = reinterpret_cast<const float*>(dv + o_gn2);
     A.bc = reinterpret_cast<const uint8_t*>(dv + o_bc);
+    A.bh = has_stage ? reinterpret_cast<const float*>(dv + o_bh) : nullptr;
     A.dzx = reinterpret_cast<const float*>(dv + o_dzx);
     A.dzy = reinterpret_cast<const float*>(dv + o_dzy);
     A.dzx2 = crest ? reinterpret_cast<const float*>(dv + o_dzx2) : nullptr;
@@ -898,6 +997,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.wet = reinterpret_cast<const float*>(dv + o_wet);
     A.gn2 = reinterpret_cast<const float*>(dv + o_gn2);
     A.bc = reinterpret_cast<const uint8_t*>(dv + o_bc);
+    A.bh = has_stage ? reinterpret_cast<const float*>(dv + o_bh) : nullptr;
     A.dzx = reinterpret_cast<const float*>(dv + o_dzx);
     A.dzy = reinterpret_cast<const float*>(dv + o_dzy);
     A.dzx2 = crest ? reinterpret_cast<const float*>(dv + o_dzx2) : nullptr;
@@ -917,15 +1017,15 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.exact = ctx->exact_special ? 1u : 0u;
     // launch configuration
     LaunchCfg cfg;
-    auto key = std::make_tuple(nx, ny, n, (int)g->mode);
+    auto key = std::make_tuple(nx, ny, n, (int)g->mode + (bnd ? 2 : 0));
     if (ctx->cluster > 0 || ctx->threads > 0) {
-      cfg = make_cfg(ctx, nx, ny, ctx->cluster > 0 ? ctx->cluster : 1, ctx->threads > 0 ? ctx->threads : 512, crest);
+      cfg = make_cfg(ctx, nx, ny, ctx->cluster > 0 ? ctx->cluster : 1, ctx->threads > 0 ? ctx->threads : 512, crest, bnd);
       if (!cfg.ok) return fail(ctx, ITR_UNSUPPORTED, "cluster=%d threads=%d does not fit a %dx%d grid in shared memory", ctx->cluster, ctx->threads, nx, ny);
     } else if (ctx->tuned.count(key)) {
       cfg = ctx->tuned[key];
       tiled = cfg.tiled;
     } else {
-      std::vector<LaunchCfg> cands = candidates(ctx, nx, ny, n, crest);
+      std::vector<LaunchCfg> cands = candidates(ctx, nx, ny, n, crest, bnd);
       if (cands.empty()) {
         tiled = true;   // a design needs more shared memory than 8 CTAs hold
       } else {
@@ -963,7 +1063,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     if (!tiled) {
       A.C = cfg.C; A.W = cfg.W; A.S = cfg.S;
       if (ctx->defer) {   // ladder group: the launch goes into the ladder's graph
-        BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T));
+        BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T), cfg.bnd);
         CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
         ctx->last_args = A; ctx->last_cfg = cfg; ctx->have_last = true;
         ctx->last_was_plain = false; ctx->last_was_tiled = false;
@@ -992,8 +1092,8 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     if (ctx->vjp) {
       const int K = ctx->vjp->K;
       CU(ctx->aTpk.ensure((size_t)n * N * 4));
-      CU(ctx->aRing.ensure((size_t)n * 2 * K * 2 * 8));
-      CU(ctx->aRingH.ensure((size_t)n * 2 * K * 2 * 8));
+      CU(ctx->aRing.ensure((size_t)n * 2 * K * 3 * 8));
+      CU(ctx->aRingH.ensure((size_t)n * 2 * K * 3 * 8));
       A.tpk = ctx->aTpk.as<unsigned>();
       A.dt_log = ctx->aRing.as<double>();
       A.max_log = 2 * K;
@@ -1015,7 +1115,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     CU(ctx->pPK.ensure(N * 4));
     dim3 grid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile);
     int nb = grid.x * grid.y;
-    CU(ctx->ppart.ensure((size_t)nb * 5 * 8));
+    CU(ctx->ppart.ensure((size_t)nb * kPart * 8));
     CU(ctx->pctl.ensure(sizeof(PlainCtl)));
     CU(cudaEventRecord(ctx->ev[1], ctx->stream));
     ctx->last_plain.clear();
@@ -1027,6 +1127,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
       A.wet = reinterpret_cast<const float*>(dv + o_wet);
       A.gn2 = reinterpret_cast<const float*>(dv + o_gn2);
       A.bc = reinterpret_cast<const uint8_t*>(dv + o_bc);
+      A.bh = has_stage ? reinterpret_cast<const float*>(dv + o_bh) + d * NB : nullptr;
       A.dzx = reinterpret_cast<const float*>(dv + o_dzx) + d * SX;
       A.dzy = reinterpret_cast<const float*>(dv + o_dzy) + d * SY;
       A.dzx2 = crest ? reinterpret_cast<const float*>(dv + o_dzx2) + d * SX : nullptr;

@@ -264,6 +264,87 @@ ITR_DEV double rain_integral_c(const Rain& R, double a, double b, RainCursor& cu
   return total;
 }
 
+// Inflow boundaries (Ghost::Inflow, boundary.rs:26-31,45-50,66-71). The inflow cells of a
+// grid fall into groups, one per distinct (hydrograph, 1 / segment length) pair; a group's
+// discharge per unit width q = rate(t) * inv_len * inflow_scale and its critical depth
+// (q^2/g)^(1/3) are the same for all its cells, so they are evaluated once per design and
+// step and the cells read them.
+constexpr int kMaxInflow = 8;       // groups
+constexpr int kMaxInflowPts = 64;   // hydrograph points over all groups
+
+struct Inflow {
+  int n;                        // groups (0: no inflow cells)
+  int off[kMaxInflow + 1];      // group g's hydrograph points are [off[g], off[g+1])
+  double inv_len[kMaxInflow];   // 1 / segment length [1/m]
+  double scale;                 // SolverParams::inflow_scale
+  double t[kMaxInflowPts];      // time [s]
+  double q[kMaxInflowPts];      // discharge [m^3/s]
+};
+
+// Real::rcbrt for f64 (crates/itr-core/src/real.rs:81-95): the f32 seed constant moved to
+// the f64 exponent and mantissa, then four short-chain Newton steps.
+ITR_DEV double rcbrt_d(double x) {
+  const unsigned long long K = 0x5540000000000000ull - (0x8782Bull << 29);
+  double r = __longlong_as_double((long long)(K - (unsigned long long)__double_as_longlong(x) / 3ull));
+  const double third = 1.0 / 3.0;
+  const double x3 = x * third;
+  const double c43 = 4.0 * third;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double r2 = r * r;
+    r = r * c43 - x3 * (r2 * r2);
+  }
+  return r;
+}
+
+// Hyetograph::rate (scenario.rs:561-570) over points [a, b) of the inflow table; the same
+// arithmetic as rain_rate.
+ITR_DEV double inflow_rate(const Inflow& F, int a, int b, double x) {
+  if (b <= a) return 0.0;
+  if (x <= F.t[a]) return F.q[a];
+  for (int k = a; k + 1 < b; ++k) {
+    if (x <= F.t[k + 1]) {
+      double t0 = F.t[k], r0 = F.q[k], t1 = F.t[k + 1], r1 = F.q[k + 1];
+      if (t1 == t0) return r1;
+      return r0 + (r1 - r0) * (x - t0) / (t1 - t0);
+    }
+  }
+  return F.q[b - 1];
+}
+
+// Group g at time t (the start of a step): x = f32 of the discharge per unit width q, and
+// y = f32 of the critical depth x * rcbrt(x) * rcbrt(x), x = q^2 / g, in f64 (boundary.rs:
+// 27-31). A ghost's depth is f32(max(h, crit)) = max(h, f32(crit)) since rounding is
+// monotone and h is already an f32; its normal discharge f32(+-q) = +-f32(q).
+ITR_DEV float2 inflow_values(const Inflow& F, int g, double t, double gacc) {
+  const double q = inflow_rate(F, F.off[g], F.off[g + 1], t) * F.inv_len[g] * F.scale;
+  const double x = q * q / gacc;
+  double crit = 0.0;
+  if (x > 0.0) {
+    const double r = rcbrt_d(x);
+    crit = x * r * r;
+  }
+  return make_float2((float)q, (float)crit);
+}
+
+// Ghost state from the interior cell (h, qx, qy) behind it (boundary.rs:36-87), for device
+// boundary codes: 0 wall (normal momentum mirrored), 1 transmissive (copy), 2 stage (the
+// design's stage depth hstage, momentum copied), 3 + g inflow group g (depth max(h, crit),
+// inward normal discharge, zero tangential discharge; inf = inflow_values of the group).
+// NX: the ghost lies across an x-normal face (west or east); inward_pos: west or north side.
+template <bool NX>
+ITR_DEV void ghost_state(int code, float& h, float& qx, float& qy, float hstage, float2 inf, bool inward_pos) {
+  if (code == 0) {
+    if (NX) qx = -qx; else qy = -qy;
+  } else if (code == 2) {
+    h = hstage;
+  } else if (code >= 3) {
+    h = h > inf.y ? h : inf.y;   // NaN h gives the critical depth, as f64::max does
+    const float qn = inward_pos ? inf.x : -inf.x;
+    if (NX) { qx = qn; qy = 0.0f; } else { qx = 0.0f; qy = qn; }
+  }
+}
+
 // Run-wide scalars of one call.
 struct RunParams {
   double duration, sync, cfl, dt_max, h_dry, h_eps, infil, initial_depth;
@@ -272,6 +353,7 @@ struct RunParams {
   int skip_dry;
   int rain_sorted;   // breakpoints non-decreasing in time: the cursor path is exact
   Rain rain;
+  Inflow inflow;
   // step-invariant f32 constants (solver.rs:269-285), rounded once on the host
   float g_f, g_half_f, inv_dx_f, inv_dy_f, h_dry_f, heps2_f, q_min_f;
   float nz;   // -0.0f, supplied at run time (see mul2)

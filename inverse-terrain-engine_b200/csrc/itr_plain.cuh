@@ -23,6 +23,11 @@ constexpr int kTile = 16;
 // 256 cells of the tile use the first 8 warps.
 constexpr int kTileThreads = 288;
 static_assert(kTileThreads >= 17 * 16, "one x-face and one y-face per thread");
+// Per-tile partial sums written by the update kernel: infiltration, positivity fix, x-edge
+// inflow and outflow volumes, volume (sync steps), and the top and bottom edges' summed
+// mass fluxes (signed: the reference nets a y-edge over its whole row before splitting it
+// into inflow and outflow, kernel.rs:452-472).
+constexpr int kPart = 7;
 // The update kernels ask for 6 resident blocks per SM (32 registers a thread): with the
 // 18x18 halo loads waiting on HBM, more resident warps beat fewer registers (measured +10%).
 
@@ -40,6 +45,7 @@ struct PlainCtl {
   unsigned smax_bits, bad;
   StepPlan pl;
   StepK k;
+  float2 inf[kMaxInflow];   // inflow groups at the step's start time (inflow_values)
 };
 
 struct PlainArgs {
@@ -47,7 +53,8 @@ struct PlainArgs {
   int nx, ny, mode;
   const float* wet;
   const float* gn2;
-  const uint8_t* bc;
+  const uint8_t* bc;  // device codes (ghost_state): 0 wall, 1 transmissive, 2 stage, 3 + inflow group
+  const float* bh;    // stage-ghost depths, per design [2 nx + 2 ny] indexed like bc; NULL without stage cells
   const float* dzx;   // design 0; design d at + d * ny * (nx + 1)
   const float* dzy;   //                         + d * (ny + 1) * nx
   const float* dzx2;
@@ -64,19 +71,19 @@ struct PlainArgs {
   float* QX;
   float* QY;
   float* PK;          // per design nx*ny
-  double* part;       // per design, per tile: [5] (infil, fix, in, out, vol)
+  double* part;       // per design, per tile: [kPart]
   PlainCtl* ctl;      // per design
   double* ledger;     // per design max_rows*8
   int max_rows;
   unsigned long long max_steps;
   unsigned* tpk;      // optional, per design nx*ny: index of the state that last raised PK
-  double* dt_log;     // optional, per design a ring of max_log (dt, rain): slot step % max_log
+  double* dt_log;     // optional, per design a ring of max_log (dt, rain, t): slot step % max_log
   int max_log;
 };
 
 // Pointers of design d inside a launch over n_designs designs.
 struct PlainDesign {
-  const float *dzx, *dzy, *dzx2, *dzy2, *h0;
+  const float *dzx, *dzy, *dzx2, *dzy2, *h0, *bh;
   float *H, *QX, *QY, *PK;
   double* part;
   PlainCtl* ctl;
@@ -92,19 +99,22 @@ ITR_DEV PlainDesign plain_design(const PlainArgs& A, int d, int n_tiles) {
   v.dzx = A.dzx + d * SX; v.dzy = A.dzy + d * SY;
   v.dzx2 = A.dzx2 ? A.dzx2 + d * SX : nullptr; v.dzy2 = A.dzy2 ? A.dzy2 + d * SY : nullptr;
   v.h0 = A.h0 + d * N;
+  v.bh = A.bh ? A.bh + (size_t)d * (2 * A.nx + 2 * A.ny) : nullptr;
   v.H = A.H + d * 2 * N; v.QX = A.QX + d * 2 * N; v.QY = A.QY + d * 2 * N;
   v.PK = A.PK + d * N;
-  v.part = A.part + (size_t)d * n_tiles * 5;
+  v.part = A.part + (size_t)d * n_tiles * kPart;
   v.ctl = A.ctl + d;
   v.ledger = A.ledger ? A.ledger + (size_t)d * A.max_rows * 8 : nullptr;
   v.tpk = A.tpk ? A.tpk + d * N : nullptr;
-  v.dt_log = A.dt_log ? A.dt_log + (size_t)d * A.max_log * 2 : nullptr;
+  v.dt_log = A.dt_log ? A.dt_log + (size_t)d * A.max_log * 3 : nullptr;
   v.cut = A.cut_d ? A.cut_d[d] : A.cut;
   v.fill = A.fill_d ? A.fill_d[d] : A.fill;
   return v;
 }
 
-// Old state of padded cell (gx, gy) with ghost cells outside (boundary.rs:36-87).
+// Old state of padded cell (gx, gy) with ghost cells outside (boundary.rs:36-87). BND: the
+// grid has stage or inflow cells (ghost_state); without, only walls flip a sign.
+template <bool BND>
 ITR_DEV void plain_load(const PlainArgs& A, const PlainDesign& D, int par, int gx, int gy, float& h, float& qx, float& qy) {
   const int nx = A.nx, ny = A.ny;
   const bool ox = gx < 0 || gx >= nx, oy = gy < 0 || gy >= ny;
@@ -113,17 +123,27 @@ ITR_DEV void plain_load(const PlainArgs& A, const PlainDesign& D, int par, int g
   int sy = gy < 0 ? 0 : (gy >= ny ? ny - 1 : gy);
   size_t i = (size_t)par * nx * ny + (size_t)sy * nx + sx;
   h = D.H[i]; qx = D.QX[i]; qy = D.QY[i];
-  if (ox) { int code = gx < 0 ? A.bc[2 * nx + sy] : A.bc[2 * nx + ny + sy]; if (code == 0) qx = -qx; }
-  else if (oy) { int code = gy < 0 ? A.bc[sx] : A.bc[nx + sx]; if (code == 0) qy = -qy; }
+  if (!BND) {
+    if (ox) { int code = gx < 0 ? A.bc[2 * nx + sy] : A.bc[2 * nx + ny + sy]; if (code == 0) qx = -qx; }
+    else if (oy) { int code = gy < 0 ? A.bc[sx] : A.bc[nx + sx]; if (code == 0) qy = -qy; }
+  } else if (ox || oy) {
+    const int p = ox ? (gx < 0 ? 2 * nx + sy : 2 * nx + ny + sy) : (gy < 0 ? sx : nx + sx);
+    const int code = A.bc[p];
+    const float hs = code == 2 ? D.bh[p] : 0.0f;
+    const float2 fi = code >= 3 ? D.ctl->inf[code - 3] : make_float2(0.0f, 0.0f);
+    if (ox) ghost_state<true>(code, h, qx, qy, hs, fi, gx < 0);
+    else ghost_state<false>(code, h, qx, qy, hs, fi, gy < 0);
+  }
 }
 
-template <bool CREST>
+template <bool CREST, bool BND = false>
 __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArgs A) {
   __shared__ float sh[18 * 18], su[18 * 18], sv[18 * 18], sc[18 * 18], sqx[18 * 18], sqy[18 * 18];
   __shared__ FaceF fx[16 * 17], fy[17 * 16];
   __shared__ float wmax[kTileThreads / 32];
   __shared__ unsigned wbad[kTileThreads / 32];
   __shared__ double wsum[kTileThreads / 32][5];
+  __shared__ double yedge[2][kTile];   // mass flux of the tile's top-edge / bottom-edge faces per column
   const PlainDesign D = plain_design(A, blockIdx.z, gridDim.x * gridDim.y);
   const PlainCtl& cl = *D.ctl;
   if (cl.done) return;
@@ -149,10 +169,11 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArg
   const bool cv = li < 256 && gx < nx && gy < ny;
   const size_t gi = (size_t)gy * nx + gx;
   const float wet_c = cv ? A.wet[gi] : 0.0f, gn2_c = cv ? A.gn2[gi] : 0.0f, pk_c = cv ? D.PK[gi] : 0.0f;
+  if (li < 2 * kTile) yedge[li / kTile][li % kTile] = 0.0;
   for (int e = li; e < 324; e += kTileThreads) {
     int hx = e % 18, hy = e / 18;
     float h, qx, qy;
-    plain_load(A, D, par, gx0 - 1 + hx, gy0 - 1 + hy, h, qx, qy);
+    plain_load<BND>(A, D, par, gx0 - 1 + hx, gy0 - 1 + hy, h, qx, qy);
     float u, v, c;
     cell_vel(h, qx, qy, k.g, k.heps2, u, v, c);
     sh[e] = h; sqx[e] = qx; sqy[e] = qy; su[e] = u; sv[e] = v; sc[e] = c;
@@ -185,11 +206,11 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArg
     bad = o.bad;
     acc[0] = (double)o.infil; acc[1] = (double)o.fix;
     if (hits) acc[4] = (double)o.h;
-    // boundary faces (kernel.rs:435-472), per face
+    // boundary faces: x-edges split per face (kernel.rs:435-450), y-edges summed first
     if (gx == 0) { double v = (double)w.m * dt_dy; if (v > 0.0) acc[2] += v; else acc[3] -= v; }
     if (gx == nx - 1) { double v = (double)e.m * dt_dy; if (v > 0.0) acc[3] += v; else acc[2] -= v; }
-    if (gy == 0) { double v = (double)n.m * dt_dx; if (v > 0.0) acc[2] += v; else acc[3] -= v; }
-    if (gy == ny - 1) { double v = (double)s.m * dt_dx; if (v > 0.0) acc[3] += v; else acc[2] -= v; }
+    if (gy == 0) yedge[0][lx] = (double)n.m;
+    if (gy == ny - 1) yedge[1][lx] = (double)s.m;
   }
   // block reductions, fixed order
   float m = smax;
@@ -205,8 +226,11 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArg
     for (int w = 0; w < kTileThreads / 32; ++w) { mm = rmax(mm, wmax[w]); bb |= wbad[w]; for (int j = 0; j < 5; ++j) ss[j] += wsum[w][j]; }
     if (mm > 0.0f) atomicMax(&D.ctl->smax_bits, __float_as_uint(mm));
     if (bb) atomicOr(&D.ctl->bad, 1u);
-    double* p = D.part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 5;
+    double* p = D.part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kPart;
     for (int j = 0; j < 5; ++j) p[j] = ss[j];
+    double yt = 0.0, yb = 0.0;
+    for (int c = 0; c < kTile; ++c) { yt += yedge[0][c]; yb += yedge[1][c]; }
+    p[5] = yt; p[6] = yb;
   }
 }
 
@@ -219,11 +243,18 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
   if (c.done) return;
   if (!first) {
     // sum block partials in block order
-    double tot[5] = {0, 0, 0, 0, 0};
+    double tot[kPart] = {0, 0, 0, 0, 0, 0, 0};
     for (int b = lane; b < n_blocks; b += 32)
-      for (int j = 0; j < 5; ++j) tot[j] += D.part[(size_t)b * 5 + j];
-    for (int j = 0; j < 5; ++j)
+      for (int j = 0; j < kPart; ++j) tot[j] += D.part[(size_t)b * kPart + j];
+    for (int j = 0; j < kPart; ++j)
       for (int o = 16; o > 0; o >>= 1) tot[j] += __shfl_xor_sync(0xffffffffu, tot[j], o);
+    {   // y_boundary (kernel.rs:452-472): the top edge is inflow when its net flux is > 0,
+        // the bottom edge outflow
+      const double dt_dx = c.pl.dt * P.dx;
+      const double vt = tot[5] * dt_dx, vb = tot[6] * dt_dx;
+      if (vt > 0.0) tot[2] += vt; else tot[3] -= vt;
+      if (vb > 0.0) tot[3] += vb; else tot[2] -= vb;
+    }
     const double smax = (double)__uint_as_float(c.smax_bits);
     const unsigned badv = c.bad;
     __syncwarp();
@@ -287,13 +318,15 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
       if (c.done) return;
     }
   }
+  // inflow ghosts of the next step, at its start time c.t (fill_ghosts(t), solver.rs)
+  if (lane < P.inflow.n) c.inf[lane] = inflow_values(P.inflow, lane, c.t, P.g);
   if (lane == 0) {
     if (!(c.t < P.duration && c.sync_index < P.n_sync)) { c.done = 1; return; }
     if (c.step >= A.max_steps) { c.status = 4; c.done = 1; return; }
     c.pl = plan_step(P, c.t, c.sync_index, c.dt_cfl);
     if (D.dt_log) {   // ring of max_log entries, slot step mod max_log
       const size_t slot = (size_t)(c.step % (unsigned long long)A.max_log);
-      D.dt_log[2 * slot] = c.pl.dt; D.dt_log[2 * slot + 1] = c.pl.rain;
+      D.dt_log[3 * slot] = c.pl.dt; D.dt_log[3 * slot + 1] = c.pl.rain; D.dt_log[3 * slot + 2] = c.t;
     }
     c.k = step_consts(P, c.pl.dt, c.pl.rain);
   }

@@ -53,7 +53,7 @@ struct StaticLayout {
   static constexpr size_t MON = BC + al256(2 * kStaticPoints);
   static constexpr size_t MMAX = MON + al256(kStaticMon * 4);
   static constexpr size_t PART = MMAX + al256(kStaticMon * 8);
-  static constexpr size_t LEDGER = PART + al256(kStaticTiles * 5 * 8);
+  static constexpr size_t LEDGER = PART + al256(kStaticTiles * kPart * 8);
   static constexpr size_t CTL = LEDGER + al256(kStaticRows * 8 * 8);
   static constexpr size_t bytes = CTL + al256(sizeof(PlainCtl));
 };
@@ -217,7 +217,7 @@ extern "C" int itr_gpu_run_plain_static(int device, const itr_params* p, const i
   // atomics) and the per-tile partials. k_plain_init rewrites the control block and the
   // state and peak planes of plane 0 as well, so nothing survives from an earlier call.
   SCU(cudaMemsetAsync(ctl, 0, sizeof(PlainCtl), st));
-  SCU(cudaMemsetAsync(part, 0, (size_t)nb * 5 * 8, st));
+  SCU(cudaMemsetAsync(part, 0, (size_t)nb * kPart * 8, st));
 
   // ---- the plain forward (the launch sequence of the context path) ----
   PlainArgs A;

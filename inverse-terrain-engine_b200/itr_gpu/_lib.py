@@ -38,13 +38,15 @@ class Grid(C.Structure):
     _fields_ = [
         ("nx", C.c_int32), ("ny", C.c_int32), ("dx", C.c_double), ("dy", C.c_double), ("g", C.c_double),
         ("mode", C.c_int32), ("wet", _fp), ("gn2", _fp), ("bc", _u8p), ("wet_count", C.c_int64),
+        ("bc_stage", _dp), ("bc_hydro", _i32p), ("bc_inv_len", _dp), ("n_hydro", C.c_int32),
+        ("hydro_off", _i32p), ("hydro_t", _dp), ("hydro_q", _dp),
     ]
 
 
 class Design(C.Structure):
     _fields_ = [
         ("dzx", _fp), ("dzy", _fp), ("dzx2", _fp), ("dzy2", _fp), ("h0", _fp),
-        ("cut_m3", C.c_double), ("fill_m3", C.c_double),
+        ("cut_m3", C.c_double), ("fill_m3", C.c_double), ("z_edge", _dp),
     ]
 
 

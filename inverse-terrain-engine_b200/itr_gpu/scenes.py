@@ -131,6 +131,27 @@ def valley_scene(cell: float, seed: int = 20261203 + 1, design_seed: int = 7 + 1
     return Scene(name, base, params, obj, editable, geo, (80.0, 100.0, 240.0, 250.0), n_prims, 300.0, 1.0, design_seed)
 
 
+def inflow_valley_scene(cell: float, seed: int = 20261203 + 1, design_seed: int = 7 + 1, n_prims: int = 2,
+                        scale: float = 1.0) -> Scene:
+    """The configuration-1 valley driven from its boundaries, the case the reference's GPU
+    backend declined (lib.rs:166-176): an upstream inflow hydrograph across the valley floor
+    on the west edge, a side-channel inflow on part of the south edge, a tailwater stage on
+    the east edge and a stage on part of the north edge; light rain. Every kind of ghost
+    (wall, transmissive, stage, inflow; x- and y-normal) occurs."""
+    sc = valley_scene(cell, seed, design_seed, n_prims, name="inflow-valley")
+    fine = sc.base.fine
+    segs = [Segment("inflow", "west", (125.0, 225.0), hydrograph=[(0.0, 0.0), (600.0, 6.0 * scale), (1800.0, 2.0 * scale),
+                                                                    (2400.0, 0.5 * scale)]),
+            Segment("inflow", "south", (200.0, 260.0), hydrograph=[(0.0, 1.0 * scale), (1200.0, 3.0 * scale), (2400.0, 0.0)]),
+            Segment("stage", "east", stage_m=10.2),
+            Segment("stage", "north", (300.0, 450.0), stage_m=11.8),
+            Segment("transmissive", "south", (350.0, 450.0))]
+    base = TerrainBase(fine, 1, segs)
+    sc.base = base
+    sc.params.rain = Hyetograph.from_mm_h([(0, 0), (720, 20), (2400, 0)])
+    return sc
+
+
 def hills_field(seed: int):
     """Configuration-2 DEM as a function of (x, y) on a 600 x 480 m domain."""
     rng = np.random.default_rng(seed)

@@ -202,6 +202,11 @@ def _ptr(a, t):
     return a.ctypes.data_as(C.POINTER(t)) if a is not None else None
 
 
+def _z_edges(base, terrains):
+    """Per-design z levels behind the boundary cells, needed when the grid has stage cells."""
+    return [t.z_edge() for t in terrains] if getattr(base, "has_stage", False) else None
+
+
 class GpuSolver:
     """GpuSolver (lib.rs:62-373) on a B200 through libitr_gpu.so."""
 
@@ -260,7 +265,7 @@ class GpuSolver:
                                [t.dzx2 for t in terrains], [t.dzy2 for t in terrains],
                                [t.initial_depth(p.initial_depth, p.initial_stage) if p.initial_stage is not None else None for t in terrains],
                                [(t.cut_m3, t.fill_m3) for t in terrains], monitors, objective, baseline_max, guard_abort,
-                               incumbent, want_peak, want_depth, ledger_rows)
+                               incumbent, want_peak, want_depth, ledger_rows, z_edge=_z_edges(base, terrains))
 
     def vjp(self, p: SolverParams, terrains: list[PreparedTerrain], monitors: MonitorSet, objective: Objective,
             checkpoint_interval: int = 128, want_peak: bool = False) -> list[GpuRun]:
@@ -270,7 +275,7 @@ class GpuSolver:
                                [t.dzx2 for t in terrains], [t.dzy2 for t in terrains],
                                [t.initial_depth(p.initial_depth, p.initial_stage) if p.initial_stage is not None else None for t in terrains],
                                [(t.cut_m3, t.fill_m3) for t in terrains], monitors, objective, want_peak=want_peak,
-                               want_depth=True, vjp_interval=checkpoint_interval)
+                               want_depth=True, vjp_interval=checkpoint_interval, z_edge=_z_edges(base, terrains))
 
     def last_vjp_timing(self) -> dict:
         f, b = C.c_double(), C.c_double()
@@ -285,8 +290,26 @@ class GpuSolver:
                            _ptr(rain_t, C.c_double), _ptr(rain_r, C.c_double), len(p.rain.pts), p.infil_capacity,
                            p.initial_depth, 1 if p.skip_dry else 0, p.inflow_scale)
 
+    @staticmethod
+    def _grid(base, arr) -> "_lib.Grid":
+        """itr_grid of a TerrainBase, with its stage and inflow tables when it has such cells."""
+        wet, gn2, bc = arr(base.wet, np.float32), arr(base.gn2, np.float32), arr(base.bc, np.uint8)
+        Gd = _lib.Grid(base.nx, base.ny, base.dx, base.dy, base.g, base.mode, _ptr(wet, C.c_float), _ptr(gn2, C.c_float),
+                       _ptr(bc, C.c_uint8), base.wet_count)
+        if getattr(base, "has_stage", False):
+            Gd.bc_stage = _ptr(arr(base.bc_stage, np.float64), C.c_double)
+        if getattr(base, "has_inflow", False):
+            hy = base.hydrographs
+            Gd.bc_hydro = _ptr(arr(base.bc_inflow, np.int32), C.c_int32)
+            Gd.bc_inv_len = _ptr(arr(base.bc_inv_len, np.float64), C.c_double)
+            Gd.n_hydro = len(hy)
+            Gd.hydro_off = _ptr(arr(np.cumsum([0] + [len(h) for h in hy]), np.int32), C.c_int32)
+            Gd.hydro_t = _ptr(arr([q[0] for h in hy for q in h] or [0.0], np.float64), C.c_double)
+            Gd.hydro_q = _ptr(arr([q[1] for h in hy for q in h] or [0.0], np.float64), C.c_double)
+        return Gd
+
     def _pack(self, base, dzx, dzy, dzx2, dzy2, h0, vols, monitors: MonitorSet, objective, baseline_max, guard_abort,
-              incumbent, want_peak, want_depth, ledger_rows, keep: list) -> dict:
+              incumbent, want_peak, want_depth, ledger_rows, keep: list, z_edge=None) -> dict:
         """ctypes views of one batch (grid, designs, monitors, objective, result slots)."""
         n = len(dzx)
         nx, ny = base.nx, base.ny
@@ -296,9 +319,7 @@ class GpuSolver:
             keep.append(a)
             return a
 
-        wet, gn2, bc = arr(base.wet, np.float32), arr(base.gn2, np.float32), arr(base.bc, np.uint8)
-        Gd = _lib.Grid(nx, ny, base.dx, base.dy, base.g, base.mode, _ptr(wet, C.c_float), _ptr(gn2, C.c_float),
-                       _ptr(bc, C.c_uint8), base.wet_count)
+        Gd = self._grid(base, arr)
         D = (_lib.Design * max(n, 1))()
         for i in range(n):
             a = arr(dzx[i], np.float32)
@@ -307,8 +328,9 @@ class GpuSolver:
             b2 = arr(dzy2[i], np.float32) if dzy2 and dzy2[i] is not None else None
             hh = arr(h0[i], np.float32) if h0 and h0[i] is not None else None
             cut, fill = vols[i] if vols else (0.0, 0.0)
+            ze = arr(z_edge[i], np.float64) if z_edge and z_edge[i] is not None else None
             D[i] = _lib.Design(_ptr(a, C.c_float), _ptr(b, C.c_float), _ptr(a2, C.c_float), _ptr(b2, C.c_float),
-                               _ptr(hh, C.c_float), cut, fill)
+                               _ptr(hh, C.c_float), cut, fill, _ptr(ze, C.c_double))
         mon = arr(monitors.cells, np.uint32)
         nm = len(mon)
         O = None
@@ -370,13 +392,13 @@ class GpuSolver:
 
     def run_arrays(self, p: SolverParams, base, dzx, dzy, dzx2, dzy2, h0, vols, monitors: MonitorSet, objective=None,
                    baseline_max=None, guard_abort=False, incumbent=None, want_peak=False, want_depth=True, ledger_rows=0,
-                   vjp_interval: int | None = None):
+                   vjp_interval: int | None = None, z_edge=None):
         """run_batch on packed per-design arrays (the C ABI's own view); with vjp_interval,
         itr_gpu_vjp instead (the runs then carry dj_ddzx / dj_ddzy)."""
         keep = []   # keep numpy buffers alive for the call
         P = self._params(p, keep)
         b = self._pack(base, dzx, dzy, dzx2, dzy2, h0, vols, monitors, objective, baseline_max, guard_abort, incumbent,
-                       want_peak, want_depth, ledger_rows, keep)
+                       want_peak, want_depth, ledger_rows, keep, z_edge)
         n, nx, ny, O, R = b["n"], b["nx"], b["ny"], b["O"], b["R"]
         gx = gy = None
         if vjp_interval:
@@ -406,7 +428,8 @@ class GpuSolver:
             packs.append(self._pack(base, [t.dzx for t in ts], [t.dzy for t in ts], [t.dzx2 for t in ts], [t.dzy2 for t in ts],
                                     [t.initial_depth(p.initial_depth, p.initial_stage) if p.initial_stage is not None else None for t in ts],
                                     [(t.cut_m3, t.fill_m3) for t in ts], g["monitors"], g.get("objective"), g.get("baseline_max"),
-                                    g.get("guard_abort", False), g.get("incumbent"), want_peak, want_depth, 0, keep))
+                                    g.get("guard_abort", False), g.get("incumbent"), want_peak, want_depth, 0, keep,
+                                    _z_edges(base, ts)))
         total = sum(b["n"] for b in packs)
         R = (_lib.Result * total)()
         k = 0
@@ -438,8 +461,6 @@ class GpuBackend:
         return f"gpu ({self.solver.adapter_info()})"
 
     def run(self, p: SolverParams, terrains: list[PreparedTerrain], monitors: MonitorSet) -> list[BatchRun]:
-        if p.inflow_scale != 1.0:
-            raise UnsupportedError("inflow scaling is not supported on the GPU backend")
         cells = terrains[0].base.nx * terrains[0].base.ny if terrains else 0
         return [BatchRun(r.monitor_max, r.steps, r.steps * cells, r.bad)
                 for r in self.solver.run_batch(p, terrains, monitors, want_depth=False)]

@@ -80,8 +80,16 @@ class TerrainBase:
         self.wet = np.where(self.wall, 0.0, 1.0).astype(np.float32)
         self.gn2 = (G * nvals * nvals).astype(np.float32)
         self.wet_count = int((~self.wall).sum())
-        self.bc, self.bc_stage, self.hydrographs, self.bc_inflow = _boundaries(segments or [], self.nx, self.ny, self.dx, self.dy,
-                                                                              fine.z_ref)
+        (self.bc, self.bc_stage, self.hydrographs, self.bc_inflow,
+         self.bc_inv_len) = _boundaries(segments or [], self.nx, self.ny, self.dx, self.dy, fine.z_ref)
+
+    @property
+    def has_stage(self) -> bool:
+        return bool((self.bc == BC_STAGE).any())
+
+    @property
+    def has_inflow(self) -> bool:
+        return bool((self.bc == BC_INFLOW).any())
 
     def cell_area(self) -> float:
         return self.dx * self.dy
@@ -179,11 +187,20 @@ def _faces(fine, lv, mode, zc, zfine, rows_cols):
     return dzx, dzx2, dzy, dzy2
 
 
+def edge_values(a: np.ndarray) -> np.ndarray:
+    """Values of the interior cells behind the boundary cells, in boundary-code order:
+    north row, south row, west column, east column."""
+    return np.concatenate([a[0, :], a[-1, :], a[:, 0], a[:, -1]])
+
+
 def _boundaries(segs, nx, ny, dx, dy, z_ref):
-    """Boundaries::from_segments (terrain.rs:151-187) as per-side-cell codes."""
+    """Boundaries::from_segments (terrain.rs:151-187) as per-side-cell codes, with each
+    stage cell's level above the datum and each inflow cell's hydrograph index and
+    1 / segment length (0 for an empty segment)."""
     codes = {s: np.full(nx if s in ("north", "south") else ny, BC_WALL, dtype=np.uint8) for s in SIDES}
     stage = {s: np.zeros(len(codes[s])) for s in SIDES}
     inflow = {s: np.full(len(codes[s]), -1, dtype=np.int64) for s in SIDES}
+    inv_len = {s: np.zeros(len(codes[s])) for s in SIDES}
     hydros = []
     for sg in segs:
         n, d = (nx, dx) if sg.side in ("north", "south") else (ny, dy)
@@ -201,12 +218,15 @@ def _boundaries(segs, nx, ny, dx, dy, z_ref):
             hydros.append(list(sg.hydrograph))
             codes[sg.side][a:e] = BC_INFLOW
             inflow[sg.side][a:e] = len(hydros) - 1
+            len_m = (e - a if e > a else 0) * d
+            inv_len[sg.side][a:e] = 1.0 / len_m if len_m > 0.0 else 0.0
         else:
             raise ValueError(f"unknown boundary kind {sg.kind}")
     bc = np.concatenate([codes["north"], codes["south"], codes["west"], codes["east"]]).astype(np.uint8)
     st = np.concatenate([stage["north"], stage["south"], stage["west"], stage["east"]])
     inf = np.concatenate([inflow["north"], inflow["south"], inflow["west"], inflow["east"]])
-    return bc, st, hydros, inf
+    il = np.concatenate([inv_len["north"], inv_len["south"], inv_len["west"], inv_len["east"]])
+    return bc, st, hydros, inf, il
 
 
 @dataclass
@@ -278,6 +298,10 @@ class PreparedTerrain:
 
     def z_level(self) -> np.ndarray:
         return self.z
+
+    def z_edge(self) -> np.ndarray:
+        """z level of the cells behind the boundary cells (itr_design.z_edge)."""
+        return edge_values(self.z)
 
     def initial_depth(self, initial_depth: float, initial_stage: float | None = None) -> np.ndarray:
         """init_state (solver.rs:287-306): depth per cell, 0 on walls."""

@@ -252,8 +252,7 @@ extern "C" void orc_scene_run(void* h, int prec, int kernel, const int64_t* bbox
 }
 
 // ------------------------------------------------------------------ flat (f32) -----
-// A terrain described only by the packed arrays of the GPU ABI. Stage/inflow ghosts are
-// not representable here (walls and transmissive only), matching the GPU path's scope.
+// A terrain described only by the packed arrays of the GPU ABI (itr_grid, itr_design).
 template <class T> struct FlatT {
   FineTerrain fine;  // only z_ref (0) and nothing else is read
   TerrainBase<T> tb;
@@ -261,10 +260,19 @@ template <class T> struct FlatT {
 };
 using Flat = FlatT<float>;
 
+// Stage and inflow ghosts of a packed terrain: itr_grid's tables (indexed like bc) and one
+// design's z_edge (z level of the cell behind each boundary cell). NULL: walls and
+// transmissive edges only.
+struct FlatBnd {
+  const double* stage; const int32_t* hydro; const double* inv_len;
+  int n_hydro; const int32_t* off; const double* ht; const double* hq;
+  const double* z_edge;
+};
+
 template <class T, class W>
 static void flat_build(FlatT<T>& F, int64_t nx, int64_t ny, double dx, double dy, int mode, const W* wet,
                        const W* gn2, const uint8_t* bc, const W* dzx, const W* dzy,
-                       const W* dzx2, const W* dzy2) {
+                       const W* dzx2, const W* dzy2, const FlatBnd* fb = nullptr) {
   TerrainBase<T>& tb = F.tb;
   tb.fine = &F.fine; tb.level = 1; tb.dx = dx; tb.dy = dy; tb.g = G_ACC;
   tb.layout = Layout((size_t)nx, (size_t)ny);
@@ -286,7 +294,29 @@ static void flat_build(FlatT<T>& F, int64_t nx, int64_t ny, double dx, double dy
   tb.bnd.west.assign(ny, Ghost{}); tb.bnd.east.assign(ny, Ghost{});
   size_t q = 0;
   for (auto* v : {&tb.bnd.north, &tb.bnd.south, &tb.bnd.west, &tb.bnd.east})
-    for (Ghost& g : *v) g.kind = bc[q++];
+    for (Ghost& g : *v) {
+      g.kind = bc[q];
+      if (fb && g.kind == GH_STAGE) g.stage = fb->stage[q];
+      if (fb && g.kind == GH_INFLOW) { g.hydro = fb->hydro[q]; g.inv_len = fb->inv_len[q]; }
+      ++q;
+    }
+  if (fb) {
+    for (int h = 0; h < fb->n_hydro; ++h) {
+      Hyetograph hg;
+      hg.t.assign(fb->ht + fb->off[h], fb->ht + fb->off[h + 1]);
+      hg.r.assign(fb->hq + fb->off[h], fb->hq + fb->off[h + 1]);
+      tb.bnd.hydrographs.push_back(hg);
+    }
+    // z levels behind the boundary cells (a stage ghost's depth is stage - z); the flat
+    // terrain reads no other z
+    if (fb->z_edge) {
+      size_t k = 0;
+      for (int64_t c = 0; c < nx; ++c) tb.z[(size_t)c] = fb->z_edge[k++];
+      for (int64_t c = 0; c < nx; ++c) tb.z[(size_t)((ny - 1) * nx + c)] = fb->z_edge[k++];
+      for (int64_t r = 0; r < ny; ++r) tb.z[(size_t)(r * nx)] = fb->z_edge[k++];
+      for (int64_t r = 0; r < ny; ++r) tb.z[(size_t)(r * nx + nx - 1)] = fb->z_edge[k++];
+    }
+  }
   F.pt.base = &tb;
   F.pt.fx0 = tb.fx0; F.pt.fx1 = tb.fx1; F.pt.fy0 = tb.fy0; F.pt.fy1 = tb.fy1;
   for (int64_t r = 0; r < ny; ++r)
@@ -308,9 +338,13 @@ extern "C" void orc_flat_run(int kernel, int64_t nx, int64_t ny, double dx, doub
                   int n_assets, const int64_t* asset_off, const int64_t* asset_pos, const double* asset_thr,
                   const double* asset_w, const double* obj_f, int want_peak,
                   double* out_s, double* mon_max, double* mon_tmax, double* ledger, int max_rows,
-                  double* h_out, double* qx_out, double* qy_out, double* peak, double* peak_step) {
+                  double* h_out, double* qx_out, double* qy_out, double* peak, double* peak_step,
+                  const double* bc_stage, const int32_t* bc_hydro, const double* bc_inv_len, int n_hydro,
+                  const int32_t* hydro_off, const double* hydro_t, const double* hydro_q, const double* z_edge) {
   Flat F;
-  flat_build(F, nx, ny, dx, dy, mode, wet, gn2, bc, dzx, dzy, dzx2, dzy2);
+  FlatBnd fbd{bc_stage, bc_hydro, bc_inv_len, n_hydro, hydro_off, hydro_t, hydro_q, z_edge};
+  const bool extras = bc_stage || bc_hydro;
+  flat_build(F, nx, ny, dx, dy, mode, wet, gn2, bc, dzx, dzy, dzx2, dzy2, extras ? &fbd : nullptr);
   ObjIn oi; ObjIn* op = nullptr;
   if (obj_f) { make_obj(oi, n_mon, mon, n_guard, guard_pos, baseline, n_assets, asset_off, asset_pos, asset_thr, asset_w, obj_f); op = &oi; }
   Solver<float> S; S.p = make_params(pv, rain_t, rain_r, n_rain);
@@ -328,9 +362,13 @@ extern "C" void orc_flat_run64(int kernel, int64_t nx, int64_t ny, double dx, do
                   int n_assets, const int64_t* asset_off, const int64_t* asset_pos, const double* asset_thr,
                   const double* asset_w, const double* obj_f, int want_peak,
                   double* out_s, double* mon_max, double* mon_tmax, double* ledger, int max_rows,
-                  double* h_out, double* qx_out, double* qy_out, double* peak, double* peak_step) {
+                  double* h_out, double* qx_out, double* qy_out, double* peak, double* peak_step,
+                  const double* bc_stage, const int32_t* bc_hydro, const double* bc_inv_len, int n_hydro,
+                  const int32_t* hydro_off, const double* hydro_t, const double* hydro_q, const double* z_edge) {
   FlatT<double> F;
-  flat_build(F, nx, ny, dx, dy, mode, wet, gn2, bc, dzx, dzy, dzx2, dzy2);
+  FlatBnd fbd{bc_stage, bc_hydro, bc_inv_len, n_hydro, hydro_off, hydro_t, hydro_q, z_edge};
+  const bool extras = bc_stage || bc_hydro;
+  flat_build(F, nx, ny, dx, dy, mode, wet, gn2, bc, dzx, dzy, dzx2, dzy2, extras ? &fbd : nullptr);
   ObjIn oi; ObjIn* op = nullptr;
   if (obj_f) { make_obj(oi, n_mon, mon, n_guard, guard_pos, baseline, n_assets, asset_off, asset_pos, asset_thr, asset_w, obj_f); op = &oi; }
   Solver<double> S; S.p = make_params(pv, rain_t, rain_r, n_rain);

@@ -61,10 +61,12 @@ def lib():
     run_args = [_d, _d, _d, C.c_int, C.c_int, _u32, C.c_int, _i64, _d, C.c_int, _i64, _i64, _d, _d, _d]
     out_args = [C.c_int, _d, _d, _d, _d, C.c_int, _d, _d, _d, _d, _d]
     L.orc_scene_run.argtypes = [C.c_void_p, C.c_int, C.c_int, _i64, _d, C.c_double, C.c_double] + run_args + [_d] + out_args
+    _i32 = C.POINTER(C.c_int32)
+    bnd_args = [_d, _i32, _d, C.c_int, _i32, _d, _d, _d]
     L.orc_flat_run.argtypes = ([C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int, _f, _f, _u8, _f, _f, _f, _f, _f]
-                               + run_args + out_args)
+                               + run_args + out_args + bnd_args)
     L.orc_flat_run64.argtypes = ([C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int, _d, _d, _u8, _d, _d, _d, _d, _d]
-                                 + run_args + out_args)
+                                 + run_args + out_args + bnd_args)
     L.orc_flat_batch.restype = C.c_double
     L.orc_flat_batch.argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, _f, _f, _u8, _f, _f, _f, _d, _d,
                                  _d, C.c_int, C.c_int, _u32, _d, _d]
@@ -198,10 +200,37 @@ def _run(call, nx, ny, params, monitors, objective, baseline, incumbent, cut, fi
                 ledger=led[:min(n_rows, max_rows)].copy(), h=h, qx=qx, qy=qy, peak=pk, peak_step=ps)
 
 
+def bnd_dict(base, terrain):
+    """Stage and inflow tables of a TerrainBase (itr_grid) with one design's z_edge, or None
+    when the grid has walls and transmissive edges only."""
+    if not (getattr(base, "has_stage", False) or getattr(base, "has_inflow", False)):
+        return None
+    return dict(stage=base.bc_stage, hydro=base.bc_inflow, inv_len=base.bc_inv_len, hydros=base.hydrographs,
+                z_edge=terrain.z_edge())
+
+
+def _bnd_args(bnd, keep):
+    if bnd is None:
+        return (None, None, None, 0, None, None, None, None)
+    i32 = C.POINTER(C.c_int32)
+
+    def a(x, dt):
+        x = np.ascontiguousarray(x, dtype=dt)
+        keep.append(x)
+        return x
+    hy = bnd["hydros"]
+    off = a(np.cumsum([0] + [len(h) for h in hy]), np.int32)
+    ht = a([q[0] for h in hy for q in h] or [0.0], np.float64)
+    hq = a([q[1] for h in hy for q in h] or [0.0], np.float64)
+    return (P(a(bnd["stage"], np.float64), C.c_double), P(a(bnd["hydro"], np.int32), C.c_int32),
+            P(a(bnd["inv_len"], np.float64), C.c_double), len(hy), off.ctypes.data_as(i32), P(ht, C.c_double),
+            P(hq, C.c_double), P(a(bnd["z_edge"], np.float64), C.c_double))
+
+
 def flat_run(base_arrays, design, params, monitors, kernel=1, objective=None, baseline=None, incumbent=None,
-             want_peak=False, max_rows=256):
+             want_peak=False, max_rows=256, bnd=None):
     """f32 run on the packed arrays of the GPU ABI: base_arrays = (nx, ny, dx, dy, mode, wet, gn2, bc),
-    design = dict(dzx, dzy, dzx2, dzy2, h0, cut, fill)."""
+    design = dict(dzx, dzy, dzx2, dzy2, h0, cut, fill), bnd = bnd_dict(...) for stage / inflow cells."""
     nx, ny, dx, dy, mode, wet, gn2, bc = base_arrays
     keep = []
 
@@ -216,13 +245,14 @@ def flat_run(base_arrays, design, params, monitors, kernel=1, objective=None, ba
     bc = np.ascontiguousarray(bc, dtype=np.uint8)
     dzx, dzy, dzx2, dzy2, h0 = (f32(design.get(k)) for k in ("dzx", "dzy", "dzx2", "dzy2", "h0"))
     cut, fill = design.get("cut", 0.0), design.get("fill", 0.0)
+    ba = _bnd_args(bnd, keep)
     return _run(lambda *a: lib().orc_flat_run(kernel, nx, ny, dx, dy, mode, P(wet, C.c_float), P(gn2, C.c_float),
                                               P(bc, C.c_uint8), P(dzx, C.c_float), P(dzy, C.c_float), P(dzx2, C.c_float),
-                                              P(dzy2, C.c_float), P(h0, C.c_float), *a),
+                                              P(dzy2, C.c_float), P(h0, C.c_float), *a, *ba),
                 nx, ny, params, monitors, objective, baseline, incumbent, cut, fill, None, want_peak, max_rows, scene=False)
 
 
-def flat_run64(base_arrays, design, params, monitors, kernel=1, objective=None, want_peak=False, max_rows=256):
+def flat_run64(base_arrays, design, params, monitors, kernel=1, objective=None, want_peak=False, max_rows=256, bnd=None):
     """The f64 scalar oracle on the same packed arrays (face jumps taken as f64)."""
     nx, ny, dx, dy, mode, wet, gn2, bc = base_arrays
     keep = []
@@ -238,9 +268,10 @@ def flat_run64(base_arrays, design, params, monitors, kernel=1, objective=None, 
     bc = np.ascontiguousarray(bc, dtype=np.uint8)
     dzx, dzy, dzx2, dzy2, h0 = (f64(design.get(k)) for k in ("dzx", "dzy", "dzx2", "dzy2", "h0"))
     cut, fill = design.get("cut", 0.0), design.get("fill", 0.0)
+    ba = _bnd_args(bnd, keep)
     return _run(lambda *a: lib().orc_flat_run64(kernel, nx, ny, dx, dy, mode, P(wet, C.c_double), P(gn2, C.c_double),
                                                 P(bc, C.c_uint8), P(dzx, C.c_double), P(dzy, C.c_double), P(dzx2, C.c_double),
-                                                P(dzy2, C.c_double), P(h0, C.c_double), *a),
+                                                P(dzy2, C.c_double), P(h0, C.c_double), *a, *ba),
                 nx, ny, params, monitors, objective, None, None, cut, fill, None, want_peak, max_rows, scene=False)
 
 

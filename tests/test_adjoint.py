@@ -144,3 +144,58 @@ def test_primitive_gradient_vs_f64_finite_differences(gpu):
             worst = max(worst, rel)
             assert rel <= FD_REL_TOL, f"primitive {i} {name}: adjoint {grad[i, k]:.6e} vs finite difference {fd:.6e} ({rel:.3%})"
     print(f"worst relative error of dJ/d(height, width, length) vs f64 central differences: {worst:.3%}")
+
+
+def test_gradient_with_stage_and_inflow_vs_f64_finite_differences(gpu):
+    """Stage (east) and inflow (west, north) ghosts on the smooth fully wet case: the ghost
+    adjoints fold onto the interior cells (a stage ghost's momentum, an inflow ghost's depth
+    above the critical depth). The stage depths are held fixed, as the finite differences,
+    which perturb face jumps only, hold them."""
+    nx, ny = 24, 16
+    segs = [Segment("inflow", "west", (20.0, 60.0), hydrograph=[(0.0, 0.2), (60.0, 0.6), (120.0, 0.3)]),
+            Segment("inflow", "north", (30.0, 80.0), hydrograph=[(0.0, 0.1), (120.0, 0.4)]),
+            Segment("stage", "east", stage_m=1.5)]
+    base = synthetic_terrain(nx, ny, 5.0, lambda x, y: 2.0 - 0.01 * x + 0.2 * math.sin(y / 15.0) + 0.1 * math.cos(x / 20.0),
+                             n=0.03, segments=segs)
+    p = SolverParams(120.0, 30.0, rain=Hyetograph.from_mm_h([(0, 50), (60, 120), (120, 0)]), initial_depth=0.3)
+    t = PreparedTerrain(base)
+    cells = [5 * nx + 8, 9 * nx + 15, 12 * nx + 20, 2 * nx + 3]
+    probe = Objective(ObjectiveDef([Asset(f"a{i}", [c], 10.0) for i, c in enumerate(cells)], []))
+    r = gpu.run_batch(p, [t], probe.monitors)[0]
+    obj = Objective(ObjectiveDef([Asset(f"a{i}", [c], float(r.monitor_max[probe.monitors.position(c)]) - 0.004, 1.0 + i)
+                                  for i, c in enumerate(cells)], []))
+    run = gpu.vjp(p, [t], obj.monitors, obj, checkpoint_interval=16)[0]
+    gx, gy = run.dj_ddzx, run.dj_ddzy
+    assert np.all(np.isfinite(gx)) and np.all(np.isfinite(gy))
+    bnd = orc.bnd_dict(base, t)
+
+    def j(dzx=None, dzy=None):
+        d = design_dict(t, p)
+        if dzx is not None:
+            d["dzx"] = dzx
+        if dzy is not None:
+            d["dzy"] = dzy
+        o = orc.flat_run64(base_arrays(base), d, p, obj.monitors, bnd=bnd)
+        return obj.evaluate(o["monitor_max"], 0.0, 0.0)["j_risk"]
+
+    dzx0 = np.asarray(t.dzx, np.float64).reshape(ny, nx + 1)
+    dzy0 = np.asarray(t.dzy, np.float64).reshape(ny + 1, nx)
+    gxi = np.abs(gx.copy()); gxi[:, 0] = 0; gxi[:, nx] = 0
+    gyi = np.abs(gy.copy()); gyi[0, :] = 0; gyi[ny, :] = 0
+    picks = [("x", np.unravel_index(i, gx.shape)) for i in np.argsort(gxi, axis=None)[-3:]]
+    picks += [("y", np.unravel_index(i, gy.shape)) for i in np.argsort(gyi, axis=None)[-3:]]
+    # and the faces next to the ghost edges
+    picks += [("x", (8, 1)), ("x", (8, nx - 1)), ("y", (1, 10))]
+    worst = 0.0
+    for kind, idx in picks:
+        base_a = dzx0 if kind == "x" else dzy0
+        up, dn = base_a.copy(), base_a.copy()
+        up[idx] += FD_STEP_M; dn[idx] -= FD_STEP_M
+        fd = ((j(dzx=up) - j(dzx=dn)) if kind == "x" else (j(dzy=up) - j(dzy=dn))) / (2 * FD_STEP_M)
+        ad = gx[idx] if kind == "x" else gy[idx]
+        if abs(fd) < 1e-6 * max(np.abs(gx).max(), np.abs(gy).max()):
+            continue   # a face with no influence on J
+        rel = abs(ad - fd) / abs(fd)
+        worst = max(worst, rel)
+        assert rel <= FD_REL_TOL, f"{kind}-face {idx}: adjoint {ad:.6e} vs finite difference {fd:.6e} (rel {rel:.3%})"
+    print(f"stage/inflow case: worst relative error vs f64 central differences: {worst:.3%}")

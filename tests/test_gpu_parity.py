@@ -5,7 +5,8 @@ both sides the results are expected bit for bit: same step count and end time, s
 depth and same per-cell peak depth. The required tolerances (<= 1e-4 m peak depth,
 <= 1e-5 relative J) are asserted too, so a failure says which bar broke.
 Mirrors crates/itr-gpu/tests/gpu.rs (lake at rest, rain volume, CPU comparison, batch vs
-single, unsupported inputs rejected).
+single). gpu.rs:112-125's stage, inflow and inflow_scale cases, which the reference's GPU
+backend rejects, run here: tests/test_boundaries.py.
 """
 from __future__ import annotations
 
@@ -16,8 +17,7 @@ import pytest
 
 import oracle_ref as orc
 from helpers import assert_bitwise, base_arrays, design_dict
-from itr_gpu import (GpuSolver, Hyetograph, MonitorSet, PreparedTerrain, Segment, SolverParams, UnsupportedError,
-                     synthetic_terrain)
+from itr_gpu import GpuSolver, Hyetograph, MonitorSet, PreparedTerrain, Segment, SolverParams, synthetic_terrain
 from itr_gpu.scenes import valley_scene
 
 pytestmark = pytest.mark.gpu
@@ -183,21 +183,6 @@ def test_batch_matches_single_bitwise(gpu):
         assert_bitwise(batch[i].depth, single.depth, f"cand {i} depth")
         np.testing.assert_array_equal(batch[i].monitor_max, single.monitor_max)
     assert not np.array_equal(batch[0].depth, batch[1].depth)
-
-
-def test_unsupported_inputs_rejected(gpu):
-    # gpu.rs:112-125: Stage/Inflow boundaries and inflow scaling are declined ("unsupported here")
-    base = synthetic_terrain(16, 16, 1.0, lambda x, y: 0.0, n=0.03,
-                             segments=[Segment("inflow", "west", hydrograph=[(0.0, 1.0)])])
-    with pytest.raises(UnsupportedError):
-        gpu.run_batch(SolverParams(10.0, 5.0), [PreparedTerrain(base)], MonitorSet())
-    base = synthetic_terrain(16, 16, 1.0, lambda x, y: 0.0, n=0.03, segments=[Segment("stage", "north", stage_m=1.0)])
-    with pytest.raises(UnsupportedError):
-        gpu.run_batch(SolverParams(10.0, 5.0), [PreparedTerrain(base)], MonitorSet())
-    base = synthetic_terrain(16, 16, 1.0, lambda x, y: 0.0, n=0.03)
-    p = SolverParams(10.0, 5.0, inflow_scale=1.2)
-    with pytest.raises(UnsupportedError):
-        gpu.run_batch(p, [PreparedTerrain(base)], MonitorSet())
 
 
 @pytest.mark.parametrize("impl", ["batched", "tiled"])
