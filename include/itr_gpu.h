@@ -243,6 +243,40 @@ int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n_
 /* Device time of the last itr_gpu_vjp: taped forward (kernels and checkpoints) and backward. */
 int itr_gpu_last_vjp_timing(itr_ctx* ctx, double* forward_ms, double* backward_ms);
 
+/* ---- Designs as primitives, materialised on the device. ----
+ * The reference builds each candidate's face jumps on the host (DesignSpace::materialize,
+ * design.rs:316-385, then PreparedTerrain::apply_edit, terrain.rs:460-505) and uploads the
+ * full per-design jump arrays (lib.rs:177-194). itr_gpu_run_primitives takes the designs as
+ * primitives and builds dz, the edited cell levels, the face jumps and the earthwork
+ * volumes on the device (bit-identical to the host path), then runs itr_gpu_run_batch's
+ * forward. Fidelity level 1 (signed faces) only; the designs start from
+ * params.initial_depth (no per-design h0). */
+enum itr_prim_kind { ITR_PRIM_BERM = 0, ITR_PRIM_SWALE = 1, ITR_PRIM_CUT = 2, ITR_PRIM_MOUND = 3 };
+
+typedef struct itr_primitive {   /* Primitive (design.rs:84-93), already quantised */
+  int32_t kind;                  /* itr_prim_kind */
+  double cx, cy;                 /* centre, world coordinates [m] */
+  double length, width;          /* [m] */
+  double angle_deg;
+  double height;                 /* [m]; negative lowers the terrain */
+} itr_primitive;
+
+typedef struct itr_design_space {  /* DesignSpace (design.rs:189-200) over the grid's cells */
+  double origin_x, origin_y;       /* GeoTransform: west edge of column 0, north edge of row 0 */
+  const double* z;                 /* nx*ny re-based cell levels of the base terrain, walls at z_wall */
+  const uint8_t* wall;             /* nx*ny, 1 = wall */
+  const uint8_t* editable;         /* nx*ny, 1 = a design may change the cell */
+  double z_wall;
+  double max_abs_dz;               /* clamp of |dz| [m] */
+} itr_design_space;
+
+/* Designs d = 0..n_designs-1 are prims[prim_off[d] .. prim_off[d+1]). cut_m3 / fill_m3
+ * (n_designs each, may be NULL) receive the earthwork volumes computed on the device. */
+int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design_space* space,
+                           int32_t n_designs, const int32_t* prim_off, const itr_primitive* prims,
+                           const uint32_t* monitors, int32_t n_mon, const itr_objective* obj, itr_result* results,
+                           double* cut_m3, double* fill_m3);
+
 /* ---- Allocation-free plain forward. No reference counterpart. ----
  * For callers that cannot allocate device memory when they run a design: a process that
  * has committed the whole device to its own pool, a caller whose other streams must not be

@@ -23,6 +23,7 @@
 #include "itr_batched.cuh"
 #include "itr_plain.cuh"
 #include "itr_adjoint.cuh"
+#include "itr_design.cuh"
 
 using namespace itr;
 
@@ -82,6 +83,15 @@ struct Collect {
   int launches = 0;
 };
 
+// A batch given as primitives (itr_gpu_run_primitives): the device materialises each design's
+// jumps, stage depths and earthwork volumes from these before the forward.
+struct Mat {
+  const itr_design_space* space = nullptr;
+  std::vector<MatPrim> prims;
+  std::vector<MatDesign> des;
+  std::vector<itr_design> ds;   // placeholders; cut/fill filled in from the device
+};
+
 struct itr_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -106,6 +116,9 @@ struct itr_ctx {
   HostBuf aRingH;
   std::vector<DevBuf> aCkpt;
   struct Vjp* vjp = nullptr;
+  Mat* mat = nullptr;
+  DevBuf mDz, mZe;
+  HostBuf mVol;
   // ladder: one child context per grid group; a deferred run stops before its launch
   std::vector<itr_ctx*> children;
   bool defer = false;
@@ -303,7 +316,7 @@ static int check_inputs(itr_ctx* ctx, const itr_params* p, const itr_grid* g, in
   }
   if (has_stage) {
     if (!g->bc_stage) return fail(ctx, ITR_INVALID_ARG, "grid has stage cells but bc_stage is NULL");
-    for (int32_t d = 0; d < n; ++d)
+    for (int32_t d = 0; d < n && !ctx->mat; ++d)
       if (!ds[d].z_edge) return fail(ctx, ITR_INVALID_ARG, "grid has stage cells but design %d has no z_edge", d);
   }
   if (has_inflow) {
@@ -327,7 +340,7 @@ static int check_inputs(itr_ctx* ctx, const itr_params* p, const itr_grid* g, in
   if (n_mon < 0 || (n_mon > 0 && !mon)) return fail(ctx, ITR_INVALID_ARG, "monitor list is invalid");
   for (int32_t k = 0; k < n_mon; ++k)
     if ((int64_t)mon[k] >= (int64_t)g->nx * g->ny) return fail(ctx, ITR_INVALID_ARG, "monitor cell out of range");
-  for (int32_t d = 0; d < n; ++d) {
+  for (int32_t d = 0; d < n && !ctx->mat; ++d) {
     if (!ds[d].dzx || !ds[d].dzy) return fail(ctx, ITR_INVALID_ARG, "design %d has no face jumps", d);
     if (g->mode == ITR_FACE_CREST && (!ds[d].dzx2 || !ds[d].dzy2)) return fail(ctx, ITR_INVALID_ARG, "design %d: crest mode needs dzx2/dzy2", d);
   }
@@ -479,12 +492,14 @@ void itr_gpu_destroy(itr_ctx* ctx) {
                     &ctx->mon, &ctx->obj_i, &ctx->obj_d, &ctx->peak, &ctx->depth, &ctx->ledger, &ctx->out, &ctx->mmax,
                     &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
                     &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy,
-                    &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon})
+                    &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon,
+                    &ctx->mDz, &ctx->mZe})
     b->release();
   for (DevBuf& b : ctx->aCkpt) b.release();
   for (itr_ctx* c : ctx->children) itr_gpu_destroy(c);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   ctx->aRingH.release();
+  ctx->mVol.release();
   ctx->stage.release();
   ctx->hout.release();
   for (int i = 0; i < 4; ++i) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -883,6 +898,11 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   const size_t o_mon = take((size_t)(n_mon > 0 ? n_mon : 1) * 4);
   const size_t o_oi = take((size_t)(n_assets + 1 + n_apos + n_guard + 1) * 4);
   const size_t o_od = take((size_t)(2 * n_assets + (n_mon > 0 ? n_mon : 1)) * 8);
+  Mat* M = ctx->mat;   // designs as primitives: the space, primitives and boxes go up instead of jumps
+  const size_t o_mz = M ? take(N * 8) : 0, o_mw = M ? take(N) : 0, o_me = M ? take(N) : 0;
+  const size_t o_mst = M && has_stage ? take(NB * 8) : 0;
+  const size_t o_mp = M ? take((M->prims.size() > 0 ? M->prims.size() : 1) * sizeof(MatPrim)) : 0;
+  const size_t o_md = M ? take((size_t)n * sizeof(MatDesign)) : 0;
   const size_t in_bytes = off;
   CU(ctx->stage.ensure(in_bytes));
   unsigned char* st = ctx->stage.as<unsigned char>();
@@ -892,12 +912,22 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   rc = build_boundaries(ctx, g, P.inflow, st + o_bc);
   if (rc != ITR_OK) return rc;
   const bool bnd = has_stage || P.inflow.n > 0;
-  if (has_stage)
+  if (has_stage && !M)
     for (int d = 0; d < n; ++d) stage_depths(g, ds[d].z_edge, reinterpret_cast<float*>(st + o_bh) + d * NB);
+  if (M) {
+    memcpy(st + o_mz, M->space->z, N * 8);
+    memcpy(st + o_mw, M->space->wall, N);
+    memcpy(st + o_me, M->space->editable, N);
+    if (has_stage) memcpy(st + o_mst, g->bc_stage, NB * 8);
+    if (!M->prims.empty()) memcpy(st + o_mp, M->prims.data(), M->prims.size() * sizeof(MatPrim));
+    memcpy(st + o_md, M->des.data(), (size_t)n * sizeof(MatDesign));
+  }
   const float hinit = (float)(p->initial_depth > 0.0 ? p->initial_depth : 0.0);
   for (int d = 0; d < n; ++d) {
-    memcpy(st + o_dzx + d * SX * 4, ds[d].dzx, SX * 4);
-    memcpy(st + o_dzy + d * SY * 4, ds[d].dzy, SY * 4);
+    if (!M) {
+      memcpy(st + o_dzx + d * SX * 4, ds[d].dzx, SX * 4);
+      memcpy(st + o_dzy + d * SY * 4, ds[d].dzy, SY * 4);
+    }
     if (crest) { memcpy(st + o_dzx2 + d * SX * 4, ds[d].dzx2, SX * 4); memcpy(st + o_dzy2 + d * SY * 4, ds[d].dzy2, SY * 4); }
     float* h0 = reinterpret_cast<float*>(st + o_h0) + d * N;
     if (ds[d].h0) memcpy(h0, ds[d].h0, N * 4);
@@ -955,6 +985,39 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
 #endif
   CU(cudaMemcpyAsync(dv, st, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
   int launches = 0;
+  if (M) {   // materialise every design on the device; the volumes come back for J
+    CU(ctx->mDz.ensure((size_t)n * N * 8));
+    CU(ctx->mZe.ensure((size_t)n * N * 8));
+    CU(ctx->mVol.ensure((size_t)n * 2 * 8));
+    MatArgs MA;
+    memset(&MA, 0, sizeof(MA));
+    MA.nx = nx; MA.ny = ny; MA.n = n;
+    MA.ox = M->space->origin_x; MA.oy = M->space->origin_y; MA.dx = g->dx; MA.dy = g->dy;
+    MA.z_wall = M->space->z_wall; MA.max_abs_dz = M->space->max_abs_dz;
+    MA.z = reinterpret_cast<const double*>(dv + o_mz);
+    MA.wall = dv + o_mw; MA.editable = dv + o_me;
+    MA.prims = reinterpret_cast<const MatPrim*>(dv + o_mp);
+    MA.des = reinterpret_cast<const MatDesign*>(dv + o_md);
+    MA.dz = ctx->mDz.as<double>(); MA.ze = ctx->mZe.as<double>();
+    MA.dzx = reinterpret_cast<float*>(dv + o_dzx); MA.dzy = reinterpret_cast<float*>(dv + o_dzy);
+    MA.cut = reinterpret_cast<double*>(dv + o_cut); MA.fill = reinterpret_cast<double*>(dv + o_fill);
+    if (has_stage) {
+      MA.bc = g->bc ? dv + o_bc : nullptr;   // device codes: stage cells keep code 2
+      MA.stage = reinterpret_cast<const double*>(dv + o_mst);
+      MA.bh = reinterpret_cast<float*>(dv + o_bh);
+    }
+    const size_t faces = SX > SY ? SX : SY;
+    const size_t items = faces > NB ? faces : NB;
+    k_materialize<<<dim3((unsigned)((N + 255) / 256), (unsigned)n), 256, 0, ctx->stream>>>(MA);
+    k_mat_jumps<<<dim3((unsigned)((items + 255) / 256), (unsigned)n), 256, 0, ctx->stream>>>(MA);
+    k_mat_volumes<<<(n + 63) / 64, 64, 0, ctx->stream>>>(MA);
+    launches += 3;
+    double* hv = ctx->mVol.as<double>();
+    CU(cudaMemcpyAsync(hv, dv + o_cut, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(hv + n, dv + o_fill, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (int d = 0; d < n; ++d) { M->ds[d].cut_m3 = hv[d]; M->ds[d].fill_m3 = hv[n + d]; }
+  }
   const unsigned long long max_steps = 2000000000ull;
 
   // impl 2, or a grid no cluster shape can hold: the tiled batched path (state in HBM)
@@ -1250,6 +1313,88 @@ extern "C" int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_g
   ctx->launches = launches;
   ctx->have_last = false;
   return ITR_OK;
+}
+
+// ------------------------------------------------------------------ primitives -------
+// Primitive::segment (design.rs:95-106) on the host, with libm sin and cos as the reference.
+static MatPrim mat_prim(const itr_primitive& q) {
+  MatPrim m;
+  memset(&m, 0, sizeof(m));
+  m.kind = q.kind; m.width = q.width; m.height = q.height;
+  if (q.kind == ITR_PRIM_MOUND) {
+    m.x0 = m.x1 = q.cx; m.y0 = m.y1 = q.cy;
+  } else {
+    const double a = q.angle_deg * (3.141592653589793 / 180.0);   // f64::to_radians
+    const double sa = std::sin(a), ca = std::cos(a);
+    const double hl = 0.5 * q.length;
+    m.x0 = q.cx - ca * hl; m.y0 = q.cy - sa * hl; m.x1 = q.cx + ca * hl; m.y1 = q.cy + sa * hl;
+  }
+  return m;
+}
+
+static double nan_min(double a, double b) { if (a != a) return b; if (b != b) return a; return a < b ? a : b; }
+static double nan_max(double a, double b) { if (a != a) return b; if (b != b) return a; return a > b ? a : b; }
+
+// The union bounding box of a design's primitives in cells (materialize, design.rs:322-340).
+static MatDesign mat_box(const MatPrim* ps, int p0, int p1, const itr_design_space* sp, const itr_grid* g) {
+  const size_t nx = (size_t)g->nx, ny = (size_t)g->ny;
+  size_t c0 = SIZE_MAX, r0 = SIZE_MAX, c1 = 0, r1 = 0;
+  auto fl = [](double v) { v = std::floor(v); return v < 0 ? 0.0 : v; };
+  auto ce = [](double v) { v = std::ceil(v); return v < 0 ? 0.0 : v; };
+  for (int k = p0; k < p1; ++k) {
+    const MatPrim& p = ps[k];
+    if (p.height == 0.0) continue;
+    const double r = 0.5 * p.width;
+    const double bx0 = nan_min(p.x0, p.x1) - r, by0 = nan_min(p.y0, p.y1) - r;
+    const double bx1 = nan_max(p.x0, p.x1) + r, by1 = nan_max(p.y0, p.y1) + r;
+    const double fc0 = (bx0 - sp->origin_x) / g->dx, fr1 = (sp->origin_y - by0) / g->dy;
+    const double fc1 = (bx1 - sp->origin_x) / g->dx, fr0 = (sp->origin_y - by1) / g->dy;
+    const size_t a = std::min((size_t)fl(fc0), nx), b = std::min((size_t)fl(fr0), ny);
+    const size_t c = std::min((size_t)ce(fc1), nx), d = std::min((size_t)ce(fr1), ny);
+    if (a < c && b < d) { c0 = std::min(c0, a); r0 = std::min(r0, b); c1 = std::max(c1, c); r1 = std::max(r1, d); }
+  }
+  MatDesign m;
+  m.p0 = p0; m.p1 = p1;
+  if (c0 >= c1 || r0 >= r1) { m.c0 = m.r0 = m.c1 = m.r1 = 0; }
+  else { m.c0 = (int)c0; m.r0 = (int)r0; m.c1 = (int)c1; m.r1 = (int)r1; }
+  return m;
+}
+
+extern "C" int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design_space* sp,
+                                      int32_t n, const int32_t* prim_off, const itr_primitive* prims, const uint32_t* mon,
+                                      int32_t n_mon, const itr_objective* ob, itr_result* res, double* cut_m3, double* fill_m3) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (!g || !sp) return fail(ctx, ITR_INVALID_ARG, "grid and design space are required");
+  if (g->mode != ITR_FACE_SIGNED) return fail(ctx, ITR_UNSUPPORTED, "designs as primitives: signed faces (fidelity level 1) only");
+  if (!sp->z || !sp->wall || !sp->editable) return fail(ctx, ITR_INVALID_ARG, "design space arrays z, wall, editable are required");
+  if (!(sp->max_abs_dz >= 0.0)) return fail(ctx, ITR_INVALID_ARG, "max_abs_dz must be non-negative");
+  if (n < 0) return fail(ctx, ITR_INVALID_ARG, "negative design count");
+  if (n > 0 && !prim_off) return fail(ctx, ITR_INVALID_ARG, "prim_off is NULL");
+  if (n > 0 && prim_off[0] < 0) return fail(ctx, ITR_INVALID_ARG, "prim_off[0] is negative");
+  for (int d = 0; d < n; ++d)
+    if (prim_off[d + 1] < prim_off[d]) return fail(ctx, ITR_INVALID_ARG, "prim_off is not non-decreasing");
+  const int total = n > 0 ? prim_off[n] : 0;
+  if (total > 0 && !prims) return fail(ctx, ITR_INVALID_ARG, "prims is NULL");
+  Mat M;
+  M.space = sp;
+  M.prims.resize((size_t)total);
+  for (int k = prim_off[0]; k < total; ++k) {
+    if (prims[k].kind < ITR_PRIM_BERM || prims[k].kind > ITR_PRIM_MOUND) return fail(ctx, ITR_INVALID_ARG, "primitive %d: unknown kind %d", k, prims[k].kind);
+    if (!(prims[k].width > 0.0)) return fail(ctx, ITR_INVALID_ARG, "primitive %d: width must be positive", k);
+    M.prims[k] = mat_prim(prims[k]);
+  }
+  M.des.resize((size_t)n);
+  for (int d = 0; d < n; ++d) M.des[d] = mat_box(M.prims.data(), prim_off[d], prim_off[d + 1], sp, g);
+  M.ds.assign((size_t)n, itr_design{});
+  ctx->mat = &M;
+  const int rc = itr_gpu_run_batch(ctx, p, g, n, M.ds.data(), mon, n_mon, ob, res);
+  ctx->mat = nullptr;
+  if (rc == ITR_OK)
+    for (int d = 0; d < n; ++d) {
+      if (cut_m3) cut_m3[d] = M.ds[d].cut_m3;
+      if (fill_m3) fill_m3[d] = M.ds[d].fill_m3;
+    }
+  return rc;
 }
 
 extern "C" int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,

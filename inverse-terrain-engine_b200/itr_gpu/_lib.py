@@ -73,6 +73,20 @@ class Result(C.Structure):
     ]
 
 
+class Primitive(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("cx", C.c_double), ("cy", C.c_double), ("length", C.c_double), ("width", C.c_double),
+        ("angle_deg", C.c_double), ("height", C.c_double),
+    ]
+
+
+class DesignSpace(C.Structure):
+    _fields_ = [
+        ("origin_x", C.c_double), ("origin_y", C.c_double), ("z", _dp), ("wall", _u8p), ("editable", _u8p),
+        ("z_wall", C.c_double), ("max_abs_dz", C.c_double),
+    ]
+
+
 class Group(C.Structure):
     _fields_ = [
         ("grid", C.POINTER(Grid)), ("n_designs", C.c_int32), ("designs", C.POINTER(Design)),
@@ -95,6 +109,9 @@ SIGNATURES = {
     "itr_gpu_vjp": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.c_int32, C.POINTER(Design), _u32p,
                               C.c_int32, C.POINTER(Objective), C.c_int32, C.POINTER(Result), _dp, _dp]),
     "itr_gpu_last_vjp_timing": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "itr_gpu_run_primitives": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(DesignSpace), C.c_int32,
+                                         _i32p, C.POINTER(Primitive), _u32p, C.c_int32, C.POINTER(Objective),
+                                         C.POINTER(Result), _dp, _dp]),
     "itr_gpu_run_plain_static": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(Grid), C.POINTER(Design), _u32p,
                                            C.c_int32, C.POINTER(Result), C.c_char_p, C.c_size_t]),
 }

@@ -322,8 +322,8 @@ class GpuSolver:
         Gd = self._grid(base, arr)
         D = (_lib.Design * max(n, 1))()
         for i in range(n):
-            a = arr(dzx[i], np.float32)
-            b = arr(dzy[i], np.float32)
+            a = arr(dzx[i], np.float32) if dzx[i] is not None else None
+            b = arr(dzy[i], np.float32) if dzy[i] is not None else None
             a2 = arr(dzx2[i], np.float32) if dzx2 and dzx2[i] is not None else None
             b2 = arr(dzy2[i], np.float32) if dzy2 and dzy2[i] is not None else None
             hh = arr(h0[i], np.float32) if h0 and h0[i] is not None else None
@@ -415,6 +415,46 @@ class GpuSolver:
         runs = self._unpack(b, R, gx, gy)
         self.last_cell_updates = sum(r.cell_updates for r in runs)
         return runs
+
+    def run_primitives(self, p: SolverParams, base, designs, monitors: MonitorSet, editable, max_abs_dz: float,
+                       objective=None, baseline_max=None, guard_abort=False, incumbent=None, want_peak=False,
+                       want_depth=True, ledger_rows=0):
+        """run_batch with every design given as its primitives (itr_gpu_run_primitives): the
+        device materialises dz, the edited levels, the face jumps and the earthwork volumes
+        (DesignSpace::materialize + PreparedTerrain::apply_edit) for a level-1 TerrainBase.
+        Returns (runs, cut_m3, fill_m3)."""
+        if base.level != 1:
+            raise UnsupportedError("designs as primitives need a fidelity level 1 terrain")
+        if p.initial_stage is not None:
+            raise UnsupportedError("designs as primitives start from initial_depth (no initial stage)")
+        keep = []
+        P = self._params(p, keep)
+        n = len(designs)
+        b = self._pack(base, [None] * n, [None] * n, None, None, None, None, monitors, objective, baseline_max, guard_abort,
+                       incumbent, want_peak, want_depth, ledger_rows, keep)
+        flat = [q for d in designs for q in d]
+        prims = (_lib.Primitive * max(len(flat), 1))()
+        for k, q in enumerate(flat):
+            prims[k] = _lib.Primitive(int(q.kind), q.cx, q.cy, q.length, q.width, q.angle_deg, q.height)
+        off = np.ascontiguousarray(np.cumsum([0] + [len(d) for d in designs]), dtype=np.int32)
+        fine = base.fine
+        z = np.ascontiguousarray(base.z, dtype=np.float64)
+        wall = np.ascontiguousarray(base.wall, dtype=np.uint8)
+        ed = np.ascontiguousarray(editable, dtype=np.uint8)
+        keep += [off, z, wall, ed, prims]
+        S = _lib.DesignSpace(fine.geo.origin_x, fine.geo.origin_y, _ptr(z, C.c_double), _ptr(wall, C.c_uint8),
+                             _ptr(ed, C.c_uint8), fine.z_wall, max_abs_dz)
+        cut = np.zeros(max(n, 1))
+        fill = np.zeros(max(n, 1))
+        O = b["O"]
+        rc = self.lib.itr_gpu_run_primitives(self.ctx, C.byref(P), C.byref(b["Gd"]), C.byref(S), n, _ptr(off, C.c_int32),
+                                             prims, _ptr(b["mon"], C.c_uint32), b["nm"],
+                                             C.byref(O) if O is not None else None, b["R"], _ptr(cut, C.c_double),
+                                             _ptr(fill, C.c_double))
+        self._check(rc, "itr_gpu_run_primitives")
+        runs = self._unpack(b, b["R"])
+        self.last_cell_updates = sum(r.cell_updates for r in runs)
+        return runs, cut[:n], fill[:n]
 
     def run_ladder(self, p: SolverParams, groups: list[dict], want_peak=False, want_depth=False) -> list[list[GpuRun]]:
         """itr_gpu_run_ladder: several grid groups (each a dict with terrains, monitors and
