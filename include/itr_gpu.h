@@ -277,6 +277,19 @@ int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g,
                            const uint32_t* monitors, int32_t n_mon, const itr_objective* obj, itr_result* results,
                            double* cut_m3, double* fill_m3);
 
+/* The adjoint of itr_gpu_run_primitives' designs, closed on the device: dJ/d(height, width,
+ * length) of every primitive, dj_dprim[3 * (k - prim_off[0]) + {0, 1, 2}] for primitive
+ * prims[k], at fixed quantised centre and angle. The device runs itr_gpu_vjp's forward and backward on
+ * the materialised designs, forms dJ/d(dz) per cell from the face-jump gradients, and
+ * contracts it with central differences of the f64 materialisation (steps 1e-4 m in height,
+ * 1e-3 m in width and length: the profile is linear in height and C1 in width and length),
+ * adding the earthwork term's derivative earth_weight (cut_cost dV_cut + fill_cost dV_fill).
+ * dj_ddzx / dj_ddzy (may be NULL) receive the face-jump gradients as itr_gpu_vjp gives them. */
+int itr_gpu_vjp_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design_space* space,
+                           int32_t n_designs, const int32_t* prim_off, const itr_primitive* prims,
+                           const uint32_t* monitors, int32_t n_mon, const itr_objective* obj, int32_t checkpoint_interval,
+                           itr_result* results, double* dj_dprim, double* dj_ddzx, double* dj_ddzy);
+
 /* ---- Allocation-free plain forward. No reference counterpart. ----
  * For callers that cannot allocate device memory when they run a design: a process that
  * has committed the whole device to its own pool, a caller whose other streams must not be

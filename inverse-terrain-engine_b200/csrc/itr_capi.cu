@@ -117,7 +117,7 @@ struct itr_ctx {
   std::vector<DevBuf> aCkpt;
   struct Vjp* vjp = nullptr;
   Mat* mat = nullptr;
-  DevBuf mDz, mZe;
+  DevBuf mDz, mZe, mAux, mJp, mJob, mOut;
   HostBuf mVol;
   // ladder: one child context per grid group; a deferred run stops before its launch
   std::vector<itr_ctx*> children;
@@ -493,7 +493,7 @@ void itr_gpu_destroy(itr_ctx* ctx) {
                     &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
                     &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy,
                     &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon,
-                    &ctx->mDz, &ctx->mZe})
+                    &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut})
     b->release();
   for (DevBuf& b : ctx->aCkpt) b.release();
   for (itr_ctx* c : ctx->children) itr_gpu_destroy(c);
@@ -1360,10 +1360,9 @@ static MatDesign mat_box(const MatPrim* ps, int p0, int p1, const itr_design_spa
   return m;
 }
 
-extern "C" int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design_space* sp,
-                                      int32_t n, const int32_t* prim_off, const itr_primitive* prims, const uint32_t* mon,
-                                      int32_t n_mon, const itr_objective* ob, itr_result* res, double* cut_m3, double* fill_m3) {
-  if (!ctx) return ITR_INVALID_ARG;
+// Checks and host preparation of a batch of designs given as primitives.
+static int build_mat(itr_ctx* ctx, const itr_grid* g, const itr_design_space* sp, int32_t n, const int32_t* prim_off,
+                     const itr_primitive* prims, Mat& M) {
   if (!g || !sp) return fail(ctx, ITR_INVALID_ARG, "grid and design space are required");
   if (g->mode != ITR_FACE_SIGNED) return fail(ctx, ITR_UNSUPPORTED, "designs as primitives: signed faces (fidelity level 1) only");
   if (!sp->z || !sp->wall || !sp->editable) return fail(ctx, ITR_INVALID_ARG, "design space arrays z, wall, editable are required");
@@ -1375,7 +1374,6 @@ extern "C" int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const i
     if (prim_off[d + 1] < prim_off[d]) return fail(ctx, ITR_INVALID_ARG, "prim_off is not non-decreasing");
   const int total = n > 0 ? prim_off[n] : 0;
   if (total > 0 && !prims) return fail(ctx, ITR_INVALID_ARG, "prims is NULL");
-  Mat M;
   M.space = sp;
   M.prims.resize((size_t)total);
   for (int k = prim_off[0]; k < total; ++k) {
@@ -1386,8 +1384,18 @@ extern "C" int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const i
   M.des.resize((size_t)n);
   for (int d = 0; d < n; ++d) M.des[d] = mat_box(M.prims.data(), prim_off[d], prim_off[d + 1], sp, g);
   M.ds.assign((size_t)n, itr_design{});
+  return ITR_OK;
+}
+
+extern "C" int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design_space* sp,
+                                      int32_t n, const int32_t* prim_off, const itr_primitive* prims, const uint32_t* mon,
+                                      int32_t n_mon, const itr_objective* ob, itr_result* res, double* cut_m3, double* fill_m3) {
+  if (!ctx) return ITR_INVALID_ARG;
+  Mat M;
+  int rc = build_mat(ctx, g, sp, n, prim_off, prims, M);
+  if (rc != ITR_OK) return rc;
   ctx->mat = &M;
-  const int rc = itr_gpu_run_batch(ctx, p, g, n, M.ds.data(), mon, n_mon, ob, res);
+  rc = itr_gpu_run_batch(ctx, p, g, n, M.ds.data(), mon, n_mon, ob, res);
   ctx->mat = nullptr;
   if (rc == ITR_OK)
     for (int d = 0; d < n; ++d) {
@@ -1414,6 +1422,80 @@ extern "C" int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g,
   const int rc = itr_gpu_run_batch(ctx, p, g, n, ds, mon, n_mon, &o, res);
   ctx->vjp = nullptr;
   return rc;
+}
+
+extern "C" int itr_gpu_vjp_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design_space* sp,
+                                      int32_t n, const int32_t* prim_off, const itr_primitive* prims, const uint32_t* mon,
+                                      int32_t n_mon, const itr_objective* ob, int32_t checkpoint_interval, itr_result* res,
+                                      double* dj_dprim, double* dj_ddzx, double* dj_ddzy) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (n > 0 && !dj_dprim) return fail(ctx, ITR_INVALID_ARG, "dj_dprim is NULL");
+  Mat M;
+  int rc = build_mat(ctx, g, sp, n, prim_off, prims, M);
+  if (rc != ITR_OK) return rc;
+  if (n == 0) return ITR_OK;
+  const int nx = g->nx, ny = g->ny;
+  const size_t N = (size_t)nx * ny, SX = (size_t)ny * (nx + 1), SY = (size_t)(ny + 1) * nx;
+  std::vector<double> gxs, gys;
+  if (!dj_ddzx) { gxs.resize((size_t)n * SX); dj_ddzx = gxs.data(); }
+  if (!dj_ddzy) { gys.resize((size_t)n * SY); dj_ddzy = gys.data(); }
+  ctx->mat = &M;
+  rc = itr_gpu_vjp(ctx, p, g, n, M.ds.data(), mon, n_mon, ob, checkpoint_interval, res, dj_ddzx, dj_ddzy);
+  ctx->mat = nullptr;
+  if (rc != ITR_OK) return rc;
+  // central differences of the materialisation, one job per (primitive, parameter)
+  const double steps[3] = {1e-4, 1e-3, 1e-3};   // height, width, length
+  std::vector<MatPrim> jp;
+  std::vector<MatJob> jobs;
+  for (int d = 0; d < n; ++d)
+    for (int k = prim_off[d]; k < prim_off[d + 1]; ++k)
+      for (int j = 0; j < 3; ++j) {
+        MatJob J;
+        memset(&J, 0, sizeof(J));
+        J.design = d;
+        J.out = 3 * (k - prim_off[0]) + j;
+        J.twoh = 2.0 * steps[j];
+        for (int sgn = 0; sgn < 2; ++sgn) {
+          const int b0 = (int)jp.size();
+          for (int q = prim_off[d]; q < prim_off[d + 1]; ++q) {
+            itr_primitive v = prims[q];
+            if (q == k) {
+              const double h = sgn == 0 ? steps[j] : -steps[j];
+              if (j == 0) v.height += h; else if (j == 1) v.width += h; else v.length += h;
+            }
+            jp.push_back(mat_prim(v));
+          }
+          MatDesign B = mat_box(jp.data(), b0, (int)jp.size(), sp, g);
+          (sgn == 0 ? J.up : J.dn) = B;
+        }
+        jobs.push_back(J);
+      }
+  const cudaStream_t st = ctx->stream;
+  CU(ctx->mAux.ensure(2 * N));
+  CU(ctx->mJp.ensure((jp.size() > 0 ? jp.size() : 1) * sizeof(MatPrim)));
+  CU(ctx->mJob.ensure((jobs.size() > 0 ? jobs.size() : 1) * sizeof(MatJob)));
+  CU(ctx->mOut.ensure((jobs.size() > 0 ? jobs.size() : 1) * 8));
+  CU(ctx->mDz.ensure((size_t)n * N * 8));
+  CU(cudaMemcpyAsync(ctx->mAux.p, sp->editable, N, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ctx->mAux.as<uint8_t>() + N, sp->wall, N, cudaMemcpyHostToDevice, st));
+  if (!jp.empty()) CU(cudaMemcpyAsync(ctx->mJp.p, jp.data(), jp.size() * sizeof(MatPrim), cudaMemcpyHostToDevice, st));
+  if (!jobs.empty()) CU(cudaMemcpyAsync(ctx->mJob.p, jobs.data(), jobs.size() * sizeof(MatJob), cudaMemcpyHostToDevice, st));
+  double* gdz = ctx->mDz.as<double>();
+  k_mat_gdz<<<dim3((unsigned)((N + 255) / 256), (unsigned)n), 256, 0, st>>>(nx, ny, ctx->aGx.as<double>(), ctx->aGy.as<double>(),
+                                                                           ctx->mAux.as<uint8_t>() + N, gdz);
+  if (!jobs.empty()) {
+    MatArgs MA;
+    memset(&MA, 0, sizeof(MA));
+    MA.nx = nx; MA.ny = ny; MA.n = n;
+    MA.ox = sp->origin_x; MA.oy = sp->origin_y; MA.dx = g->dx; MA.dy = g->dy;
+    MA.z_wall = sp->z_wall; MA.max_abs_dz = sp->max_abs_dz;
+    MA.editable = ctx->mAux.as<uint8_t>();
+    k_mat_grad<<<(unsigned)jobs.size(), 256, 0, st>>>(MA, ctx->mJp.as<MatPrim>(), ctx->mJob.as<MatJob>(), gdz, ob->earth_weight,
+                                                      ob->cut_cost, ob->fill_cost, ctx->mOut.as<double>());
+    CU(cudaMemcpyAsync(dj_dprim, ctx->mOut.p, jobs.size() * 8, cudaMemcpyDeviceToHost, st));
+  }
+  CU(cudaStreamSynchronize(st));
+  return ITR_OK;
 }
 
 extern "C" int itr_gpu_last_vjp_timing(itr_ctx* ctx, double* forward_ms, double* backward_ms) {

@@ -160,4 +160,84 @@ __global__ void k_mat_volumes(const MatArgs M) {
   M.fill[d] = fill;
 }
 
+// ---- the design chain of the adjoint: dJ/d(height, width, length) per primitive ----
+// dJ/d(dz) per cell from the face-jump gradients (level 1: each interior jump is the
+// difference of its two cells' levels, the edge jumps stay 0, walls keep z_wall), then per
+// primitive parameter the central difference of the f64 materialisation contracted with it,
+// plus the earthwork term lambda (cut_cost dV_cut + fill_cost dV_fill) (objective.rs:95-128).
+
+// dJ/d(dz) of every cell of every design (grid: cells / 256 x designs).
+__global__ void k_mat_gdz(int nx, int ny, const double* gx, const double* gy, const uint8_t* wall, double* gdz) {
+  const int d = blockIdx.y;
+  const size_t N = (size_t)nx * ny;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int r = (int)(i / nx), c = (int)(i % nx);
+  const double* X = gx + (size_t)d * ny * (nx + 1) + (size_t)r * (nx + 1);
+  const double* Y = gy + (size_t)d * (ny + 1) * nx;
+  const double a = (c >= 1) ? X[c] : 0.0, b = (c + 1 <= nx - 1) ? X[c + 1] : 0.0;
+  const double e = (r >= 1) ? Y[(size_t)r * nx + c] : 0.0, f = (r + 1 <= ny - 1) ? Y[(size_t)(r + 1) * nx + c] : 0.0;
+  gdz[(size_t)d * N + i] = wall[i] ? 0.0 : ((a - b) + e) - f;
+}
+
+// One central difference: the up and down perturbed primitive sets of one parameter of one
+// primitive of design `design`, each with its own box.
+struct MatJob {
+  int design;
+  MatDesign up, dn;   // primitives [p0, p1) of the job's prim table, and the boxes
+  double twoh;        // 2 h
+  int out;            // output index (primitive * 3 + parameter)
+};
+
+// dz of cell (r, c) for the primitives [p0, p1) inside box B (0 outside it or if not editable).
+__device__ __forceinline__ double mat_cell(const MatArgs& M, const MatPrim* ps, const MatDesign& B, int r, int c) {
+  if (!(c >= B.c0 && c < B.c1 && r >= B.r0 && r < B.r1) || !M.editable[(size_t)r * M.nx + c]) return 0.0;
+  double acc = 0.0;
+  for (int q = B.p0; q < B.p1; ++q) {
+    const MatPrim p = ps[q];
+    if (p.height == 0.0) continue;
+    double s = 0.0;
+    for (int sy = 0; sy < 4; ++sy)
+      for (int sx = 0; sx < 4; ++sx) {
+        const double x = M.ox + ((double)c + ((double)sx + 0.5) / 4.0) * M.dx;
+        const double y = M.oy - ((double)r + ((double)sy + 0.5) / 4.0) * M.dy;
+        s += mat_profile(p, x, y);
+      }
+    acc += p.height * s * (1.0 / 16.0);
+  }
+  return acc < -M.max_abs_dz ? -M.max_abs_dz : (acc > M.max_abs_dz ? M.max_abs_dz : acc);
+}
+
+// One block per job: sum gdz * (dz_up - dz_dn) over the union of the two boxes, and the
+// cut / fill volumes of both sets; out = sum / 2h + lambda (cut_cost dcut + fill_cost dfill) / 2h.
+__global__ void k_mat_grad(const MatArgs M, const MatPrim* jp, const MatJob* jobs, const double* gdz, double earth_w,
+                           double cut_cost, double fill_cost, double* out) {
+  const MatJob J = jobs[blockIdx.x];
+  const int c0 = min(J.up.c0, J.dn.c0), r0 = min(J.up.r0, J.dn.r0);
+  const int c1 = max(J.up.c1, J.dn.c1), r1 = max(J.up.r1, J.dn.r1);
+  const int w = c1 - c0, h = r1 - r0;
+  const size_t N = (size_t)M.nx * M.ny;
+  const double a = M.dx * M.dy;
+  double s[5] = {0, 0, 0, 0, 0};   // contraction, cut up, fill up, cut down, fill down
+  for (int k = threadIdx.x; w > 0 && h > 0 && k < w * h; k += blockDim.x) {
+    const int r = r0 + k / w, c = c0 + k % w;
+    const double u = mat_cell(M, jp, J.up, r, c), v = mat_cell(M, jp, J.dn, r, c);
+    s[0] += gdz[(size_t)J.design * N + (size_t)r * M.nx + c] * (u - v);
+    if (u > 0.0) s[2] += u * a; else s[1] -= u * a;
+    if (v > 0.0) s[4] += v * a; else s[3] -= v * a;
+  }
+  __shared__ double red[32][5];
+  for (int j = 0; j < 5; ++j)
+    for (int o = 16; o > 0; o >>= 1) s[j] += __shfl_xor_sync(0xffffffffu, s[j], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int j = 0; j < 5; ++j) red[threadIdx.x >> 5][j] = s[j];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[5] = {0, 0, 0, 0, 0};
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
+      for (int j = 0; j < 5; ++j) t[j] += red[q][j];
+    out[J.out] = t[0] / J.twoh + earth_w * (cut_cost * (t[1] - t[3]) + fill_cost * (t[2] - t[4])) / J.twoh;
+  }
+}
+
 }  // namespace itr

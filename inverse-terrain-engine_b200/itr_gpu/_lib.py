@@ -112,6 +112,9 @@ SIGNATURES = {
     "itr_gpu_run_primitives": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(DesignSpace), C.c_int32,
                                          _i32p, C.POINTER(Primitive), _u32p, C.c_int32, C.POINTER(Objective),
                                          C.POINTER(Result), _dp, _dp]),
+    "itr_gpu_vjp_primitives": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(DesignSpace), C.c_int32,
+                                         _i32p, C.POINTER(Primitive), _u32p, C.c_int32, C.POINTER(Objective), C.c_int32,
+                                         C.POINTER(Result), _dp, _dp, _dp]),
     "itr_gpu_run_plain_static": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(Grid), C.POINTER(Design), _u32p,
                                            C.c_int32, C.POINTER(Result), C.c_char_p, C.c_size_t]),
 }

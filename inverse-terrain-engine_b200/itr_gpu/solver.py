@@ -416,22 +416,9 @@ class GpuSolver:
         self.last_cell_updates = sum(r.cell_updates for r in runs)
         return runs
 
-    def run_primitives(self, p: SolverParams, base, designs, monitors: MonitorSet, editable, max_abs_dz: float,
-                       objective=None, baseline_max=None, guard_abort=False, incumbent=None, want_peak=False,
-                       want_depth=True, ledger_rows=0):
-        """run_batch with every design given as its primitives (itr_gpu_run_primitives): the
-        device materialises dz, the edited levels, the face jumps and the earthwork volumes
-        (DesignSpace::materialize + PreparedTerrain::apply_edit) for a level-1 TerrainBase.
-        Returns (runs, cut_m3, fill_m3)."""
+    def _space(self, base, designs, editable, max_abs_dz, keep):
         if base.level != 1:
             raise UnsupportedError("designs as primitives need a fidelity level 1 terrain")
-        if p.initial_stage is not None:
-            raise UnsupportedError("designs as primitives start from initial_depth (no initial stage)")
-        keep = []
-        P = self._params(p, keep)
-        n = len(designs)
-        b = self._pack(base, [None] * n, [None] * n, None, None, None, None, monitors, objective, baseline_max, guard_abort,
-                       incumbent, want_peak, want_depth, ledger_rows, keep)
         flat = [q for d in designs for q in d]
         prims = (_lib.Primitive * max(len(flat), 1))()
         for k, q in enumerate(flat):
@@ -444,6 +431,48 @@ class GpuSolver:
         keep += [off, z, wall, ed, prims]
         S = _lib.DesignSpace(fine.geo.origin_x, fine.geo.origin_y, _ptr(z, C.c_double), _ptr(wall, C.c_uint8),
                              _ptr(ed, C.c_uint8), fine.z_wall, max_abs_dz)
+        keep.append(S)
+        return S, off, prims
+
+    def vjp_primitives(self, p: SolverParams, base, designs, monitors: MonitorSet, objective, editable, max_abs_dz: float,
+                       checkpoint_interval: int = 128):
+        """itr_gpu_vjp_primitives: forward runs of designs given as primitives, and
+        dJ/d(height, width, length) of every primitive from the design chain on the device.
+        Returns (runs with dj_ddzx / dj_ddzy, [per design an array (n_prims, 3)])."""
+        if p.initial_stage is not None:
+            raise UnsupportedError("designs as primitives start from initial_depth (no initial stage)")
+        keep = []
+        P = self._params(p, keep)
+        n = len(designs)
+        S, off, prims = self._space(base, designs, editable, max_abs_dz, keep)
+        b = self._pack(base, [None] * n, [None] * n, None, None, None, None, monitors, objective, None, False, None,
+                       False, True, 0, keep)
+        nx, ny = base.nx, base.ny
+        gx = np.zeros((n, ny, nx + 1))
+        gy = np.zeros((n, ny + 1, nx))
+        gp = np.zeros(max(3 * int(off[-1]), 1))
+        rc = self.lib.itr_gpu_vjp_primitives(self.ctx, C.byref(P), C.byref(b["Gd"]), C.byref(S), n, _ptr(off, C.c_int32), prims,
+                                             _ptr(b["mon"], C.c_uint32), b["nm"], C.byref(b["O"]), int(checkpoint_interval),
+                                             b["R"], _ptr(gp, C.c_double), _ptr(gx, C.c_double), _ptr(gy, C.c_double))
+        self._check(rc, "itr_gpu_vjp_primitives")
+        runs = self._unpack(b, b["R"], gx, gy)
+        return runs, [gp[3 * off[d]:3 * off[d + 1]].reshape(-1, 3) for d in range(n)]
+
+    def run_primitives(self, p: SolverParams, base, designs, monitors: MonitorSet, editable, max_abs_dz: float,
+                       objective=None, baseline_max=None, guard_abort=False, incumbent=None, want_peak=False,
+                       want_depth=True, ledger_rows=0):
+        """run_batch with every design given as its primitives (itr_gpu_run_primitives): the
+        device materialises dz, the edited levels, the face jumps and the earthwork volumes
+        (DesignSpace::materialize + PreparedTerrain::apply_edit) for a level-1 TerrainBase.
+        Returns (runs, cut_m3, fill_m3)."""
+        if p.initial_stage is not None:
+            raise UnsupportedError("designs as primitives start from initial_depth (no initial stage)")
+        keep = []
+        P = self._params(p, keep)
+        n = len(designs)
+        S, off, prims = self._space(base, designs, editable, max_abs_dz, keep)
+        b = self._pack(base, [None] * n, [None] * n, None, None, None, None, monitors, objective, baseline_max, guard_abort,
+                       incumbent, want_peak, want_depth, ledger_rows, keep)
         cut = np.zeros(max(n, 1))
         fill = np.zeros(max(n, 1))
         O = b["O"]

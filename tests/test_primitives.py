@@ -87,3 +87,38 @@ def test_coarse_level_rejected(gpu):
     coarse = TerrainBase(sc.base.fine, 2, [])
     with pytest.raises(UnsupportedError):
         gpu.run_primitives(sc.params, coarse, [[]], sc.monitors, np.ones((coarse.ny, coarse.nx), bool), 1.0)
+
+
+def test_design_chain_on_device_matches_host_chain(gpu):
+    """itr_gpu_vjp_primitives: the forward on the device-materialised designs, its adjoint,
+    and dJ/d(height, width, length) contracted on the device equal the host chain
+    (itr_gpu/adjoint.py primitive_gradient) on the same face-jump gradients, up to the order
+    of the f64 sums."""
+    import math
+    from itr_gpu import Asset, Hyetograph, Objective, ObjectiveDef, Segment, SolverParams, synthetic_terrain
+    from itr_gpu.adjoint import primitive_gradient
+    from itr_gpu.design import BERM, SWALE
+    nx, ny = 24, 16
+    base = synthetic_terrain(nx, ny, 5.0, lambda x, y: 2.0 - 0.01 * x + 0.2 * math.sin(y / 15.0) + 0.1 * math.cos(x / 20.0),
+                             n=0.03, segments=[Segment("transmissive", "east")])
+    p = SolverParams(120.0, 30.0, rain=Hyetograph.from_mm_h([(0, 50), (60, 120), (120, 0)]), initial_depth=0.3)
+    cells = [5 * nx + 8, 9 * nx + 15, 12 * nx + 20]
+    probe = Objective(ObjectiveDef([Asset(f"a{i}", [c], 10.0) for i, c in enumerate(cells)], []))
+    r0 = gpu.run_batch(p, [PreparedTerrain(base)], probe.monitors)[0]
+    odef = ObjectiveDef([Asset(f"a{i}", [c], float(r0.monitor_max[probe.monitors.position(c)]) - 0.004, 1.0 + i)
+                         for i, c in enumerate(cells)], [], earth_weight=1e-3)
+    obj = Objective(odef)
+    editable = np.ones((ny, nx), dtype=bool)
+    designs = [[Primitive(BERM, 55.0, 45.0, 40.0, 10.0, 30.0, 0.20), Primitive(SWALE, 85.0, 30.0, 30.0, 8.0, 110.0, -0.15)],
+               [Primitive(CUT, 60.0, 40.0, 30.0, 12.0, 0.0, -0.2)],
+               [Primitive(MOUND, 70.0, 50.0, 0.0, 20.0, 0.0, 0.3), Primitive(BERM, 40.0, 20.0, 25.0, 6.0, 80.0, 0.1)]]
+    runs, grads = gpu.vjp_primitives(p, base, designs, obj.monitors, obj, editable, 1.0, checkpoint_interval=16)
+    for d, prims in enumerate(designs):
+        host = primitive_gradient(base, base.fine.geo, editable, 1.0, prims, runs[d].dj_ddzx, runs[d].dj_ddzy, odef)
+        scale = max(np.abs(host).max(), 1e-30)
+        np.testing.assert_allclose(grads[d], host, rtol=1e-9, atol=1e-12 * scale, err_msg=f"design {d}")
+        assert np.any(grads[d] != 0.0)
+    # the forward part equals the device-materialised forward
+    fw, _, _ = gpu.run_primitives(p, base, designs, obj.monitors, editable, 1.0, objective=obj)
+    for a, b in zip(runs, fw):
+        assert a.steps == b.steps and np.array_equal(a.monitor_max, b.monitor_max) and a.j == b.j
