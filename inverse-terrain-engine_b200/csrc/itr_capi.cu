@@ -1368,13 +1368,14 @@ static int build_mat(itr_ctx* ctx, const itr_grid* g, const itr_design_space* sp
   if (!sp->z || !sp->wall || !sp->editable) return fail(ctx, ITR_INVALID_ARG, "design space arrays z, wall, editable are required");
   if (!(sp->max_abs_dz >= 0.0)) return fail(ctx, ITR_INVALID_ARG, "max_abs_dz must be non-negative");
   if (n < 0) return fail(ctx, ITR_INVALID_ARG, "negative design count");
-  if (n > 0 && !prim_off) return fail(ctx, ITR_INVALID_ARG, "prim_off is NULL");
-  if (n > 0 && prim_off[0] < 0) return fail(ctx, ITR_INVALID_ARG, "prim_off[0] is negative");
+  M.space = sp;
+  if (n == 0) return ITR_OK;
+  if (!prim_off) return fail(ctx, ITR_INVALID_ARG, "prim_off is NULL");
+  if (prim_off[0] < 0) return fail(ctx, ITR_INVALID_ARG, "prim_off[0] is negative");
   for (int d = 0; d < n; ++d)
     if (prim_off[d + 1] < prim_off[d]) return fail(ctx, ITR_INVALID_ARG, "prim_off is not non-decreasing");
-  const int total = n > 0 ? prim_off[n] : 0;
+  const int total = prim_off[n];
   if (total > 0 && !prims) return fail(ctx, ITR_INVALID_ARG, "prims is NULL");
-  M.space = sp;
   M.prims.resize((size_t)total);
   for (int k = prim_off[0]; k < total; ++k) {
     if (prims[k].kind < ITR_PRIM_BERM || prims[k].kind > ITR_PRIM_MOUND) return fail(ctx, ITR_INVALID_ARG, "primitive %d: unknown kind %d", k, prims[k].kind);
