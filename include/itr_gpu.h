@@ -159,6 +159,7 @@ typedef struct itr_result {
   int32_t n_rows;           /* ledger rows written */
   double volume_m3;         /* stored volume at the end */
   double rel_residual;      /* |ledger residual| / gross input at the last sync */
+  uint64_t warm_start_steps;/* steps taken over from the baseline record (RunSummary::warm_start_steps) */
 } itr_result;
 
 /* GpuSolver::new (lib.rs:85). device < 0 selects the current device. Returns NULL on
@@ -189,6 +190,8 @@ int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int3
  *   "cluster"  CTAs per design of the batched kernel (0 = autotune)
  *   "graph"    tiled path: 1 = replay each block of steps as one CUDA graph (default 1)
  *   "steps_per_submit"  plain and tiled paths: steps between host polls (default 64)
+ *   "warm_start"  1 = start each design from the baseline record (itr_gpu_record_baseline) where
+ *                 that is exact; 0 = always cold (default)
  *   "exact_special"     1 = the batched kernel computes every reciprocal and square root
  *                       with the IEEE-exact library routines instead of its own branch-free
  *                       ones (identical results; for checking, default 0)
@@ -242,6 +245,24 @@ int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n_
 
 /* Device time of the last itr_gpu_vjp: taped forward (kernels and checkpoints) and backward. */
 int itr_gpu_last_vjp_timing(itr_ctx* ctx, double* forward_ms, double* backward_ms);
+
+/* ---- Warm starts from a recorded baseline (BaselineRecord, solver.rs:95-118; used by the
+ * evaluator, evaluator.rs:423). ----
+ * itr_gpu_record_baseline runs `base` (the unedited terrain) to its end on the device and
+ * keeps, every checkpoint_interval steps, its state, running peaks, integrator and ledger,
+ * and which rows had held water by then. With option "warm_start" = 1, later batches on the
+ * same grid and params (itr_gpu_run_batch, itr_gpu_run_primitives; not the adjoint) start
+ * each design from the latest checkpoint at which every row its edit can reach (the cells
+ * on both sides of every face jump that differs from base's, and the cells behind stage
+ * edges whose depth differs) had stayed dry; rows beside stage or inflow edges count as
+ * wet from the start, as in the reference (solver.rs:404-423). Dry cells exchange exactly
+ * zero flux, so up to that point the design's run is the baseline's bit for bit: results
+ * equal a cold start (the ledger to f64 rounding on the cluster path). A design whose
+ * initial depth differs from base's, or a batch with an incumbent abort (the reference's
+ * warm start skips the bound at the syncs it jumps over), starts cold. The record lives in
+ * the context until the next itr_gpu_record_baseline; result (may be NULL) gets base's run. */
+int itr_gpu_record_baseline(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design* base,
+                            const uint32_t* monitors, int32_t n_mon, int32_t checkpoint_interval, itr_result* result);
 
 /* ---- Designs as primitives, materialised on the device. ----
  * The reference builds each candidate's face jumps on the host (DesignSpace::materialize,

@@ -67,6 +67,7 @@ struct BatchArgs {
   DesignOut* out;     // n_designs
   unsigned long long max_steps;
   unsigned exact;     // 1: every paired reciprocal through the IEEE routine (checking)
+  const WarmStart* warm;   // optional, per design (state NULL: cold start)
 };
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -432,9 +433,22 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   };
 
   // ---------------------------------------------------------------- initial state ----
+  // (or a warm start: the baseline's state, peaks and integrator at a checkpoint)
+  const WarmStart* WS = (A.warm && A.warm[d].state) ? &A.warm[d] : nullptr;
+  const double t_start = WS ? WS->t : 0.0;
   double s0_l = 0.0, v0_l = 0.0;
   for (int idx = tid; idx < nr * nx; idx += blockDim.x) {
     const int r = ra + idx / nx, c = idx % nx;
+    if (WS) {
+      const size_t i = (size_t)r * nx + c, NN = (size_t)nx * ny;
+      const float h = WS->state[i], qx = WS->state[NN + i], qy = WS->state[2 * NN + i];
+      float u, v, cc;
+      cell_vel(h, qx, qy, P.g_f, P.heps2_f, u, v, cc);
+      sm.S4[idx] = make_float4(h, qx, qy, u);
+      sm.S2[idx] = make_float2(v, cc);
+      sm.PK[idx] = WS->state[3 * NN + i];
+      continue;
+    }
     const float h = A.h0[cell0_off + (size_t)r * nx + c];
     float u, v, cc;
     cell_vel(h, 0.0f, 0.0f, P.g_f, P.heps2_f, u, v, cc);
@@ -453,9 +467,10 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   // that carry no cell compute on zeros (finite operands, no needless reciprocal fallbacks)
   for (int i = tid; i < 2 * S * K * vlanes; i += blockDim.x) sm.PF[i] = 0.0f;
   if (tid < 8) { sm.slot[tid] = 0u; sm.LED[tid] = 0.0; }
+  if (WS && q == 0 && tid == 0) { sm.LED[0] = WS->tot_infil; sm.LED[1] = WS->tot_fix; sm.LED[2] = WS->tot_in; sm.LED[3] = WS->tot_out; }
   if (tid == 0) mbar_init(sm.mbar, blockDim.x);
   // inflow ghosts of step 0 (at t = 0); each later step's are written one step ahead
-  if (BND && wid == nwarps - 1 && lane < P.inflow.n) sm.INF[lane] = inflow_values(P.inflow, lane, 0.0, P.g);
+  if (BND && wid == nwarps - 1 && lane < P.inflow.n) sm.INF[lane] = inflow_values(P.inflow, lane, t_start, P.g);
   {
     double sw = s0_l;
 #pragma unroll
@@ -470,18 +485,19 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     for (int w = 0; w < nwarps; ++w) { const double a = rr[w * 8 + 0]; s0 = s0 > a ? s0 : a; v0 += rr[w * 8 + 1]; }
   }
   v0 *= P.area;
+  if (WS) v0 = WS->v0;
   if (CLUSTERED) { cluster_arrive(); cluster_wait(); } else __syncthreads();   // red reused below
 
   // ------------------------------------------------------------------ integrator ----
-  double t = 0.0;
-  unsigned long long step = 0;
-  unsigned sync_index = 0;
-  double dt_cfl = s0 > 0.0 ? dmin_num(P.cfl / s0, P.dt_max) : P.dt_max;
-  double acc_rain = 0.0;
+  double t = t_start;
+  unsigned long long step = WS ? WS->step : 0ull;
+  unsigned sync_index = WS ? WS->sync_index : 0u;
+  double dt_cfl = WS ? WS->dt_cfl : (s0 > 0.0 ? dmin_num(P.cfl / s0, P.dt_max) : P.dt_max);
+  double acc_rain = WS ? WS->acc_rain : 0.0;
   int status = 0;
   unsigned breach_cell = 0, breach_sync = 0;
-  double violation = 0.0, lower_bound = 0.0, volume = v0, rel_res = 0.0;
-  int n_rows = 0;
+  double violation = 0.0, lower_bound = 0.0, volume = WS ? WS->volume : v0, rel_res = WS ? WS->rel_res : 0.0;
+  int n_rows = WS ? WS->n_rows : 0;
   GroupSync<CLUSTERED> gs;
   gs.mbar = sm.mbar; gs.phase = 0; gs.timed_out = false;
   const float heps2 = P.heps2_f;

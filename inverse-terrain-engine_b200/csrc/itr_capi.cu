@@ -92,6 +92,22 @@ struct Mat {
   std::vector<itr_design> ds;   // placeholders; cut/fill filled in from the device
 };
 
+// Baseline record for warm starts (BaselineRecord, solver.rs:95-118): checkpoints of the
+// base terrain's run every K steps (state, peaks, integrator), which rows had held water by
+// each, the base's ledger, and what the record was made with (to match later batches).
+struct Record {
+  bool valid = false;
+  RunParams P;                                   // params, grid scalars, rain and inflow tables
+  int nx = 0, ny = 0, mode = 0;
+  std::vector<float> wet, gn2, dzx, dzy, dzx2, dzy2, bh, h0;   // h0 empty: initial_depth on open cells
+  std::vector<uint8_t> bc, open_rows;            // device codes; rows beside stage / inflow edges
+  struct Ckpt { DevBuf state; WarmStart ws; std::vector<uint8_t> wet; };   // state: [4][N] floats, then ny row flags
+  std::vector<Ckpt> ck;
+  std::vector<PlainCtl> ctl;                     // control block at each checkpoint
+  std::vector<double> ledger;                    // base's ledger rows, 8 doubles each
+  int K = 64;
+};
+
 struct itr_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -117,6 +133,11 @@ struct itr_ctx {
   std::vector<DevBuf> aCkpt;
   struct Vjp* vjp = nullptr;
   Mat* mat = nullptr;
+  Record* rec = nullptr;         // the baseline record (itr_gpu_record_baseline)
+  Record* recording = nullptr;   // set while the record is being made
+  int warm_start = 0;
+  std::vector<uint64_t> warm_steps;   // per design of the last batch
+  DevBuf wsb;
   DevBuf mDz, mZe, mAux, mJp, mJob, mOut;
   HostBuf mVol;
   // ladder: one child context per grid group; a deferred run stops before its launch
@@ -274,6 +295,7 @@ static std::vector<LaunchCfg> candidates(itr_ctx* ctx, int nx, int ny, int n_des
 static int autotune(itr_ctx* ctx, const BatchArgs& A0, const std::vector<LaunchCfg>& cands, int n, LaunchCfg* best) {
   BatchArgs A = A0;
   A.max_steps = (unsigned long long)ctx->probe_steps;
+  A.warm = nullptr;   // probe the cold start: the shapes compare the same
   A.ledger_out = nullptr;
   A.max_rows = 0;
   A.obj.enabled = 0;
@@ -493,10 +515,14 @@ void itr_gpu_destroy(itr_ctx* ctx) {
                     &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
                     &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy,
                     &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon,
-                    &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut})
+                    &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut, &ctx->wsb})
     b->release();
   for (DevBuf& b : ctx->aCkpt) b.release();
   for (itr_ctx* c : ctx->children) itr_gpu_destroy(c);
+  if (ctx->rec) {
+    for (auto& c : ctx->rec->ck) c.state.release();
+    delete ctx->rec;
+  }
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   ctx->aRingH.release();
   ctx->mVol.release();
@@ -529,6 +555,7 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   else if (k == "steps_per_submit") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "steps_per_submit must be >= 1"); ctx->steps_per_submit = (int)value; }
   else if (k == "autotune") { ctx->autotune = value != 0; ctx->tuned.clear(); }
   else if (k == "exact_special") ctx->exact_special = value != 0;
+  else if (k == "warm_start") ctx->warm_start = value != 0;
   else if (k == "probe_steps") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "probe_steps must be >= 1"); ctx->probe_steps = (int)value; }
   else return fail(ctx, ITR_INVALID_ARG, "unknown option '%s'", key);
   if (k == "threads" || k == "cluster") ctx->tuned.clear();
@@ -624,7 +651,22 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
   }
   PlainCtl* hc = ctx->hout.as<PlainCtl>();
   int rc = ITR_OK;
+  Record* rec = ctx->recording;
+  if (rec) {   // the control block after the first plan: checkpoint 0's integrator
+    CU(cudaMemcpyAsync(hc, A.ctl, sizeof(PlainCtl), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+  }
   for (uint64_t polls = 0;; ++polls) {
+    if (rec) {   // baseline record: state, peaks and integrator at the start of this block
+      rec->ck.emplace_back();
+      Record::Ckpt& ck = rec->ck.back();
+      cudaError_t e = ck.state.ensure(4 * N * 4 + (size_t)A.ny);
+      if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "baseline record: %s", cudaGetErrorString(e)); break; }
+      k_rec_state<<<dim3(64), 256, 0, st>>>(A, ck.state.as<float>());
+      k_rec_rows<<<dim3((unsigned)A.ny), 128, 0, st>>>(A, ck.state.as<float>(), ck.state.as<uint8_t>() + 4 * N * 4);
+      *launches += 2;
+      rec->ctl.push_back(hc[0]);
+    }
     if (tape) {   // checkpoint: the state at the start of this block
       if (ctx->aCkpt.size() <= polls) ctx->aCkpt.emplace_back();
       cudaError_t e = ctx->aCkpt[polls].ensure((size_t)n * 3 * N * 4);
@@ -836,6 +878,7 @@ static int collect_results(itr_ctx* ctx, const Collect& c) {
     r.n_rows = o.n_rows < r.max_rows ? o.n_rows : r.max_rows;
     r.volume_m3 = o.volume;
     r.rel_residual = o.rel_residual;
+    r.warm_start_steps = (size_t)d < ctx->warm_steps.size() ? ctx->warm_steps[d] : 0;
     if (r.monitor_max) for (int k = 0; k < n_mon; ++k) r.monitor_max[k] = (double)hmm[(size_t)d * n_mon + k];
     if (r.ledger && r.max_rows > 0) memcpy(r.ledger, hled + (size_t)d * max_rows * 8, (size_t)r.n_rows * 64);
     r.j = 0.0; r.feasible = 1; r.violation = 0.0;
@@ -865,6 +908,56 @@ static int collect_results(itr_ctx* ctx, const Collect& c) {
     ctx->vjp_bwd_ms = b_ms;
   }
   return ITR_OK;
+}
+
+// ------------------------------------------------------------------ warm starts ------
+// Whether a batch runs on the grid and params the baseline record was made with.
+static bool record_matches(const Record& R, const RunParams& P, const itr_grid* g, const uint8_t* dbc) {
+  const size_t N = (size_t)g->nx * g->ny, NB = 2 * (size_t)(g->nx + g->ny);
+  if (!R.valid || R.nx != g->nx || R.ny != g->ny || R.mode != g->mode) return false;
+  if (memcmp(&R.P, &P, sizeof(RunParams)) != 0) return false;
+  return memcmp(R.wet.data(), g->wet, N * 4) == 0 && memcmp(R.gn2.data(), g->gn2, N * 4) == 0 &&
+         memcmp(R.bc.data(), dbc, NB) == 0;
+}
+
+// Rows of a design whose cells sit beside a face jump (or behind a stage edge) that differs
+// from the base's: until one of them holds water, the design's run is the base's.
+static bool touched_rows(const Record& R, const itr_grid* g, const itr_design& ds, std::vector<uint8_t>& t) {
+  const int nx = g->nx, ny = g->ny;
+  const size_t N = (size_t)nx * ny, SX = (size_t)ny * (nx + 1), SY = (size_t)(ny + 1) * nx, NB = 2 * (size_t)(nx + ny);
+  if (ds.h0 ? (R.h0.empty() || memcmp(ds.h0, R.h0.data(), N * 4) != 0) : !R.h0.empty()) return false;   // other start
+  t.assign((size_t)ny, 0);
+  auto differ = [](const float* a, const float* b, size_t i) { return memcmp(a + i, b + i, 4) != 0; };
+  const bool crest = g->mode == ITR_FACE_CREST;
+  for (size_t i = 0; i < SX; ++i)
+    if (differ(ds.dzx, R.dzx.data(), i) || (crest && differ(ds.dzx2, R.dzx2.data(), i))) t[i / (nx + 1)] = 1;
+  for (size_t i = 0; i < SY; ++i)
+    if (differ(ds.dzy, R.dzy.data(), i) || (crest && differ(ds.dzy2, R.dzy2.data(), i))) {
+      const int f = (int)(i / nx);
+      if (f >= 1) t[f - 1] = 1;
+      if (f < ny) t[f] = 1;
+    }
+  if (!R.bh.empty()) {
+    std::vector<float> bh(NB);
+    stage_depths(g, ds.z_edge, bh.data());
+    for (size_t i = 0; i < NB; ++i)
+      if (memcmp(&bh[i], &R.bh[i], 4) != 0) {
+        const int row = i < (size_t)nx ? 0 : i < 2 * (size_t)nx ? ny - 1 : (int)((i - 2 * (size_t)nx) % ny);
+        t[row] = 1;
+      }
+  }
+  return true;
+}
+
+// The latest checkpoint at which every touched row had stayed dry and none is beside a
+// stage or inflow edge (BaselineRecord::best_for, solver.rs:110-115); 0 means a cold start.
+static size_t warm_pick(const Record& R, const std::vector<uint8_t>& t) {
+  for (size_t c = R.ck.size(); c-- > 1;) {
+    bool ok = true;
+    for (int j = 0; j < R.ny && ok; ++j) ok = !(t[j] && (R.ck[c].wet[j] || R.open_rows[j]));
+    if (ok) return c;
+  }
+  return 0;
 }
 
 // ------------------------------------------------------------------ run_batch -------
@@ -1018,6 +1111,43 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     CU(cudaStreamSynchronize(ctx->stream));
     for (int d = 0; d < n; ++d) { M->ds[d].cut_m3 = hv[d]; M->ds[d].fill_m3 = hv[n + d]; }
   }
+  // ---- warm starts from the baseline record ----
+  ctx->warm_steps.assign((size_t)n, 0);
+  const WarmStart* warm_dev = nullptr;
+  if (ctx->warm_start && ctx->rec && !ctx->vjp && !ctx->recording && !(ob && ob->has_incumbent) &&
+      record_matches(*ctx->rec, P, g, st + o_bc)) {
+    const Record& R = *ctx->rec;
+    std::vector<WarmStart> ws((size_t)n);
+    memset(ws.data(), 0, ws.size() * sizeof(WarmStart));
+    bool any = false;
+    for (int d = 0; d < n; ++d) {
+      std::vector<uint8_t> t;
+      if (M) {   // a box of primitives: its rows and the one on either side (the edit_rows of apply_edit)
+        if (!R.h0.empty()) continue;
+        t.assign((size_t)ny, 0);
+        const MatDesign& B = M->des[d];
+        if (B.c0 < B.c1 && B.r0 < B.r1)
+          for (int r = B.r0 - 1; r <= B.r1; ++r) if (r >= 0 && r < ny) t[r] = 1;
+      } else if (!touched_rows(R, g, ds[d], t)) {
+        continue;
+      }
+      const size_t c = warm_pick(R, t);
+      if (c == 0) continue;
+      ws[d] = R.ck[c].ws;
+      ctx->warm_steps[d] = ws[d].step;
+      any = true;
+      const int rows = ws[d].n_rows < max_rows ? ws[d].n_rows : max_rows;   // the base's ledger rows so far
+      if (rows > 0)
+        CU(cudaMemcpyAsync(ctx->ledger.as<double>() + (size_t)d * max_rows * 8, R.ledger.data(), (size_t)rows * 64,
+                           cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (any) {
+      CU(ctx->wsb.ensure((size_t)n * sizeof(WarmStart)));
+      CU(cudaMemcpyAsync(ctx->wsb.p, ws.data(), (size_t)n * sizeof(WarmStart), cudaMemcpyHostToDevice, ctx->stream));
+      CU(cudaStreamSynchronize(ctx->stream));   // ws is a local vector
+      warm_dev = ctx->wsb.as<WarmStart>();
+    }
+  }
   const unsigned long long max_steps = 2000000000ull;
 
   // impl 2, or a grid no cluster shape can hold: the tiled batched path (state in HBM)
@@ -1051,6 +1181,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.ledger = max_rows > 0 ? ctx->ledger.as<double>() : nullptr;
     A.max_rows = max_rows;
     A.max_steps = max_steps;
+    A.warm = warm_dev;
     return e;
   };
   if (ctx->impl == 0 && !tiled) {
@@ -1078,6 +1209,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.out = ctx->out.as<DesignOut>();
     A.max_steps = max_steps;
     A.exact = ctx->exact_special ? 1u : 0u;
+    A.warm = warm_dev;
     // launch configuration
     LaunchCfg cfg;
     auto key = std::make_tuple(nx, ny, n, (int)g->mode + (bnd ? 2 : 0));
@@ -1104,6 +1236,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
           PlainArgs T;
           CU(tiled_args(T));
           T.max_steps = (unsigned long long)ctx->probe_steps;
+          T.warm = nullptr;
           T.obj.enabled = 0; T.ledger = nullptr; T.max_rows = 0;
           int dummy = 0;
           float t_ms = 0.0f;
@@ -1204,6 +1337,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
       A.ledger = max_rows > 0 ? ctx->ledger.as<double>() + (size_t)d * max_rows * 8 : nullptr;
       A.max_rows = max_rows;
       A.max_steps = max_steps;
+      A.warm = warm_dev ? warm_dev + d : nullptr;
       rc = run_plain_design(ctx, A, nb, grid, &launches);
       if (rc != ITR_OK) return rc;
       // copy this design's outputs into the batched output slots
@@ -1312,6 +1446,88 @@ extern "C" int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_g
   ctx->cell_updates = cu;
   ctx->launches = launches;
   ctx->have_last = false;
+  return ITR_OK;
+}
+
+// ------------------------------------------------------------------ baseline record ----
+extern "C" int itr_gpu_record_baseline(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design* base,
+                                       const uint32_t* mon, int32_t n_mon, int32_t K, itr_result* result) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (!base) return fail(ctx, ITR_INVALID_ARG, "base design is NULL");
+  if (K < 1 || K > 65536) return fail(ctx, ITR_INVALID_ARG, "checkpoint interval out of range");
+  int rc = check_inputs(ctx, p, g, 1, base, mon, n_mon, nullptr);
+  if (rc != ITR_OK) return rc;
+  CU(cudaSetDevice(ctx->device));
+  if (ctx->rec) {   // a new record replaces the old one
+    for (auto& c : ctx->rec->ck) c.state.release();
+    delete ctx->rec;
+    ctx->rec = nullptr;
+  }
+  const int nx = g->nx, ny = g->ny;
+  const size_t N = (size_t)nx * ny, SX = (size_t)ny * (nx + 1), SY = (size_t)(ny + 1) * nx, NB = 2 * (size_t)(nx + ny);
+  Record* R = new Record();
+  R->K = K; R->nx = nx; R->ny = ny; R->mode = g->mode;
+  R->P = make_run_params(p, g);
+  R->bc.resize(NB);
+  rc = build_boundaries(ctx, g, R->P.inflow, R->bc.data());
+  if (rc != ITR_OK) { delete R; return rc; }
+  R->wet.assign(g->wet, g->wet + N); R->gn2.assign(g->gn2, g->gn2 + N);
+  R->dzx.assign(base->dzx, base->dzx + SX); R->dzy.assign(base->dzy, base->dzy + SY);
+  if (g->mode == ITR_FACE_CREST) { R->dzx2.assign(base->dzx2, base->dzx2 + SX); R->dzy2.assign(base->dzy2, base->dzy2 + SY); }
+  if (base->h0) R->h0.assign(base->h0, base->h0 + N);
+  bool has_stage = false;
+  R->open_rows.assign((size_t)ny, 0);
+  for (size_t i = 0; i < NB; ++i) {
+    const bool open = g->bc[i] == ITR_BC_STAGE || g->bc[i] == ITR_BC_INFLOW;
+    has_stage = has_stage || g->bc[i] == ITR_BC_STAGE;
+    if (!open) continue;   // rows beside water-creating edges are wet from the start (solver.rs:404-423)
+    const int row = i < (size_t)nx ? 0 : i < 2 * (size_t)nx ? ny - 1 : (int)((i - 2 * (size_t)nx) % ny);
+    R->open_rows[row] = 1;
+  }
+  if (has_stage) { R->bh.resize(NB); stage_depths(g, base->z_edge, R->bh.data()); }
+  // the base's run on the tiled path, checkpointed every K steps, with its whole ledger
+  const int max_rows = (int)R->P.n_sync;
+  std::vector<double> led((size_t)(max_rows > 0 ? max_rows : 1) * 8);
+  itr_result local;
+  memset(&local, 0, sizeof(local));
+  if (result) { local.monitor_max = result->monitor_max; local.peak = result->peak; local.depth = result->depth; }
+  local.ledger = led.data();
+  local.max_rows = max_rows;
+  const int impl0 = ctx->impl, k0 = ctx->steps_per_submit, w0 = ctx->warm_start;
+  ctx->impl = 2; ctx->steps_per_submit = K; ctx->warm_start = 0;
+  ctx->recording = R;
+  rc = itr_gpu_run_batch(ctx, p, g, 1, base, mon, n_mon, nullptr, &local);
+  ctx->recording = nullptr;
+  ctx->impl = impl0; ctx->steps_per_submit = k0; ctx->warm_start = w0;
+  auto drop = [&]() { for (auto& c : R->ck) c.state.release(); delete R; };
+  if (rc != ITR_OK) { drop(); return rc; }
+  for (size_t c = 0; c < R->ck.size(); ++c) {
+    Record::Ckpt& ck = R->ck[c];
+    ck.wet.resize((size_t)ny);
+    const cudaError_t e = cudaMemcpy(ck.wet.data(), ck.state.as<uint8_t>() + 4 * N * 4, (size_t)ny, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { drop(); return fail(ctx, ITR_DEVICE_ERROR, "baseline record: %s", cudaGetErrorString(e)); }
+    const PlainCtl& cl = R->ctl[c];
+    WarmStart w;
+    memset(&w, 0, sizeof(w));
+    w.state = ck.state.as<float>();
+    w.t = cl.t; w.dt_cfl = cl.dt_cfl; w.acc_rain = cl.acc_rain; w.v0 = cl.v0; w.volume = cl.volume; w.rel_res = cl.rel_res;
+    w.tot_infil = cl.tot_infil; w.tot_fix = cl.tot_fix; w.tot_in = cl.tot_in; w.tot_out = cl.tot_out;
+    w.step = cl.step; w.sync_index = cl.sync_index; w.n_rows = cl.n_rows;
+    ck.ws = w;
+  }
+  R->ledger.assign(led.begin(), led.begin() + (size_t)local.n_rows * 8);
+  if (result) {
+    double* ul = result->ledger;
+    const int um = result->max_rows;
+    itr_result keep = local;
+    keep.ledger = ul; keep.max_rows = um;
+    keep.n_rows = local.n_rows < um ? local.n_rows : um;
+    if (ul && keep.n_rows > 0) memcpy(ul, led.data(), (size_t)keep.n_rows * 64);
+    if (!ul) keep.n_rows = 0;
+    *result = keep;
+  }
+  R->valid = true;
+  ctx->rec = R;
   return ITR_OK;
 }
 

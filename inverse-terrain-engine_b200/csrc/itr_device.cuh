@@ -442,6 +442,17 @@ struct DevObjective {
 };
 
 // Per-design scalar results written by the kernels.
+// A design's warm start (Solver::run_impl from a Checkpoint, solver.rs:354-378): the
+// baseline's state at a checkpoint and its integrator there. state == NULL: cold start.
+struct WarmStart {
+  const float* state;   // [4][nx*ny]: h, qx, qy, running peak depth
+  double t, dt_cfl, acc_rain, v0, volume, rel_res;
+  double tot_infil, tot_fix, tot_in, tot_out;   // ledger totals (infil, fix per unit area)
+  unsigned long long step;
+  unsigned sync_index;
+  int n_rows;
+};
+
 struct DesignOut {
   unsigned long long steps;
   double t_end;

@@ -79,6 +79,7 @@ struct PlainArgs {
   unsigned* tpk;      // optional, per design nx*ny: index of the state that last raised PK
   double* dt_log;     // optional, per design a ring of max_log (dt, rain, t): slot step % max_log
   int max_log;
+  const WarmStart* warm;   // optional, per design (state NULL: cold)
 };
 
 // Pointers of design d inside a launch over n_designs designs.
@@ -332,11 +333,27 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
   }
 }
 
-// Initial state and the first dt (solver.rs:381-390).
+// Initial state and the first dt (solver.rs:381-390), or a warm start's checkpoint.
 __global__ void k_plain_init(const PlainArgs A) {
   const PlainDesign D = plain_design(A, blockIdx.x, 0);
   const int nx = A.nx, ny = A.ny, n = nx * ny;
   const RunParams& P = A.P;
+  const WarmStart* W = (A.warm && A.warm[blockIdx.x].state) ? &A.warm[blockIdx.x] : nullptr;
+  if (W) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      D.H[i] = W->state[i]; D.QX[i] = W->state[n + i]; D.QY[i] = W->state[2 * n + i]; D.PK[i] = W->state[3 * n + i];
+      if (D.tpk) D.tpk[i] = 0u;
+    }
+    if (threadIdx.x == 0) {
+      PlainCtl c;
+      memset(&c, 0, sizeof(c));
+      c.t = W->t; c.dt_cfl = W->dt_cfl; c.acc_rain = W->acc_rain; c.v0 = W->v0; c.volume = W->volume; c.rel_res = W->rel_res;
+      c.tot_infil = W->tot_infil; c.tot_fix = W->tot_fix; c.tot_in = W->tot_in; c.tot_out = W->tot_out;
+      c.step = W->step; c.sync_index = W->sync_index; c.n_rows = W->n_rows;
+      *D.ctl = c;
+    }
+    return;
+  }
   __shared__ double ss[32], sv[32];
   double s0 = 0.0, v0 = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -366,6 +383,31 @@ __global__ void k_plain_init(const PlainArgs A) {
     c.dt_cfl = s > 0.0 ? dmin_num(P.cfl / s, P.dt_max) : P.dt_max;
     *D.ctl = c;
   }
+}
+
+// Baseline record (one design): the current state plane and running peaks into dst [4][N].
+__global__ void k_rec_state(const PlainArgs A, float* dst) {
+  const PlainDesign D = plain_design(A, 0, 0);
+  const size_t N = (size_t)A.nx * A.ny;
+  const int par = D.ctl->par;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    dst[i] = D.H[par * N + i]; dst[N + i] = D.QX[par * N + i]; dst[2 * N + i] = D.QY[par * N + i]; dst[3 * N + i] = D.PK[i];
+  }
+}
+
+// Whether row blockIdx.x has held water in any state so far: initial depth or running peak
+// above 0 in any of its cells (the peak plane is state [3] of a record checkpoint).
+__global__ void k_rec_rows(const PlainArgs A, const float* state, uint8_t* wet) {
+  const int r = blockIdx.x, nx = A.nx;
+  const size_t N = (size_t)A.nx * A.ny;
+  const PlainDesign D = plain_design(A, 0, 0);
+  int any = 0;
+  for (int c = threadIdx.x; c < nx; c += blockDim.x) {
+    const size_t i = (size_t)r * nx + c;
+    any |= (D.h0[i] > 0.0f || state[3 * N + i] > 0.0f) ? 1 : 0;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) wet[r] = any ? 1 : 0;
 }
 
 // Per-design results of a tiled batched run: the scalar outcome from the control block and

@@ -69,7 +69,7 @@ class Result(C.Structure):
         ("sync_count", C.c_uint32), ("status", C.c_int32), ("breach_cell", C.c_uint32),
         ("breach_sync", C.c_uint32), ("violation", C.c_double), ("lower_bound", C.c_double),
         ("j", C.c_double), ("feasible", C.c_int32), ("n_rows", C.c_int32),
-        ("volume_m3", C.c_double), ("rel_residual", C.c_double),
+        ("volume_m3", C.c_double), ("rel_residual", C.c_double), ("warm_start_steps", C.c_uint64),
     ]
 
 
@@ -109,6 +109,8 @@ SIGNATURES = {
     "itr_gpu_vjp": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.c_int32, C.POINTER(Design), _u32p,
                               C.c_int32, C.POINTER(Objective), C.c_int32, C.POINTER(Result), _dp, _dp]),
     "itr_gpu_last_vjp_timing": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "itr_gpu_record_baseline": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(Design), _u32p,
+                                          C.c_int32, C.c_int32, C.POINTER(Result)]),
     "itr_gpu_run_primitives": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(DesignSpace), C.c_int32,
                                          _i32p, C.POINTER(Primitive), _u32p, C.c_int32, C.POINTER(Objective),
                                          C.POINTER(Result), _dp, _dp]),

@@ -187,6 +187,7 @@ class GpuRun:
     cell_updates: int = 0
     dj_ddzx: np.ndarray | None = None   # itr_gpu_vjp: dJ/d(x-face jump), (ny, nx+1)
     dj_ddzy: np.ndarray | None = None   # itr_gpu_vjp: dJ/d(y-face jump), (ny+1, nx)
+    warm_start_steps: int = 0           # steps taken over from the baseline record
 
 
 @dataclass
@@ -387,6 +388,7 @@ class GpuSolver:
                                breach_sync=int(r.breach_sync), violation=float(r.violation), lower_bound=float(r.lower_bound),
                                j=float(r.j), feasible=bool(r.feasible), sync_count=int(r.sync_count),
                                rel_residual=float(r.rel_residual), cell_updates=int(r.cell_updates),
+                               warm_start_steps=int(r.warm_start_steps),
                                dj_ddzx=gx[i] if gx is not None else None, dj_ddzy=gy[i] if gy is not None else None))
         return runs
 
@@ -457,6 +459,22 @@ class GpuSolver:
         self._check(rc, "itr_gpu_vjp_primitives")
         runs = self._unpack(b, b["R"], gx, gy)
         return runs, [gp[3 * off[d]:3 * off[d + 1]].reshape(-1, 3) for d in range(n)]
+
+    def record_baseline(self, p: SolverParams, terrain: PreparedTerrain, monitors: MonitorSet, checkpoint_interval: int = 64,
+                        want_peak: bool = False, ledger_rows: int = 0) -> GpuRun:
+        """itr_gpu_record_baseline: run the unedited terrain with checkpoints every
+        checkpoint_interval steps; with set_option("warm_start", 1) later batches on the same
+        grid and params start each design from the latest checkpoint where that is exact."""
+        keep = []
+        P = self._params(p, keep)
+        h0 = [terrain.initial_depth(p.initial_depth, p.initial_stage)] if p.initial_stage is not None else None
+        b = self._pack(terrain.base, [terrain.dzx], [terrain.dzy], [terrain.dzx2], [terrain.dzy2], h0,
+                       [(terrain.cut_m3, terrain.fill_m3)], monitors, None, None, False, None, want_peak, True, ledger_rows,
+                       keep, _z_edges(terrain.base, [terrain]))
+        rc = self.lib.itr_gpu_record_baseline(self.ctx, C.byref(P), C.byref(b["Gd"]), b["D"], _ptr(b["mon"], C.c_uint32),
+                                              b["nm"], int(checkpoint_interval), b["R"])
+        self._check(rc, "itr_gpu_record_baseline")
+        return self._unpack(b, b["R"])[0]
 
     def run_primitives(self, p: SolverParams, base, designs, monitors: MonitorSet, editable, max_abs_dz: float,
                        objective=None, baseline_max=None, guard_abort=False, incumbent=None, want_peak=False,
