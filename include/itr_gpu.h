@@ -311,6 +311,16 @@ int itr_gpu_vjp_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g,
                            const uint32_t* monitors, int32_t n_mon, const itr_objective* obj, int32_t checkpoint_interval,
                            itr_result* results, double* dj_dprim, double* dj_ddzx, double* dj_ddzy);
 
+/* ---- Headless map image (presentation, not on the hot path). ----
+ * The reference's result viewer draws its map with a WebGL fragment shader (viewer/viewer.js:
+ * 72-100): a hillshade of the terrain, a logarithmic depth ramp (mode 0) or a diverging ramp
+ * of depth differences (mode 1), and hatching where worse_dz > 1 cm. itr_gpu_render_map
+ * computes the same image on the device without a graphics stack: rgba receives
+ * (scale*nx) x (scale*ny) pixels, 4 bytes each, row 0 the northern row. z: cell levels (NaN
+ * = no data); value: depth or difference per cell; worse_dz may be NULL (no hatching). */
+int itr_gpu_render_map(itr_ctx* ctx, int32_t nx, int32_t ny, double cell_size, const float* z, const float* value,
+                       const float* worse_dz, int32_t mode, float vex, int32_t scale, uint8_t* rgba);
+
 /* ---- Allocation-free plain forward. No reference counterpart. ----
  * For callers that cannot allocate device memory when they run a design: a process that
  * has committed the whole device to its own pool, a caller whose other streams must not be

@@ -24,6 +24,7 @@
 #include "itr_plain.cuh"
 #include "itr_adjoint.cuh"
 #include "itr_design.cuh"
+#include "itr_render.cuh"
 
 using namespace itr;
 
@@ -139,6 +140,7 @@ struct itr_ctx {
   std::vector<uint64_t> warm_steps;   // per design of the last batch
   DevBuf wsb;
   DevBuf mDz, mZe, mAux, mJp, mJob, mOut;
+  DevBuf rIn, rOut;   // map rendering
   HostBuf mVol;
   // ladder: one child context per grid group; a deferred run stops before its launch
   std::vector<itr_ctx*> children;
@@ -515,7 +517,7 @@ void itr_gpu_destroy(itr_ctx* ctx) {
                     &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
                     &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy,
                     &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon,
-                    &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut, &ctx->wsb})
+                    &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut, &ctx->wsb, &ctx->rIn, &ctx->rOut})
     b->release();
   for (DevBuf& b : ctx->aCkpt) b.release();
   for (itr_ctx* c : ctx->children) itr_gpu_destroy(c);
@@ -1446,6 +1448,36 @@ extern "C" int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_g
   ctx->cell_updates = cu;
   ctx->launches = launches;
   ctx->have_last = false;
+  return ITR_OK;
+}
+
+// ------------------------------------------------------------------ map image ---------
+extern "C" int itr_gpu_render_map(itr_ctx* ctx, int32_t nx, int32_t ny, double cell_size, const float* z, const float* value,
+                                  const float* worse_dz, int32_t mode, float vex, int32_t scale, uint8_t* rgba) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (nx < 1 || ny < 1 || (int64_t)nx * ny > (1ll << 28)) return fail(ctx, ITR_INVALID_ARG, "bad grid size");
+  if (scale < 1 || (int64_t)nx * scale * (int64_t)ny * scale > (1ll << 30)) return fail(ctx, ITR_INVALID_ARG, "bad scale");
+  if (!z || !value || !rgba) return fail(ctx, ITR_INVALID_ARG, "z, value and rgba are required");
+  if (mode != 0 && mode != 1) return fail(ctx, ITR_INVALID_ARG, "mode must be 0 (depth) or 1 (difference)");
+  if (!(cell_size > 0.0)) return fail(ctx, ITR_INVALID_ARG, "cell size must be positive");
+  CU(cudaSetDevice(ctx->device));
+  const size_t N = (size_t)nx * ny, P = N * (size_t)scale * scale;
+  CU(ctx->rIn.ensure(3 * N * 4));
+  CU(ctx->rOut.ensure(P * 4));
+  float* din = ctx->rIn.as<float>();
+  CU(cudaMemcpyAsync(din, z, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(din + N, value, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+  if (worse_dz) CU(cudaMemcpyAsync(din + 2 * N, worse_dz, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+  RenderArgs A;
+  A.nx = nx; A.ny = ny; A.scale = scale; A.mode = mode; A.worse = worse_dz ? 1 : 0;
+  A.vex = vex; A.cs = (float)cell_size;
+  A.z = din; A.value = din + N; A.dz = worse_dz ? din + 2 * N : nullptr;
+  A.out = ctx->rOut.as<uchar4>();
+  const dim3 blk(16, 16), grd((unsigned)((nx * scale + 15) / 16), (unsigned)((ny * scale + 15) / 16));
+  k_render_map<<<grd, blk, 0, ctx->stream>>>(A);
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(rgba, ctx->rOut.p, P * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
   return ITR_OK;
 }
 

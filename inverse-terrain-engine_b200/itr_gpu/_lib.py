@@ -109,6 +109,8 @@ SIGNATURES = {
     "itr_gpu_vjp": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.c_int32, C.POINTER(Design), _u32p,
                               C.c_int32, C.POINTER(Objective), C.c_int32, C.POINTER(Result), _dp, _dp]),
     "itr_gpu_last_vjp_timing": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "itr_gpu_render_map": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, _fp, _fp, _fp, C.c_int32, C.c_float,
+                                     C.c_int32, _u8p]),
     "itr_gpu_record_baseline": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(Design), _u32p,
                                           C.c_int32, C.c_int32, C.POINTER(Result)]),
     "itr_gpu_run_primitives": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(DesignSpace), C.c_int32,

@@ -460,6 +460,20 @@ class GpuSolver:
         runs = self._unpack(b, b["R"], gx, gy)
         return runs, [gp[3 * off[d]:3 * off[d + 1]].reshape(-1, 3) for d in range(n)]
 
+    def render_map(self, z, value, cell_size: float, mode: int = 0, vex: float = 1.0, scale: int = 1, worse_dz=None):
+        """itr_gpu_render_map: the result viewer's map of `value` (depth, mode 0, or depth
+        difference, mode 1) over the hillshaded terrain z, as an RGBA uint8 image of shape
+        (scale ny, scale nx, 4), row 0 north."""
+        z = np.ascontiguousarray(z, dtype=np.float32)
+        ny, nx = z.shape
+        v = np.ascontiguousarray(value, dtype=np.float32).reshape(ny, nx)
+        w = None if worse_dz is None else np.ascontiguousarray(worse_dz, dtype=np.float32).reshape(ny, nx)
+        out = np.zeros((ny * scale, nx * scale, 4), dtype=np.uint8)
+        rc = self.lib.itr_gpu_render_map(self.ctx, nx, ny, float(cell_size), _ptr(z, C.c_float), _ptr(v, C.c_float),
+                                         _ptr(w, C.c_float), int(mode), float(vex), int(scale), _ptr(out, C.c_uint8))
+        self._check(rc, "itr_gpu_render_map")
+        return out
+
     def record_baseline(self, p: SolverParams, terrain: PreparedTerrain, monitors: MonitorSet, checkpoint_interval: int = 64,
                         want_peak: bool = False, ledger_rows: int = 0) -> GpuRun:
         """itr_gpu_record_baseline: run the unedited terrain with checkpoints every

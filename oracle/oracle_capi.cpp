@@ -377,6 +377,65 @@ extern "C" void orc_flat_run64(int kernel, int64_t nx, int64_t ny, double dx, do
   write_result(R, S, out_s, mon_max, mon_tmax, ledger, max_rows, h_out, qx_out, qy_out, peak, peak_step);
 }
 
+// The result viewer's map (viewer/viewer.js:72-100, ramps :55-71), restated in f32 as the
+// fragment shader computes it, one pixel per (scale x scale) of a cell: the checker for the
+// device image. rgba gets (scale nx) x (scale ny) pixels, row 0 north.
+static float orc_mix(float a, float b, float f) { return a * (1.0f - f) + b * f; }
+static void orc_ramp(const float (*C)[3], int n, float t, float* o) {
+  const float x = std::fmin(std::fmax(t, 0.0f), 1.0f) * (float)(n - 1);
+  const int i = std::min((int)std::floor(x), n - 2);
+  const float f = x - (float)i;
+  for (int k = 0; k < 3; ++k) o[k] = orc_mix(C[i][k], C[i + 1][k], f);
+}
+extern "C" void orc_render_map(int nx, int ny, double cell_size, const float* z, const float* value, const float* dz,
+                               int mode, float vex, int scale, uint8_t* rgba) {
+  static const float DR[8][3] = {{0.8706f, 0.9216f, 0.9686f}, {0.7765f, 0.8588f, 0.9373f}, {0.6196f, 0.7922f, 0.8824f},
+                                 {0.4196f, 0.6824f, 0.8392f}, {0.2588f, 0.5725f, 0.7765f}, {0.1294f, 0.4431f, 0.7098f},
+                                 {0.0314f, 0.3176f, 0.6118f}, {0.0314f, 0.1882f, 0.4196f}};
+  static const float FR[7][3] = {{0.1294f, 0.4000f, 0.6745f}, {0.4039f, 0.6627f, 0.8118f}, {0.8196f, 0.8980f, 0.9412f},
+                                 {0.9686f, 0.9686f, 0.9686f}, {0.9922f, 0.8588f, 0.7804f}, {0.9373f, 0.5412f, 0.3843f},
+                                 {0.6980f, 0.0941f, 0.1686f}};
+  const float cs = (float)cell_size;
+  auto Z = [&](int cx, int cy) {
+    cx = std::min(std::max(cx, 0), nx - 1); cy = std::min(std::max(cy, 0), ny - 1);
+    const float v = z[(size_t)cy * nx + cx];
+    return v != v ? 1e9f : v;
+  };
+  auto u8 = [](float v) { return (uint8_t)std::nearbyint(std::fmin(std::fmax(v, 0.0f), 1.0f) * 255.0f); };
+  const int W = nx * scale, H = ny * scale;
+  for (int py = 0; py < H; ++py)
+    for (int px = 0; px < W; ++px) {
+      const float cxf = ((float)px + 0.5f) / (float)scale, cyf = ((float)py + 0.5f) / (float)scale;
+      const int cx = (int)cxf, cy = (int)cyf;
+      const size_t i = (size_t)cy * nx + cx;
+      float col[3];
+      const float zc = z[i];
+      if (zc != zc || zc > 1e8f) {
+        col[0] = col[1] = col[2] = 0.87f;
+      } else {
+        float gx = (Z(cx + 1, cy) - Z(cx - 1, cy)) / (2.0f * cs) * vex;
+        float gy = (Z(cx, cy + 1) - Z(cx, cy - 1)) / (2.0f * cs) * vex;
+        if (std::fabs(gx) > 1e6f) gx = 0.0f;
+        if (std::fabs(gy) > 1e6f) gy = 0.0f;
+        const float nl = std::sqrt(gx * gx + gy * gy + 1.0f);
+        const float ll = std::sqrt(0.25f + 0.25f + 0.49f);
+        const float d = (-gx / nl) * (-0.5f / ll) + (gy / nl) * (0.5f / ll) + (1.0f / nl) * (0.7f / ll);
+        const float g = 0.3f + 0.6f * std::fmin(std::fmax(d, 0.0f), 1.0f);
+        col[0] = col[1] = col[2] = g;
+        const float v = value[i];
+        if (mode == 0) { if (v > 0.0050f) orc_ramp(DR, 8, std::log(v / 0.0050f) / std::log(400.0f), col); }
+        else if (std::fabs(v) > 0.005f) orc_ramp(FR, 7, std::fmin(std::fmax(v / 0.20f, -1.0f), 1.0f) * 0.5f + 0.5f, col);
+        if (dz) {
+          const float s = (cxf + cyf) * 0.5f;
+          if (dz[i] > 0.01f && s - std::floor(s) < 0.5f)
+            for (int k = 0; k < 3; ++k) col[k] = orc_mix(col[k], 0.0f, 0.7f);
+        }
+      }
+      uint8_t* o = rgba + ((size_t)py * W + px) * 4;
+      o[0] = u8(col[0]); o[1] = u8(col[1]); o[2] = u8(col[2]); o[3] = 255;
+    }
+}
+
 // Candidate-parallel f32 fused runs (one design per thread, the reference's default search
 // mode, crates/itr-opt/src/evaluator.rs:337-352), for the timed CPU baseline. Face arrays are
 // per design (n_designs * ny*(nx+1) and n_designs * (ny+1)*nx). Returns wall seconds; steps

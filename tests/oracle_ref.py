@@ -71,6 +71,7 @@ def lib():
     L.orc_flat_batch.argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, _f, _f, _u8, _f, _f, _f, _d, _d,
                                  _d, C.c_int, C.c_int, _u32, _d, _d]
     L.orc_validation.argtypes = [C.c_int, C.c_int, _d]
+    L.orc_render_map.argtypes = [C.c_int, C.c_int, C.c_double, _f, _f, _f, C.c_int, C.c_float, C.c_int, _u8]
     _lib = L
     return L
 
@@ -198,6 +199,18 @@ def _run(call, nx, ny, params, monitors, objective, baseline, incumbent, cut, fi
                 dt_min=out_s[10], dt_max=out_s[11], dt_mean=out_s[12], cell_updates=int(out_s[13]),
                 rows_skipped=int(out_s[14]), monitor_max=mm[:nm].copy(), monitor_tmax=mt[:nm].copy(),
                 ledger=led[:min(n_rows, max_rows)].copy(), h=h, qx=qx, qy=qy, peak=pk, peak_step=ps)
+
+
+def render_map(z, value, cell_size, mode=0, vex=1.0, scale=1, worse_dz=None):
+    """The viewer's map image restated on the CPU (RGBA uint8, (scale ny, scale nx, 4))."""
+    z = np.ascontiguousarray(z, dtype=np.float32)
+    ny, nx = z.shape
+    v = np.ascontiguousarray(value, dtype=np.float32).reshape(ny, nx)
+    w = None if worse_dz is None else np.ascontiguousarray(worse_dz, dtype=np.float32).reshape(ny, nx)
+    out = np.zeros((ny * scale, nx * scale, 4), dtype=np.uint8)
+    lib().orc_render_map(nx, ny, float(cell_size), P(z, C.c_float), P(v, C.c_float), P(w, C.c_float), int(mode), float(vex),
+                         int(scale), P(out, C.c_uint8))
+    return out
 
 
 def bnd_dict(base, terrain):
