@@ -129,7 +129,9 @@ struct itr_ctx {
   // tiled batched path: state planes, tile partials, control blocks of all designs
   DevBuf tH, tQX, tQY, tpart, tctl;
   // adjoint: argmax states, (dt, rain) ring, checkpoints, tape, adjoint state, gradients
-  DevBuf aTpk, aRing, aTape, aLA, aLB, aGx, aGy, aSeg, aNst, aSeedC, aSeedS, aSeedW, aSeedN, aTmon;
+  DevBuf aTpk, aRing, aTape, aTape2, aLA, aLB, aGx, aGy, aSeg, aNst, aSeedC, aSeedS, aSeedW, aSeedN, aTmon;
+  cudaStream_t stream2 = nullptr;   // adjoint: the replay of the next segment runs beside the backward steps
+  cudaEvent_t ev_rep[2] = {nullptr, nullptr}, ev_adj[2] = {nullptr, nullptr}, ev_bwd = nullptr;
   HostBuf aRingH;
   std::vector<DevBuf> aCkpt;
   struct Vjp* vjp = nullptr;
@@ -515,7 +517,7 @@ void itr_gpu_destroy(itr_ctx* ctx) {
   for (DevBuf* b : {&ctx->wet, &ctx->gn2, &ctx->bc, &ctx->dzx, &ctx->dzy, &ctx->dzx2, &ctx->dzy2, &ctx->h0, &ctx->cut, &ctx->fill,
                     &ctx->mon, &ctx->obj_i, &ctx->obj_d, &ctx->peak, &ctx->depth, &ctx->ledger, &ctx->out, &ctx->mmax,
                     &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
-                    &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy,
+                    &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aTape2, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy,
                     &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon,
                     &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut, &ctx->wsb, &ctx->rIn, &ctx->rOut})
     b->release();
@@ -526,6 +528,12 @@ void itr_gpu_destroy(itr_ctx* ctx) {
     delete ctx->rec;
   }
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->ev_rep[i]) cudaEventDestroy(ctx->ev_rep[i]);
+    if (ctx->ev_adj[i]) cudaEventDestroy(ctx->ev_adj[i]);
+  }
+  if (ctx->ev_bwd) cudaEventDestroy(ctx->ev_bwd);
+  if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   ctx->aRingH.release();
   ctx->mVol.release();
   ctx->stage.release();
@@ -713,6 +721,7 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
                         const float* hmm, const DesignOut* hdo) {
   Vjp* V = ctx->vjp;
   const int nx = F.nx, ny = F.ny, K = V->K;
+  int rc_ = ITR_OK;
   const size_t N = (size_t)nx * ny, SX = (size_t)ny * (nx + 1), SY = (size_t)(ny + 1) * nx;
   const cudaStream_t st = ctx->stream;
   // argmax states of the monitored cells
@@ -794,20 +803,55 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
         q[2] = have ? V->dt[d][3 * s + 2] : 0.0;
       }
   CU(cudaMemcpyAsync(ctx->aSeg.p, segh, nblocks * seg_elems * 8, cudaMemcpyHostToDevice, st));
+  // Two tapes: segment b's replay fills tape b % 2 on the second stream while the backward
+  // steps of segment b + 1 read the other tape on the context stream, so each launch's
+  // last partial wave overlaps the other stream's blocks. Events keep the order: a
+  // segment's backward waits for its replay, a replay for the backward that last read its
+  // tape. Same kernels, same order per tape: the gradients are unchanged.
+  if (!ctx->stream2) {
+    CU(cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      CU(cudaEventCreateWithFlags(&ctx->ev_rep[i], cudaEventDisableTiming));
+      CU(cudaEventCreateWithFlags(&ctx->ev_adj[i], cudaEventDisableTiming));
+    }
+    CU(cudaEventCreateWithFlags(&ctx->ev_bwd, cudaEventDisableTiming));
+  }
+  CU(ctx->aTape2.ensure((size_t)K * S3 * 4));
+  float* tapes[2] = {ctx->aTape.as<float>(), ctx->aTape2.as<float>()};
+  const cudaStream_t s2 = ctx->stream2;
+  CU(cudaEventRecord(ctx->ev_bwd, st));   // the set-up above, before the first replay
+  CU(cudaStreamWaitEvent(s2, ctx->ev_bwd, 0));
+  auto replay = [&](uint64_t b) -> int {
+    const int slot = (int)(b & 1u);
+    if (b + 2 < nblocks) CU(cudaStreamWaitEvent(s2, ctx->ev_adj[slot], 0));   // segment b + 2's backward is done with it
+    CU(cudaMemcpyAsync(tapes[slot], ctx->aCkpt[b].p, S3 * 4, cudaMemcpyDeviceToDevice, s2));
+    AdjArgs R = A;
+    R.tape = tapes[slot];
+    R.step0 = b * K;
+    R.seg = ctx->aSeg.as<double>() + b * seg_elems;
+    for (int j = 0; j + 1 < K; ++j) {
+      if (bnd) k_adj_replay<true><<<grid, kTileThreads, 0, s2>>>(R, j);
+      else k_adj_replay<false><<<grid, kTileThreads, 0, s2>>>(R, j);
+    }
+    CU(cudaEventRecord(ctx->ev_rep[slot], s2));
+    return ITR_OK;
+  };
+  rc_ = replay(nblocks - 1);
+  if (rc_ != ITR_OK) return rc_;
   for (uint64_t b = nblocks; b-- > 0;) {   // no host round trip between segments
-    CU(cudaMemcpyAsync(ctx->aTape.p, ctx->aCkpt[b].p, S3 * 4, cudaMemcpyDeviceToDevice, st));
+    const int slot = (int)(b & 1u);
+    CU(cudaStreamWaitEvent(st, ctx->ev_rep[slot], 0));
+    A.tape = tapes[slot];
     A.step0 = b * K;
     A.seg = ctx->aSeg.as<double>() + b * seg_elems;
-    for (int j = 0; j + 1 < K; ++j) {
-      if (bnd) k_adj_replay<true><<<grid, kTileThreads, 0, st>>>(A, j);
-      else k_adj_replay<false><<<grid, kTileThreads, 0, st>>>(A, j);
-    }
     for (int j = K - 1; j >= 0; --j) {
       A.lin = lin; A.lout = lout;
       if (bnd) k_adj_step<true><<<grid, kTileThreads, 0, st>>>(A, j);
       else k_adj_step<false><<<grid, kTileThreads, 0, st>>>(A, j);
       std::swap(lin, lout);
     }
+    CU(cudaEventRecord(ctx->ev_adj[slot], st));
+    if (b > 0) { rc_ = replay(b - 1); if (rc_ != ITR_OK) return rc_; }
     CU(cudaGetLastError());
   }
   CU(cudaMemcpyAsync(V->gx, ctx->aGx.p, (size_t)n * SX * 8, cudaMemcpyDeviceToHost, st));
