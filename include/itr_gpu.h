@@ -234,14 +234,22 @@ int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_groups, cons
  * The forward runs to completion on the tiled path (aborts off), keeping the state every
  * checkpoint_interval steps; the backward recomputes each segment and steps the discrete
  * adjoint back through it with the recorded dt sequence held fixed. results are the
- * forward's, as itr_gpu_run_batch gives them. Signed face mode only (ITR_UNSUPPORTED
- * otherwise); obj must have at least one asset. With stage cells the stage ghosts' depths
+ * forward's, as itr_gpu_run_batch gives them. Signed faces; a crest-mode grid (coarse
+ * levels) needs itr_gpu_vjp_crest (ITR_UNSUPPORTED here); obj must have at least one asset.
+ * With stage cells the stage ghosts' depths
  * (stage - z_edge) are held fixed: the result is the derivative with respect to the face
  * jumps alone. Device memory: checkpoints of 12 B per cell
  * per design per interval, a tape of checkpoint_interval states. */
 int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n_designs, const itr_design* designs,
                 const uint32_t* monitors, int32_t n_mon, const itr_objective* obj, int32_t checkpoint_interval,
                 itr_result* results, double* dj_ddzx, double* dj_ddzy);
+
+/* itr_gpu_vjp for a crest-mode grid (face_crest, numerics.rs:114-129: two non-negative jumps
+ * per face, one for each side): dj_ddzx / dj_ddzy receive dJ/d(dzx) / dJ/d(dzy) (the first
+ * jumps, itr_design.dzx/dzy) and dj_ddzx2 / dj_ddzy2 dJ/d(dzx2) / dJ/d(dzy2), same layouts. */
+int itr_gpu_vjp_crest(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n_designs, const itr_design* designs,
+                      const uint32_t* monitors, int32_t n_mon, const itr_objective* obj, int32_t checkpoint_interval,
+                      itr_result* results, double* dj_ddzx, double* dj_ddzy, double* dj_ddzx2, double* dj_ddzy2);
 
 /* Device time of the last itr_gpu_vjp: taped forward (kernels and checkpoints) and backward. */
 int itr_gpu_last_vjp_timing(itr_ctx* ctx, double* forward_ms, double* backward_ms);

@@ -24,7 +24,8 @@
 // ghost copies (a stage ghost's momentum, an inflow ghost's depth where it exceeds the
 // critical depth). The stage depths themselves (stage - z behind the edge) are held fixed:
 // the gradient is the one with respect to the face jumps alone.
-// Signed face mode (fidelity level 1) only.
+// Crest faces (coarse fidelity levels): two jumps per face, d_l and d_r, each side reduced by
+// its own jump; the gradient comes in both jump arrays.
 #pragma once
 #include "itr_plain.cuh"
 
@@ -39,6 +40,8 @@ struct AdjArgs {
   const float* bh;                    // stage-ghost depths per design [2 nx + 2 ny], or NULL
   const float* dzx;                   // all designs, as the forward
   const float* dzy;
+  const float* dzx2;                  // crest mode: the second jumps, else NULL
+  const float* dzy2;
   const unsigned long long* n_steps;  // per design: steps of the forward run
   const double* seg;                  // per design [K][3]: (dt, rain, t) of this segment's steps
   int K;
@@ -48,6 +51,8 @@ struct AdjArgs {
   float* lout;                        // per design [3][N]: adjoint of the state before it
   double* gdzx;                       // per design ny*(nx+1)
   double* gdzy;                       // per design (ny+1)*nx
+  double* gdzx2;                      // crest mode: gradients of the second jumps
+  double* gdzy2;
   const unsigned* seed_cell;          // per design max_seeds: argmax cell of an asset
   const unsigned* seed_state;         //   the state index at which it peaked
   const float* seed_w;                //   w_k sigmoid((P_k - eta_k) / tau)
@@ -110,7 +115,7 @@ ITR_DEV void ghost_bwd(int code, float lh, float lu, float lv, float lc, float h
 }
 
 // ---- forward replay: x_{n+1} = F(x_n) with the recorded (dt, rain) ----
-template <bool BND>
+template <bool BND, bool CREST>
 __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A, int j) {
   __shared__ float sh[18 * 18], su[18 * 18], sv[18 * 18], sc[18 * 18], sqx[18 * 18], sqy[18 * 18];
   __shared__ FaceF fx[16 * 17], fy[17 * 16];
@@ -125,6 +130,8 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A,
   const StepK k = step_consts(A.P, sg[0], sg[1]);
   const float* dzx = A.dzx + d * SX;
   const float* dzy = A.dzy + d * SY;
+  const float* dzx2 = CREST ? A.dzx2 + d * SX : nullptr;
+  const float* dzy2 = CREST ? A.dzy2 + d * SY : nullptr;
   const float* bh = BND && A.bh ? A.bh + (size_t)d * (2 * nx + 2 * ny) : nullptr;
   adj_inflow<BND>(A, sg[2], sinf);
   const int gx0 = blockIdx.x * kTile, gy0 = blockIdx.y * kTile;
@@ -136,6 +143,7 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A,
   const size_t xo = (size_t)(gy0 + fxr) * (nx + 1) + gx0 + fxcol;
   const size_t yo = (size_t)(gy0 + fyr_) * nx + gx0 + fycol;
   const float xd = xv ? dzx[xo] : 0.0f, yd = yv ? dzy[yo] : 0.0f;
+  const float xd2 = (CREST && xv) ? dzx2[xo] : 0.0f, yd2 = (CREST && yv) ? dzy2[yo] : 0.0f;
   const int lx = li % 16, ly = li / 16, gx = gx0 + lx, gy = gy0 + ly;
   const bool cv = li < 256 && gx < nx && gy < ny;
   const size_t gi = (size_t)gy * nx + gx;
@@ -150,11 +158,11 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A,
   __syncthreads();
   if (xv) {
     const int a = (fxr + 1) * 18 + fxcol;
-    fx[li] = face<true, false>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], xd, 0.0f, k);
+    fx[li] = face<true, CREST>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], xd, xd2, k);
   }
   if (yv) {
     const int a = fyr_ * 18 + fycol + 1, b = a + 18;
-    fy[li] = face<false, false>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], yd, 0.0f, k);
+    fy[li] = face<false, CREST>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], yd, yd2, k);
   }
   __syncthreads();
   if (cv) {
@@ -167,19 +175,22 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_adj_replay(const AdjArgs A,
 
 // ---- adjoints of the pieces of one step ----
 
-// Input adjoints of face_signed + hll (numerics.rs:60-112) given the output adjoints.
-struct FaceBwd { float hl, ul, vl, cl, hr, ur, vr, cr, dz; };
+// Input adjoints of face_signed / face_crest + hll (numerics.rs:60-129) given the output
+// adjoints. dz: the (first) jump's adjoint; dz2: the crest face's second jump's.
+struct FaceBwd { float hl, ul, vl, cl, hr, ur, vr, cr, dz, dz2; };
 
-template <bool NORMAL_X>
+template <bool NORMAL_X, bool CREST>
 ITR_DEV FaceBwd face_bwd(float hl, float ul, float vl, float cl, float hr, float ur, float vr, float cr, float dz,
-                         const StepK& k, float lm, float lnl, float lnr, float lt) {
-  // forward, as face_signed / hll compute it
+                         float dz2, const StepK& k, float lm, float lnl, float lnr, float lt) {
+  // forward, as face_signed / face_crest and hll compute it
   const bool pos = dz > 0.0f;
-  const float a_l = hl - rmax(dz, 0.0f), a_r = hr - rmax(-dz, 0.0f);
+  const float a_l = CREST ? hl - dz : hl - rmax(dz, 0.0f), a_r = CREST ? hr - dz2 : hr - rmax(-dz, 0.0f);
   const float hsl = rmax(a_l, 0.0f), hsr = rmax(a_r, 0.0f);
   const float hred = pos ? hsl : hsr;
-  const float cred = sqrt_rn(k.g * hred);
-  const float csl = pos ? cred : cl, csr = pos ? cr : cred;
+  const float cred = CREST ? 0.0f : sqrt_rn(k.g * hred);
+  const float csl_c = (CREST && dz > 0.0f) ? sqrt_rn(k.g * hsl) : cl;
+  const float csr_c = (CREST && dz2 > 0.0f) ? sqrt_rn(k.g * hsr) : cr;
+  const float csl = CREST ? csl_c : (pos ? cred : cl), csr = CREST ? csr_c : (pos ? cr : cred);
   const float unl = NORMAL_X ? ul : vl, utl = NORMAL_X ? vl : ul;
   const float unr = NORMAL_X ? ur : vr, utr = NORMAL_X ? vr : ur;
   const bool dry_l = !(hsl > 0.0f), dry_r = !(hsr > 0.0f);
@@ -238,14 +249,20 @@ ITR_DEV FaceBwd face_bwd(float hl, float ul, float vl, float cl, float hr, float
     lcsl += 0.5f * lcs; lcsr += 0.5f * lcs; lunl += 0.25f * lcs; lunr -= 0.25f * lcs;
   }
   FaceBwd b;
-  float lcred = 0.0f;
   b.cl = 0.0f; b.cr = 0.0f;
-  if (pos) { lcred += lcsl; b.cr = lcsr; } else { b.cl = lcsl; lcred += lcsr; }
-  const float lhred = cred > 0.0f ? lcred * k.g * 0.5f / cred : 0.0f;
-  if (pos) lhsl += lhred; else lhsr += lhred;
+  if (CREST) {   // each side's celerity is its reduced depth's where its jump is positive
+    if (dz > 0.0f) { if (csl > 0.0f) lhsl += lcsl * k.g * 0.5f / csl; } else b.cl = lcsl;
+    if (dz2 > 0.0f) { if (csr > 0.0f) lhsr += lcsr * k.g * 0.5f / csr; } else b.cr = lcsr;
+  } else {
+    float lcred = 0.0f;
+    if (pos) { lcred += lcsl; b.cr = lcsr; } else { b.cl = lcsl; lcred += lcsr; }
+    const float lhred = cred > 0.0f ? lcred * k.g * 0.5f / cred : 0.0f;
+    if (pos) lhsl += lhred; else lhsr += lhred;
+  }
   const float la_l = a_l > 0.0f ? lhsl : 0.0f, la_r = a_r > 0.0f ? lhsr : 0.0f;
   b.hl = la_l; b.hr = la_r;
-  b.dz = (dz > 0.0f ? -la_l : 0.0f) + (dz < 0.0f ? la_r : 0.0f);
+  if (CREST) { b.dz = -la_l; b.dz2 = -la_r; }
+  else { b.dz = (dz > 0.0f ? -la_l : 0.0f) + (dz < 0.0f ? la_r : 0.0f); b.dz2 = 0.0f; }
   b.ul = NORMAL_X ? lunl : lutl; b.vl = NORMAL_X ? lutl : lunl;
   b.ur = NORMAL_X ? lunr : lutr; b.vr = NORMAL_X ? lutr : lunr;
   return b;
@@ -295,11 +312,12 @@ ITR_DEV void sources_bwd(float h, float qx, float qy, const FaceF& w, const Face
 // four faces' input adjoints (ghost sides folded back onto the interior cell).
 constexpr int kR = 20, kQ = 18;
 
-template <bool BND>
+template <bool BND, bool CREST>
 __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int j) {
   __shared__ float sh[kR * kR], sqx[kR * kR], sqy[kR * kR], su[kR * kR], sv[kR * kR], sc[kR * kR];
   __shared__ FaceF fx[kQ * 19], fy[19 * kQ];           // forward faces of the 18x18 cells
   __shared__ float jx[kQ * 19], jy[19 * kQ];            // their jumps
+  __shared__ float jx2[CREST ? kQ * 19 : 1], jy2[CREST ? 19 * kQ : 1];   // crest: second jumps
   __shared__ float l1[3][kQ * kQ];                      // adjoint of (h1, qx1, qy1)
   __shared__ float bx[16 * 17][8], by[17 * 16][8];      // face input adjoints: L (h,u,v,c), R (h,u,v,c)
   __shared__ float2 sinf[kMaxInflow];                   // the step's inflow group values
@@ -324,22 +342,29 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
   const StepK k = step_consts(A.P, sg[0], sg[1]);
   const float* dzx = A.dzx + d * SX;
   const float* dzy = A.dzy + d * SY;
+  const float* dzx2 = CREST ? A.dzx2 + d * SX : nullptr;
+  const float* dzy2 = CREST ? A.dzy2 + d * SY : nullptr;
   const float* bh = BND && A.bh ? A.bh + (size_t)d * (2 * nx + 2 * ny) : nullptr;
   adj_inflow<BND>(A, sg[2], sinf);
   // 1. state and velocities of the 20x20 region; the face jumps and this thread's old
   //    gradient sums are loaded first, so all these loads are in flight together
   float jxa = 0.0f, jxb = 0.0f, jya = 0.0f, jyb = 0.0f;
   const int e2 = li + kTileThreads;
-  auto xjump = [&](int e) -> float {
+  auto xjump = [&](const float* a, int e) -> float {
     const int jr = e / 19, fi = e % 19, row = gy0 - 1 + jr, f = gx0 - 1 + fi;
-    return (row >= 0 && row < ny && f >= 0 && f <= nx) ? dzx[(size_t)row * (nx + 1) + f] : 0.0f;
+    return (row >= 0 && row < ny && f >= 0 && f <= nx) ? a[(size_t)row * (nx + 1) + f] : 0.0f;
   };
-  auto yjump = [&](int e) -> float {
+  auto yjump = [&](const float* a, int e) -> float {
     const int fr = e / kQ, ic = e % kQ, col = gx0 - 1 + ic, f = gy0 - 1 + fr;
-    return (col >= 0 && col < nx && f >= 0 && f <= ny) ? dzy[(size_t)f * nx + col] : 0.0f;
+    return (col >= 0 && col < nx && f >= 0 && f <= ny) ? a[(size_t)f * nx + col] : 0.0f;
   };
-  jxa = xjump(li); jya = yjump(li);
-  if (e2 < kQ * 19) { jxb = xjump(e2); jyb = yjump(e2); }
+  jxa = xjump(dzx, li); jya = yjump(dzy, li);
+  if (e2 < kQ * 19) { jxb = xjump(dzx, e2); jyb = yjump(dzy, e2); }
+  float jx2a = 0.0f, jx2b = 0.0f, jy2a = 0.0f, jy2b = 0.0f;
+  if (CREST) {
+    jx2a = xjump(dzx2, li); jy2a = yjump(dzy2, li);
+    if (e2 < kQ * 19) { jx2b = xjump(dzx2, e2); jy2b = yjump(dzy2, e2); }
+  }
   // the faces this thread differentiates in step 4 and whether its tile owns them
   const int yr4 = li / 17 + 1, xl4 = li % 17 + 1, yt4 = li / 16 + 1, xc4 = li % 16 + 1;
   const int row4 = gy0 - 1 + yr4, fx4 = gx0 - 1 + xl4, col4 = gx0 - 1 + xc4, fy4 = gy0 - 1 + yt4;
@@ -348,6 +373,9 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
   double* gxp = A.gdzx + d * SX + (size_t)row4 * (nx + 1) + fx4;
   double* gyp = A.gdzy + d * SY + (size_t)fy4 * nx + col4;
   const double gx_old = xown ? *gxp : 0.0, gy_old = yown ? *gyp : 0.0;
+  double* gxp2 = CREST ? A.gdzx2 + d * SX + (size_t)row4 * (nx + 1) + fx4 : nullptr;
+  double* gyp2 = CREST ? A.gdzy2 + d * SY + (size_t)fy4 * nx + col4 : nullptr;
+  const double gx2_old = (CREST && xown) ? *gxp2 : 0.0, gy2_old = (CREST && yown) ? *gyp2 : 0.0;
   for (int e = li; e < kR * kR; e += kTileThreads) {
     const int ix = e % kR, iy = e / kR;
     float h, qx, qy, u, v, c;
@@ -357,6 +385,10 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
   }
   jx[li] = jxa; jy[li] = jya;
   if (e2 < kQ * 19) { jx[e2] = jxb; jy[e2] = jyb; }
+  if (CREST) {
+    jx2[li] = jx2a; jy2[li] = jy2a;
+    if (e2 < kQ * 19) { jx2[e2] = jx2b; jy2[e2] = jy2b; }
+  }
   __syncthreads();
   // 2. forward faces of the 18x18 cells: x-face (jr, fi) joins region cells (fi, jr+1) and
   //    (fi+1, jr+1); y-face (fr, ic) joins (ic+1, fr) and (ic+1, fr+1)
@@ -367,7 +399,8 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
       FaceF o{};
       if (row >= 0 && row < ny && f >= 0 && f <= nx) {
         const int a = (jr + 1) * kR + fi;
-        o = face<true, false>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], jx[e], 0.0f, k);
+        o = face<true, CREST>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], jx[e],
+                              CREST ? jx2[e] : 0.0f, k);
       }
       fx[e] = o;
     }
@@ -377,7 +410,7 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
       FaceF o{};
       if (col >= 0 && col < nx && f >= 0 && f <= ny) {
         const int a = fr * kR + ic + 1, b = a + kR;
-        o = face<false, false>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], jy[e], 0.0f, k);
+        o = face<false, CREST>(sh[a], su[a], sv[a], sc[a], sh[b], su[b], sv[b], sc[b], jy[e], CREST ? jy2[e] : 0.0f, k);
       }
       fy[e] = o;
     }
@@ -417,11 +450,12 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
         const float lnl = -k.dtdx * l1[1][L], lnr = k.dtdx * l1[1][R];
         const float lt = -k.dtdx * l1[2][L] + k.dtdx * l1[2][R];
         const int a = (yr + 1) * kR + xl;   // region cell of L
-        const float dz = jx[yr * 19 + xl];
-        const FaceBwd b = face_bwd<true>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], dz, k,
+        const float dz = jx[yr * 19 + xl], dz2 = CREST ? jx2[yr * 19 + xl] : 0.0f;
+        const FaceBwd b = face_bwd<true, CREST>(sh[a], su[a], sv[a], sc[a], sh[a + 1], su[a + 1], sv[a + 1], sc[a + 1], dz, dz2, k,
                                          lm, lnl, lnr, lt);
         o[0] = b.hl; o[1] = b.ul; o[2] = b.vl; o[3] = b.cl; o[4] = b.hr; o[5] = b.ur; o[6] = b.vr; o[7] = b.cr;
         if (xown) *gxp = gx_old + (double)b.dz;
+        if (CREST && xown) *gxp2 = gx2_old + (double)b.dz2;
       }
     }
     {  // y-face between (xc, yt-1) and (xc, yt) of the 18x18 region, yt = 1..17
@@ -435,11 +469,12 @@ __global__ void __launch_bounds__(kTileThreads) k_adj_step(const AdjArgs A, int 
         const float lt = -k.dtdy * l1[1][T] + k.dtdy * l1[1][B];
         const float lnl = -k.dtdy * l1[2][T], lnr = k.dtdy * l1[2][B];
         const int a = yt * kR + xc + 1;      // region cell of T
-        const float dz = jy[yt * kQ + xc];
-        const FaceBwd b = face_bwd<false>(sh[a], su[a], sv[a], sc[a], sh[a + kR], su[a + kR], sv[a + kR], sc[a + kR], dz,
+        const float dz = jy[yt * kQ + xc], dz2 = CREST ? jy2[yt * kQ + xc] : 0.0f;
+        const FaceBwd b = face_bwd<false, CREST>(sh[a], su[a], sv[a], sc[a], sh[a + kR], su[a + kR], sv[a + kR], sc[a + kR], dz, dz2,
                                           k, lm, lnl, lnr, lt);
         o[0] = b.hl; o[1] = b.ul; o[2] = b.vl; o[3] = b.cl; o[4] = b.hr; o[5] = b.ur; o[6] = b.vr; o[7] = b.cr;
         if (yown) *gyp = gy_old + (double)b.dz;
+        if (CREST && yown) *gyp2 = gy2_old + (double)b.dz2;
       }
     }
   }

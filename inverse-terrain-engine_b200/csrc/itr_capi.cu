@@ -129,7 +129,7 @@ struct itr_ctx {
   // tiled batched path: state planes, tile partials, control blocks of all designs
   DevBuf tH, tQX, tQY, tpart, tctl;
   // adjoint: argmax states, (dt, rain) ring, checkpoints, tape, adjoint state, gradients
-  DevBuf aTpk, aRing, aTape, aTape2, aLA, aLB, aGx, aGy, aSeg, aNst, aSeedC, aSeedS, aSeedW, aSeedN, aTmon;
+  DevBuf aTpk, aRing, aTape, aTape2, aLA, aLB, aGx, aGy, aGx2, aGy2, aSeg, aNst, aSeedC, aSeedS, aSeedW, aSeedN, aTmon;
   cudaStream_t stream2 = nullptr;   // adjoint: the replay of the next segment runs beside the backward steps
   cudaEvent_t ev_rep[2] = {nullptr, nullptr}, ev_adj[2] = {nullptr, nullptr}, ev_bwd = nullptr;
   HostBuf aRingH;
@@ -517,7 +517,7 @@ void itr_gpu_destroy(itr_ctx* ctx) {
   for (DevBuf* b : {&ctx->wet, &ctx->gn2, &ctx->bc, &ctx->dzx, &ctx->dzy, &ctx->dzx2, &ctx->dzy2, &ctx->h0, &ctx->cut, &ctx->fill,
                     &ctx->mon, &ctx->obj_i, &ctx->obj_d, &ctx->peak, &ctx->depth, &ctx->ledger, &ctx->out, &ctx->mmax,
                     &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
-                    &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aTape2, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy,
+                    &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aTape2, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy, &ctx->aGx2, &ctx->aGy2,
                     &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon,
                     &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut, &ctx->wsb, &ctx->rIn, &ctx->rOut})
     b->release();
@@ -630,6 +630,8 @@ struct Vjp {
   uint64_t blocks = 0;                    // checkpoints written (one per block of K steps)
   double* gx;                             // host outputs
   double* gy;
+  double* gx2 = nullptr;                  // crest mode: gradients of the second jumps
+  double* gy2 = nullptr;
 };
 
 static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* launches) {
@@ -777,6 +779,12 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   CU(cudaMemsetAsync(ctx->aLA.p, 0, S3 * 4, st));
   CU(cudaMemsetAsync(ctx->aGx.p, 0, (size_t)n * SX * 8, st));
   CU(cudaMemsetAsync(ctx->aGy.p, 0, (size_t)n * SY * 8, st));
+  const bool crest = F.mode == ITR_FACE_CREST;
+  if (crest) {
+    CU(ctx->aGx2.ensure((size_t)n * SX * 8)); CU(ctx->aGy2.ensure((size_t)n * SY * 8));
+    CU(cudaMemsetAsync(ctx->aGx2.p, 0, (size_t)n * SX * 8, st));
+    CU(cudaMemsetAsync(ctx->aGy2.p, 0, (size_t)n * SY * 8, st));
+  }
   AdjArgs A;
   memset(&A, 0, sizeof(A));
   A.P = F.P; A.nx = nx; A.ny = ny; A.n_designs = n;
@@ -785,6 +793,10 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   A.seg = ctx->aSeg.as<double>(); A.K = K;
   A.tape = ctx->aTape.as<float>();
   A.gdzx = ctx->aGx.as<double>(); A.gdzy = ctx->aGy.as<double>();
+  if (crest) {
+    A.dzx2 = F.dzx2; A.dzy2 = F.dzy2;
+    A.gdzx2 = ctx->aGx2.as<double>(); A.gdzy2 = ctx->aGy2.as<double>();
+  }
   A.seed_cell = ctx->aSeedC.as<unsigned>(); A.seed_state = ctx->aSeedS.as<unsigned>(); A.seed_w = ctx->aSeedW.as<float>();
   A.seed_n = ctx->aSeedN.as<int>(); A.max_seeds = ms;
   const dim3 grid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile, (unsigned)n);
@@ -830,8 +842,13 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
     R.step0 = b * K;
     R.seg = ctx->aSeg.as<double>() + b * seg_elems;
     for (int j = 0; j + 1 < K; ++j) {
-      if (bnd) k_adj_replay<true><<<grid, kTileThreads, 0, s2>>>(R, j);
-      else k_adj_replay<false><<<grid, kTileThreads, 0, s2>>>(R, j);
+      if (crest) {
+        if (bnd) k_adj_replay<true, true><<<grid, kTileThreads, 0, s2>>>(R, j);
+        else k_adj_replay<false, true><<<grid, kTileThreads, 0, s2>>>(R, j);
+      } else {
+        if (bnd) k_adj_replay<true, false><<<grid, kTileThreads, 0, s2>>>(R, j);
+        else k_adj_replay<false, false><<<grid, kTileThreads, 0, s2>>>(R, j);
+      }
     }
     CU(cudaEventRecord(ctx->ev_rep[slot], s2));
     return ITR_OK;
@@ -846,8 +863,13 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
     A.seg = ctx->aSeg.as<double>() + b * seg_elems;
     for (int j = K - 1; j >= 0; --j) {
       A.lin = lin; A.lout = lout;
-      if (bnd) k_adj_step<true><<<grid, kTileThreads, 0, st>>>(A, j);
-      else k_adj_step<false><<<grid, kTileThreads, 0, st>>>(A, j);
+      if (crest) {
+        if (bnd) k_adj_step<true, true><<<grid, kTileThreads, 0, st>>>(A, j);
+        else k_adj_step<false, true><<<grid, kTileThreads, 0, st>>>(A, j);
+      } else {
+        if (bnd) k_adj_step<true, false><<<grid, kTileThreads, 0, st>>>(A, j);
+        else k_adj_step<false, false><<<grid, kTileThreads, 0, st>>>(A, j);
+      }
       std::swap(lin, lout);
     }
     CU(cudaEventRecord(ctx->ev_adj[slot], st));
@@ -856,6 +878,8 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   }
   CU(cudaMemcpyAsync(V->gx, ctx->aGx.p, (size_t)n * SX * 8, cudaMemcpyDeviceToHost, st));
   CU(cudaMemcpyAsync(V->gy, ctx->aGy.p, (size_t)n * SY * 8, cudaMemcpyDeviceToHost, st));
+  if (crest && V->gx2) CU(cudaMemcpyAsync(V->gx2, ctx->aGx2.p, (size_t)n * SX * 8, cudaMemcpyDeviceToHost, st));
+  if (crest && V->gy2) CU(cudaMemcpyAsync(V->gy2, ctx->aGy2.p, (size_t)n * SY * 8, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   return ITR_OK;
 }
@@ -1698,19 +1722,21 @@ extern "C" int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const i
   return rc;
 }
 
-extern "C" int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
-                           const uint32_t* mon, int32_t n_mon, const itr_objective* ob, int32_t checkpoint_interval,
-                           itr_result* res, double* dj_ddzx, double* dj_ddzy) {
+static int vjp_impl(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
+                    const uint32_t* mon, int32_t n_mon, const itr_objective* ob, int32_t checkpoint_interval,
+                    itr_result* res, double* dj_ddzx, double* dj_ddzy, double* dj_ddzx2, double* dj_ddzy2) {
   if (!ctx) return ITR_INVALID_ARG;
   if (!ob || ob->n_assets < 1) return fail(ctx, ITR_INVALID_ARG, "the adjoint needs an objective with assets");
-  if (!g || g->mode != ITR_FACE_SIGNED) return fail(ctx, ITR_UNSUPPORTED, "the adjoint supports signed face jumps only");
+  if (!g) return fail(ctx, ITR_INVALID_ARG, "grid is NULL");
+  if (g->mode == ITR_FACE_CREST && n > 0 && (!dj_ddzx2 || !dj_ddzy2))
+    return fail(ctx, ITR_UNSUPPORTED, "crest faces: use itr_gpu_vjp_crest for the second jumps' gradients");
   if (checkpoint_interval < 1 || checkpoint_interval > 65536) return fail(ctx, ITR_INVALID_ARG, "checkpoint interval out of range");
   if (n > 0 && (!dj_ddzx || !dj_ddzy)) return fail(ctx, ITR_INVALID_ARG, "gradient outputs are NULL");
   itr_objective o = *ob;          // the taped forward runs every design to its end
   o.guard_abort = 0;
   o.has_incumbent = 0;
   Vjp V;
-  V.K = checkpoint_interval; V.gx = dj_ddzx; V.gy = dj_ddzy;
+  V.K = checkpoint_interval; V.gx = dj_ddzx; V.gy = dj_ddzy; V.gx2 = dj_ddzx2; V.gy2 = dj_ddzy2;
   ctx->vjp = &V;
   const int rc = itr_gpu_run_batch(ctx, p, g, n, ds, mon, n_mon, &o, res);
   ctx->vjp = nullptr;
@@ -1789,6 +1815,20 @@ extern "C" int itr_gpu_vjp_primitives(itr_ctx* ctx, const itr_params* p, const i
   }
   CU(cudaStreamSynchronize(st));
   return ITR_OK;
+}
+
+extern "C" int itr_gpu_vjp(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
+                           const uint32_t* mon, int32_t n_mon, const itr_objective* ob, int32_t checkpoint_interval,
+                           itr_result* res, double* dj_ddzx, double* dj_ddzy) {
+  return vjp_impl(ctx, p, g, n, ds, mon, n_mon, ob, checkpoint_interval, res, dj_ddzx, dj_ddzy, nullptr, nullptr);
+}
+
+extern "C" int itr_gpu_vjp_crest(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
+                                 const uint32_t* mon, int32_t n_mon, const itr_objective* ob, int32_t checkpoint_interval,
+                                 itr_result* res, double* dj_ddzx, double* dj_ddzy, double* dj_ddzx2, double* dj_ddzy2) {
+  if (ctx && g && g->mode != ITR_FACE_CREST) return fail(ctx, ITR_INVALID_ARG, "itr_gpu_vjp_crest needs a crest-mode grid");
+  if (ctx && n > 0 && (!dj_ddzx2 || !dj_ddzy2)) return fail(ctx, ITR_INVALID_ARG, "second-jump gradient outputs are NULL");
+  return vjp_impl(ctx, p, g, n, ds, mon, n_mon, ob, checkpoint_interval, res, dj_ddzx, dj_ddzy, dj_ddzx2, dj_ddzy2);
 }
 
 extern "C" int itr_gpu_last_vjp_timing(itr_ctx* ctx, double* forward_ms, double* backward_ms) {

@@ -108,6 +108,8 @@ SIGNATURES = {
     "itr_gpu_run_ladder": (C.c_int, [C.c_void_p, C.POINTER(Params), C.c_int32, C.POINTER(Group), C.POINTER(Result)]),
     "itr_gpu_vjp": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.c_int32, C.POINTER(Design), _u32p,
                               C.c_int32, C.POINTER(Objective), C.c_int32, C.POINTER(Result), _dp, _dp]),
+    "itr_gpu_vjp_crest": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.c_int32, C.POINTER(Design), _u32p,
+                                    C.c_int32, C.POINTER(Objective), C.c_int32, C.POINTER(Result), _dp, _dp, _dp, _dp]),
     "itr_gpu_last_vjp_timing": (C.c_int, [C.c_void_p, _dp, _dp]),
     "itr_gpu_render_map": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, _fp, _fp, _fp, C.c_int32, C.c_float,
                                      C.c_int32, _u8p]),

@@ -188,6 +188,8 @@ class GpuRun:
     dj_ddzx: np.ndarray | None = None   # itr_gpu_vjp: dJ/d(x-face jump), (ny, nx+1)
     dj_ddzy: np.ndarray | None = None   # itr_gpu_vjp: dJ/d(y-face jump), (ny+1, nx)
     warm_start_steps: int = 0           # steps taken over from the baseline record
+    dj_ddzx2: np.ndarray | None = None  # itr_gpu_vjp_crest: dJ/d(second x-face jump)
+    dj_ddzy2: np.ndarray | None = None
 
 
 @dataclass
@@ -408,13 +410,23 @@ class GpuSolver:
                 raise ValueError("the adjoint needs an objective")
             gx = np.zeros((n, ny, nx + 1), dtype=np.float64)
             gy = np.zeros((n, ny + 1, nx), dtype=np.float64)
-            rc = self.lib.itr_gpu_vjp(self.ctx, C.byref(P), C.byref(b["Gd"]), n, b["D"], _ptr(b["mon"], C.c_uint32), b["nm"],
-                                      C.byref(O), int(vjp_interval), R, _ptr(gx, C.c_double), _ptr(gy, C.c_double))
+            if base.mode == _lib.FACE_CREST:   # itr_gpu_vjp_crest: both jumps of every face
+                gx2 = np.zeros_like(gx)
+                gy2 = np.zeros_like(gy)
+                rc = self.lib.itr_gpu_vjp_crest(self.ctx, C.byref(P), C.byref(b["Gd"]), n, b["D"], _ptr(b["mon"], C.c_uint32),
+                                                b["nm"], C.byref(O), int(vjp_interval), R, _ptr(gx, C.c_double),
+                                                _ptr(gy, C.c_double), _ptr(gx2, C.c_double), _ptr(gy2, C.c_double))
+            else:
+                rc = self.lib.itr_gpu_vjp(self.ctx, C.byref(P), C.byref(b["Gd"]), n, b["D"], _ptr(b["mon"], C.c_uint32),
+                                          b["nm"], C.byref(O), int(vjp_interval), R, _ptr(gx, C.c_double), _ptr(gy, C.c_double))
         else:
             rc = self.lib.itr_gpu_run_batch(self.ctx, C.byref(P), C.byref(b["Gd"]), n, b["D"], _ptr(b["mon"], C.c_uint32),
                                             b["nm"], C.byref(O) if O is not None else None, R)
         self._check(rc, "itr_gpu_run_batch")
         runs = self._unpack(b, R, gx, gy)
+        if vjp_interval and base.mode == _lib.FACE_CREST:
+            for i, r in enumerate(runs):
+                r.dj_ddzx2, r.dj_ddzy2 = gx2[i], gy2[i]
         self.last_cell_updates = sum(r.cell_updates for r in runs)
         return runs
 

@@ -199,3 +199,50 @@ def test_gradient_with_stage_and_inflow_vs_f64_finite_differences(gpu):
         worst = max(worst, rel)
         assert rel <= FD_REL_TOL, f"{kind}-face {idx}: adjoint {ad:.6e} vs finite difference {fd:.6e} (rel {rel:.3%})"
     print(f"stage/inflow case: worst relative error vs f64 central differences: {worst:.3%}")
+
+
+def test_crest_gradient_vs_f64_finite_differences(gpu):
+    """Crest faces (a coarse fidelity level, face_crest: each side reduced by its own jump):
+    itr_gpu_vjp_crest gives dJ/d(first jump) and dJ/d(second jump) of every face, against
+    central differences of the f64 oracle on jumps well away from the d > 0 switch."""
+    base = synthetic_terrain(48, 32, 2.5, lambda x, y: 2.0 - 0.01 * x + 0.2 * math.sin(y / 15.0) + 0.1 * math.cos(x / 20.0)
+                             + 0.05 * math.sin(x / 3.0) * math.cos(y / 4.0), n=0.03,
+                             segments=[Segment("transmissive", "east")], level=2)
+    assert base.mode == 1
+    nx, ny = base.nx, base.ny
+    p = SolverParams(120.0, 30.0, rain=Hyetograph.from_mm_h([(0, 50), (60, 120), (120, 0)]), initial_depth=0.3)
+    t = PreparedTerrain(base)
+    cells = [5 * nx + 8, 9 * nx + 15, 12 * nx + 20]
+    probe = Objective(ObjectiveDef([Asset(f"a{i}", [c], 10.0) for i, c in enumerate(cells)], []))
+    r = gpu.run_batch(p, [t], probe.monitors)[0]
+    obj = Objective(ObjectiveDef([Asset(f"a{i}", [c], float(r.monitor_max[probe.monitors.position(c)]) - 0.004, 1.0 + i)
+                                  for i, c in enumerate(cells)], []))
+    run = gpu.vjp(p, [t], obj.monitors, obj, checkpoint_interval=16)[0]
+    grads = {"dzx": run.dj_ddzx, "dzy": run.dj_ddzy, "dzx2": run.dj_ddzx2, "dzy2": run.dj_ddzy2}
+    jumps = {"dzx": np.asarray(t.dzx, np.float64).reshape(ny, nx + 1), "dzy": np.asarray(t.dzy, np.float64).reshape(ny + 1, nx),
+             "dzx2": np.asarray(t.dzx2, np.float64).reshape(ny, nx + 1), "dzy2": np.asarray(t.dzy2, np.float64).reshape(ny + 1, nx)}
+    for a in grads.values():
+        assert np.all(np.isfinite(a))
+
+    def j(name, arr):
+        d = design_dict(t, p)
+        d[name] = arr
+        o = orc.flat_run64(base_arrays(base), d, p, obj.monitors)
+        return obj.evaluate(o["monitor_max"], 0.0, 0.0)["j_risk"]
+
+    worst, checked = 0.0, 0
+    for name, g in grads.items():
+        cand = np.abs(g) * (jumps[name] > 10 * FD_STEP_M)
+        for i in np.argsort(cand, axis=None)[-2:]:
+            idx = np.unravel_index(i, g.shape)
+            if cand[idx] == 0.0:
+                continue
+            up, dn = jumps[name].copy(), jumps[name].copy()
+            up[idx] += FD_STEP_M; dn[idx] -= FD_STEP_M
+            fd = (j(name, up) - j(name, dn)) / (2 * FD_STEP_M)
+            rel = abs(g[idx] - fd) / abs(fd)
+            worst = max(worst, rel)
+            checked += 1
+            assert rel <= FD_REL_TOL, f"{name} {idx}: adjoint {g[idx]:.6e} vs finite difference {fd:.6e} ({rel:.3%})"
+    assert checked >= 6
+    print(f"crest faces: worst relative error vs f64 central differences: {worst:.3%}")
