@@ -172,7 +172,7 @@ def cpu_baseline(sc, terrs, budget_s=20.0):
     wall, steps, _ = orc.flat_batch(threads, base_arrays(sc.base), [t.dzx for t in terrs[:n]], [t.dzy for t in terrs[:n]], None,
                                     p, sc.monitors)
     cs = float(steps.sum()) * sc.base.nx * sc.base.ny
-    return {"value": cs / wall, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+    return {"value": cs / wall, "unit": "cell-steps/s", "cores": threads, "kind": "port", "value_1_thread": rate1,
             "sample": f"{n} designs x first {p.duration_s:.0f} s of the storm (of {sc.params.duration_s:.0f} s), "
                       f"f32 fused CPU port, candidate-parallel on {threads} threads, {wall:.1f} s wall",
             "cell_steps": cs, "wall_s": wall}
@@ -422,7 +422,7 @@ def main():
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(sc, terrs)
-            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample", "value_1_thread")}
         line = {
             "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": k_total_ms / args.steps, "higher_is_better": True,
