@@ -606,7 +606,7 @@ static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid,
   for (uint64_t guard = 0;; ++guard) {
     for (int s = 0; s < ctx->steps_per_submit; ++s) {
       launch_update(A, grid, ctx->stream);
-      k_plain_finalize<<<1, 32, 0, ctx->stream>>>(A, n_blocks, 0);
+      k_plain_finalize<<<1, kFinThreads, 0, ctx->stream>>>(A, n_blocks, 0);
       *launches += 2;
     }
     CU(cudaMemcpyAsync(hctl, A.ctl, sizeof(PlainCtl), cudaMemcpyDeviceToHost, ctx->stream));
@@ -648,7 +648,7 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
   auto block = [&]() {
     for (int s = 0; s < K; ++s) {
       launch_update(A, grid, st);
-      k_plain_finalize<<<n, 32, 0, st>>>(A, nb, 0);
+      k_plain_finalize<<<n, kFinThreads, 0, st>>>(A, nb, 0);
     }
   };
   cudaGraphExec_t ge = nullptr;

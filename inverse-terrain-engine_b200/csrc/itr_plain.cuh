@@ -222,6 +222,15 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArg
   const int wid = li >> 5;
   if ((li & 31) == 0) { wmax[wid] = m; wbad[wid] = b; for (int j = 0; j < 5; ++j) wsum[wid][j] = acc[j]; }
   __syncthreads();
+  double yt = 0.0, yb = 0.0;   // the tile's top / bottom edge fluxes, summed by warp 0
+  if (li < 32) {
+    yt = li < kTile ? yedge[0][li] : 0.0;
+    yb = li < kTile ? yedge[1][li] : 0.0;
+    for (int o = kTile / 2; o > 0; o >>= 1) {
+      yt += __shfl_xor_sync(0xffffffffu, yt, o);
+      yb += __shfl_xor_sync(0xffffffffu, yb, o);
+    }
+  }
   if (li == 0) {
     float mm = 0.0f; unsigned bb = 0u; double ss[5] = {0, 0, 0, 0, 0};
     for (int w = 0; w < kTileThreads / 32; ++w) { mm = rmax(mm, wmax[w]); bb |= wbad[w]; for (int j = 0; j < 5; ++j) ss[j] += wsum[w][j]; }
@@ -229,26 +238,41 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArg
     if (bb) atomicOr(&D.ctl->bad, 1u);
     double* p = D.part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kPart;
     for (int j = 0; j < 5; ++j) p[j] = ss[j];
-    double yt = 0.0, yb = 0.0;
-    for (int c = 0; c < kTile; ++c) { yt += yedge[0][c]; yb += yedge[1][c]; }
     p[5] = yt; p[6] = yb;
   }
 }
 
-// Advance the integrator after a step (or plan the first step when `first`).
+// Threads per design of the step finalize (any multiple of 32 up to 1024 works).
+constexpr int kFinThreads = 256;
+
+// Advance the integrator after a step (or plan the first step when `first`). Launched with
+// a block of warps per design: all of them sum the tile partials (one warp alone waits on
+// hundreds of dependent rounds of loads for a large grid), warp 0 does the rest.
 __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
+  __shared__ double red[32][kPart];
   const PlainDesign D = plain_design(A, blockIdx.x, n_blocks);
   PlainCtl& c = *D.ctl;
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const RunParams& P = A.P;
   if (c.done) return;
+  double tot[kPart] = {0, 0, 0, 0, 0, 0, 0};
   if (!first) {
-    // sum block partials in block order
-    double tot[kPart] = {0, 0, 0, 0, 0, 0, 0};
-    for (int b = lane; b < n_blocks; b += 32)
+    for (int b = threadIdx.x; b < n_blocks; b += blockDim.x)
       for (int j = 0; j < kPart; ++j) tot[j] += D.part[(size_t)b * kPart + j];
     for (int j = 0; j < kPart; ++j)
       for (int o = 16; o > 0; o >>= 1) tot[j] += __shfl_xor_sync(0xffffffffu, tot[j], o);
+    if (nw > 1) {
+      if (lane == 0)
+        for (int j = 0; j < kPart; ++j) red[wid][j] = tot[j];
+      __syncthreads();
+      for (int j = 0; j < kPart; ++j) {
+        tot[j] = lane < nw ? red[lane][j] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) tot[j] += __shfl_xor_sync(0xffffffffu, tot[j], o);
+      }
+    }
+  }
+  if (wid != 0) return;
+  if (!first) {
     {   // y_boundary (kernel.rs:452-472): the top edge is inflow when its net flux is > 0,
         // the bottom edge outflow
       const double dt_dx = c.pl.dt * P.dx;
