@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define ITR_GPU_ABI_VERSION 2
+#define ITR_GPU_ABI_VERSION 3
 
 typedef struct itr_ctx itr_ctx;
 
@@ -51,8 +51,8 @@ enum itr_run_status {
   ITR_RUN_UNHEALTHY = 3        /* negative depth beyond h_dry or NaN (numerics.rs:163) */
 };
 
-/* SolverParams (crates/itr-hydro/src/solver.rs:27-49). locked_dt and cfl_hard have no
- * counterpart here (baseline-locked dt is not part of the batch path). inflow_scale
+/* SolverParams (crates/itr-hydro/src/solver.rs:27-49). locked_dt and cfl_hard are set on the
+ * context with itr_gpu_set_locked_dt (one schedule per grid, shared by the batch). inflow_scale
  * multiplies every inflow hydrograph as in fill_ghosts (boundary.rs:27); the reference GPU
  * backend rejected values other than 1 (backend.rs:53-55), this one takes any. */
 typedef struct itr_params {
@@ -160,6 +160,8 @@ typedef struct itr_result {
   double volume_m3;         /* stored volume at the end */
   double rel_residual;      /* |ledger residual| / gross input at the last sync */
   uint64_t warm_start_steps;/* steps taken over from the baseline record (RunSummary::warm_start_steps) */
+  double dt_fallback_t;     /* locked dt: time of the sync snapshot the run fell back to, -1 if it
+                               kept the schedule or ran adaptively (RunSummary::dt_fallback_t) */
 } itr_result;
 
 /* GpuSolver::new (lib.rs:85). device < 0 selects the current device. Returns NULL on
@@ -197,6 +199,21 @@ int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int3
  *                       ones (identical results; for checking, default 0)
  * Returns ITR_INVALID_ARG for an unknown key. */
 int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value);
+
+/* Baseline-locked dt (SolverParams::locked_dt and cfl_hard, solver.rs:42-46; the run loop at
+ * solver.rs:436-483; Problem::build sets it from the baseline's record, problem.rs:196-198).
+ * Later itr_gpu_run_batch / itr_gpu_run_primitives calls on this context step every design
+ * with dt[step] while dt[step] * smax of the design's current state <= cfl_hard (the baseline's
+ * own dts, e.g. from a run of the unedited terrain, keep a zero edit bit-identical to it). At
+ * the first step where that fails, or when the schedule has run out, the design goes back to
+ * its last sync snapshot (state, peaks, integrator, ledger) and continues with the adaptive dt;
+ * itr_result.dt_fallback_t gets the snapshot's time. The clip to the next sync instant still
+ * applies. The schedule is copied; n = 0 (or dt NULL) clears it. With a schedule set the
+ * designs start cold (no warm start), and the paths that have no locked dt return
+ * ITR_UNSUPPORTED: impl 1 and 2, grids that only fit the tiled path, the adjoint and the
+ * ladder. itr_gpu_record_baseline runs adaptively, like the reference's baseline. Device
+ * memory while a schedule is set: 28 B per cell per design for the snapshot. */
+int itr_gpu_set_locked_dt(itr_ctx* ctx, const double* dt, uint64_t n, double cfl_hard);
 
 /* Timing of the last run_batch on the device, CUDA events on the context stream:
  * kernel_ms = the forward kernel(s) alone, total_ms = copies + kernels. last_cell_updates

@@ -40,6 +40,17 @@ namespace itr {
 namespace cg = cooperative_groups;
 
 
+// Scalars of one CTA at a sync snapshot of a baseline-locked run (the Checkpoint of
+// solver.rs:78-92 that the fallback restores): the integrator, which is the same in every
+// CTA of a design, and this CTA's f64 ledger totals.
+struct LockedSnap {
+  double t, dt_cfl, s_cur, acc_rain, volume, rel_res;
+  double led[4];
+  unsigned long long step;
+  unsigned sync_index;
+  int n_rows;
+};
+
 struct BatchArgs {
   RunParams P;
   int nx, ny, mode;
@@ -68,6 +79,16 @@ struct BatchArgs {
   unsigned long long max_steps;
   unsigned exact;     // 1: every paired reciprocal through the IEEE routine (checking)
   const WarmStart* warm;   // optional, per design (state NULL: cold start)
+  // Baseline-locked dt (SolverParams::locked_dt / cfl_hard, solver.rs:42-46); read only by the
+  // LOCKED instantiation, which is launched when locked_dt is set.
+  const double* locked_dt;   // n_locked dts of the baseline, shared by every design
+  unsigned long long n_locked;
+  double cfl_hard;
+  float4* snap4;             // sync snapshot of the state, n_designs * nx*ny (h, qx, qy, u)
+  float2* snap2;             //                                              (v, c)
+  float* snapk;              //                              running peaks
+  LockedSnap* snap_s;        // n_designs * C records
+  double* fallback_t;        // n_designs: time the run fell back to adaptive dt, -1 for none
 };
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -341,7 +362,26 @@ ITR_DEV Face2 shfl_down_face2(const Face2& f) {
   return o;
 }
 
-template <bool CREST, bool CLUSTERED, int MAXT, bool BND>
+// Sync snapshot of one CTA of a baseline-locked run: its rows of the state and peaks (cells
+// [0, ncell) of shared memory, global offset base) and, by thread 0, the integrator scalars and
+// the CTA's ledger totals into record `rec`. Ends with a CTA barrier, so no thread writes the
+// state of the next step before all of it is saved.
+ITR_DEV void locked_save(const BatchArgs& A, const Smem& sm, size_t base, int ncell, size_t rec, double t, double dt_cfl,
+                         double s_cur, double acc_rain, double volume, double rel_res, unsigned long long step,
+                         unsigned sync_index, int n_rows) {
+  for (int idx = threadIdx.x; idx < ncell; idx += blockDim.x) {
+    A.snap4[base + idx] = sm.S4[idx]; A.snap2[base + idx] = sm.S2[idx]; A.snapk[base + idx] = sm.PK[idx];
+  }
+  if (threadIdx.x == 0) {
+    LockedSnap& o = A.snap_s[rec];
+    o.t = t; o.dt_cfl = dt_cfl; o.s_cur = s_cur; o.acc_rain = acc_rain; o.volume = volume; o.rel_res = rel_res;
+    for (int j = 0; j < 4; ++j) o.led[j] = sm.LED[j];
+    o.step = step; o.sync_index = sync_index; o.n_rows = n_rows;
+  }
+  __syncthreads();
+}
+
+template <bool CREST, bool CLUSTERED, int MAXT, bool BND, bool LOCKED = false>
 __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int C = A.C;
@@ -538,9 +578,49 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     return left;
   };
 
+  // ---- baseline-locked dt (solver.rs:436-483, 611-614) ----
+  // Each step takes the baseline's dt while dt * smax of the current state stays within
+  // cfl_hard. At the first step where it would not (or the schedule has run out), every CTA
+  // restores its rows and scalars from the last sync snapshot and the run continues with the
+  // adaptive dt. smax, the step and the schedule are the same in every thread of the cluster,
+  // so the decision is uniform.
+  bool locked_live = LOCKED;
+  double s_cur = s0;
+  if constexpr (LOCKED) {
+    if (q == 0 && tid == 0) A.fallback_t[d] = -1.0;
+    locked_save(A, sm, cell0_off + (size_t)ra * nx, nr * nx, (size_t)d * C + q, t, dt_cfl, s_cur, acc_rain, volume, rel_res,
+                step, sync_index, n_rows);
+  }
+
   while (t < P.duration && sync_index < P.n_sync) {
     if (step >= A.max_steps) { status = 4; break; }
-    const StepPlan pl = plan_step_c(P, t, sync_index, dt_cfl, rcur);
+    double dt_pick = 0.0;
+    if constexpr (LOCKED) {
+      dt_pick = dmin_num(dt_cfl, P.dt_max);
+      if (locked_live) {
+        if (step < A.n_locked && A.locked_dt[step] * s_cur <= A.cfl_hard) {
+          dt_pick = A.locked_dt[step];
+        } else {
+          gs.full();   // every CTA has finished reading this CTA's shared memory
+          for (int idx = tid; idx < nr * nx; idx += blockDim.x) {
+            const size_t g = cell0_off + (size_t)ra * nx + idx;
+            sm.S4[idx] = A.snap4[g]; sm.S2[idx] = A.snap2[g]; sm.PK[idx] = A.snapk[g];
+          }
+          const LockedSnap& o = A.snap_s[(size_t)d * C + q];
+          t = o.t; dt_cfl = o.dt_cfl; s_cur = o.s_cur; acc_rain = o.acc_rain; volume = o.volume; rel_res = o.rel_res;
+          step = o.step; sync_index = o.sync_index; n_rows = o.n_rows;
+          if (tid < 4) { sm.LED[tid] = o.led[tid]; sm.slot[tid] = 0u; }
+          rcur.seg = 0; rcur.brk = 0;
+          if (BND && wid == nwarps - 1 && lane < P.inflow.n)
+            sm.INF[(int)(step & 1ull) * kMaxInflow + lane] = inflow_values(P.inflow, lane, t, P.g);
+          if (q == 0 && tid == 0) A.fallback_t[d] = t;
+          locked_live = false;
+          gs.full();   // the restored state of every CTA visible before the next step
+          continue;
+        }
+      }
+    }
+    const StepPlan pl = LOCKED ? plan_step_dt_c(P, t, sync_index, dt_pick, rcur) : plan_step_c(P, t, sync_index, dt_cfl, rcur);
     StepK k = step_consts(P, pl.dt, pl.rain);
     k.exact = A.exact;
     const int sp = (int)(step & 1ull);
@@ -778,6 +858,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     acc_rain += pl.rain * P.area * P.wet_count;
     if (badv) { status = 3; break; }
     dt_cfl = smax > 0.0 ? P.cfl / smax : P.dt_max;
+    if constexpr (LOCKED) s_cur = smax;
     if (pl.hits) {
       // ---- sync point: volume, ledger row, guard and incumbent tests ----
       sync_index += 1;
@@ -865,6 +946,11 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       }
       gs.full();
       if (decision != 0) { status = decision; break; }
+      if constexpr (LOCKED) {
+        if (locked_live)
+          locked_save(A, sm, cell0_off + (size_t)ra * nx, nr * nx, (size_t)d * C + q, t, dt_cfl, s_cur, acc_rain, volume,
+                      rel_res, step, sync_index, n_rows);
+      }
     }
   }
   if (gs.timed_out) status = 5;

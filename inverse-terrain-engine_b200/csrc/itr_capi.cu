@@ -122,6 +122,13 @@ struct itr_ctx {
   int autotune = 1, autotune_top = 6, probe_steps = 200;
   int exact_special = 0;
   float tune_ms = 0.0f;
+  // baseline-locked dt (itr_gpu_set_locked_dt): the schedule, its limit, the snapshot buffers
+  // and, per design of the last batch, the fallback time (-1: none)
+  std::vector<double> locked_dt;
+  double cfl_hard = 0.5;
+  bool locked_run = false;
+  DevBuf lDt, lS4, lS2, lSk, lSs, lFb;
+  std::vector<double> fallback;
   // device buffers (batched path)
   DevBuf wet, gn2, bc, dzx, dzy, dzx2, dzy2, h0, cut, fill, mon, obj_i, obj_d, peak, depth, ledger, out, mmax;
   // plain path scratch
@@ -190,18 +197,22 @@ static int fail(itr_ctx* c, int code, const char* fmt, ...) {
 // ------------------------------------------------------------------ kernels table ----
 typedef void (*BatchedFn)(const BatchArgs);
 
-static BatchedFn batched_fn(bool crest, bool clustered, int maxt, bool bnd) {
-#define PICK(CR, CL, BD)                                              \
-  if (maxt <= 256) return k_batched<CR, CL, 256, BD>;                 \
-  if (maxt <= 512) return k_batched<CR, CL, 512, BD>;                 \
-  if (maxt <= 768) return k_batched<CR, CL, 768, BD>;                 \
-  return k_batched<CR, CL, 1024, BD>;
-  if (bnd) {
-    if (crest) { if (clustered) { PICK(true, true, true) } else { PICK(true, false, true) } }
-    else { if (clustered) { PICK(false, true, true) } else { PICK(false, false, true) } }
-  }
-  if (crest) { if (clustered) { PICK(true, true, false) } else { PICK(true, false, false) } }
-  else { if (clustered) { PICK(false, true, false) } else { PICK(false, false, false) } }
+static BatchedFn batched_fn(bool crest, bool clustered, int maxt, bool bnd, bool locked = false) {
+#define PICK(CR, CL, BD, LK)                                          \
+  if (maxt <= 256) return k_batched<CR, CL, 256, BD, LK>;             \
+  if (maxt <= 512) return k_batched<CR, CL, 512, BD, LK>;             \
+  if (maxt <= 768) return k_batched<CR, CL, 768, BD, LK>;             \
+  return k_batched<CR, CL, 1024, BD, LK>;
+#define PICK4(LK)                                                                                  \
+  if (bnd) {                                                                                       \
+    if (crest) { if (clustered) { PICK(true, true, true, LK) } else { PICK(true, false, true, LK) } } \
+    else { if (clustered) { PICK(false, true, true, LK) } else { PICK(false, false, true, LK) } }    \
+  }                                                                                                \
+  if (crest) { if (clustered) { PICK(true, true, false, LK) } else { PICK(true, false, false, LK) } } \
+  else { if (clustered) { PICK(false, true, false, LK) } else { PICK(false, false, false, LK) } }
+  if (locked) { PICK4(true) }
+  PICK4(false)
+#undef PICK4
 #undef PICK
 }
 
@@ -229,7 +240,7 @@ static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_targe
 
 static int launch_batched(itr_ctx* ctx, const BatchArgs& A, const LaunchCfg& cfg, int n_designs, bool set_attr = true) {
   const bool crest = A.mode == 1, clustered = cfg.C > 1;
-  BatchedFn fn = batched_fn(crest, clustered, maxt_bucket(cfg.T), cfg.bnd);
+  BatchedFn fn = batched_fn(crest, clustered, maxt_bucket(cfg.T), cfg.bnd, A.locked_dt != nullptr);
   if (set_attr) CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   cudaLaunchConfig_t lc;
   memset(&lc, 0, sizeof(lc));
@@ -519,7 +530,8 @@ void itr_gpu_destroy(itr_ctx* ctx) {
                     &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
                     &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aTape2, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy, &ctx->aGx2, &ctx->aGy2,
                     &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon,
-                    &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut, &ctx->wsb, &ctx->rIn, &ctx->rOut})
+                    &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut, &ctx->wsb, &ctx->rIn, &ctx->rOut,
+                    &ctx->lDt, &ctx->lS4, &ctx->lS2, &ctx->lSk, &ctx->lSs, &ctx->lFb})
     b->release();
   for (DevBuf& b : ctx->aCkpt) b.release();
   for (itr_ctx* c : ctx->children) itr_gpu_destroy(c);
@@ -569,6 +581,17 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   else if (k == "probe_steps") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "probe_steps must be >= 1"); ctx->probe_steps = (int)value; }
   else return fail(ctx, ITR_INVALID_ARG, "unknown option '%s'", key);
   if (k == "threads" || k == "cluster") ctx->tuned.clear();
+  return ITR_OK;
+}
+
+int itr_gpu_set_locked_dt(itr_ctx* ctx, const double* dt, uint64_t n, double cfl_hard) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (n > 0 && !dt) return fail(ctx, ITR_INVALID_ARG, "locked dt schedule is NULL");
+  if (n > 0 && !(cfl_hard > 0.0)) return fail(ctx, ITR_INVALID_ARG, "cfl_hard must be positive");
+  for (uint64_t i = 0; i < n; ++i)
+    if (!(dt[i] > 0.0) || !std::isfinite(dt[i])) return fail(ctx, ITR_INVALID_ARG, "locked dt %llu is not a positive number", (unsigned long long)i);
+  ctx->locked_dt.assign(dt ? dt : nullptr, dt ? dt + n : nullptr);
+  ctx->cfl_hard = cfl_hard;
   return ITR_OK;
 }
 
@@ -913,6 +936,8 @@ static int collect_results(itr_ctx* ctx, const Collect& c) {
     CU(cudaMemcpyAsync(hmm, ctx->mmax.p, (size_t)tot * 4, cudaMemcpyDeviceToHost, ctx->stream));
   }
   if (max_rows > 0) CU(cudaMemcpyAsync(hled, ctx->ledger.p, (size_t)n * max_rows * 64, cudaMemcpyDeviceToHost, ctx->stream));
+  ctx->fallback.assign((size_t)n, -1.0);
+  if (ctx->locked_run) CU(cudaMemcpyAsync(ctx->fallback.data(), ctx->lFb.p, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
   for (int d = 0; d < n; ++d) {
     if (res[d].peak) CU(cudaMemcpyAsync(res[d].peak, ctx->peak.as<float>() + d * N, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
     if (res[d].depth) CU(cudaMemcpyAsync(res[d].depth, ctx->depth.as<float>() + d * N, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -949,6 +974,7 @@ static int collect_results(itr_ctx* ctx, const Collect& c) {
     r.volume_m3 = o.volume;
     r.rel_residual = o.rel_residual;
     r.warm_start_steps = (size_t)d < ctx->warm_steps.size() ? ctx->warm_steps[d] : 0;
+    r.dt_fallback_t = ctx->fallback[(size_t)d];
     if (r.monitor_max) for (int k = 0; k < n_mon; ++k) r.monitor_max[k] = (double)hmm[(size_t)d * n_mon + k];
     if (r.ledger && r.max_rows > 0) memcpy(r.ledger, hled + (size_t)d * max_rows * 8, (size_t)r.n_rows * 64);
     r.j = 0.0; r.feasible = 1; r.violation = 0.0;
@@ -1181,10 +1207,16 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     CU(cudaStreamSynchronize(ctx->stream));
     for (int d = 0; d < n; ++d) { M->ds[d].cut_m3 = hv[d]; M->ds[d].fill_m3 = hv[n + d]; }
   }
-  // ---- warm starts from the baseline record ----
+  // ---- baseline-locked dt: the batched cluster kernel only; the baseline record runs adaptively ----
+  const bool locked = !ctx->locked_dt.empty() && !ctx->recording;
+  ctx->locked_run = false;
+  if (locked && (ctx->impl != 0 || ctx->vjp || ctx->defer))
+    return fail(ctx, ITR_UNSUPPORTED, "a baseline-locked dt schedule runs on the batched cluster kernel only (impl 0, "
+                                      "no adjoint, no ladder)");
+  // ---- warm starts from the baseline record (a locked run starts cold: its snapshot is the start) ----
   ctx->warm_steps.assign((size_t)n, 0);
   const WarmStart* warm_dev = nullptr;
-  if (ctx->warm_start && ctx->rec && !ctx->vjp && !ctx->recording && !(ob && ob->has_incumbent) &&
+  if (ctx->warm_start && ctx->rec && !ctx->vjp && !ctx->recording && !locked && !(ob && ob->has_incumbent) &&
       record_matches(*ctx->rec, P, g, st + o_bc)) {
     const Record& R = *ctx->rec;
     std::vector<WarmStart> ws((size_t)n);
@@ -1286,7 +1318,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     if (ctx->cluster > 0 || ctx->threads > 0) {
       cfg = make_cfg(ctx, nx, ny, ctx->cluster > 0 ? ctx->cluster : 1, ctx->threads > 0 ? ctx->threads : 512, crest, bnd);
       if (!cfg.ok) return fail(ctx, ITR_UNSUPPORTED, "cluster=%d threads=%d does not fit a %dx%d grid in shared memory", ctx->cluster, ctx->threads, nx, ny);
-    } else if (ctx->tuned.count(key)) {
+    } else if (ctx->tuned.count(key) && !(locked && ctx->tuned[key].tiled)) {
       cfg = ctx->tuned[key];
       tiled = cfg.tiled;
     } else {
@@ -1301,7 +1333,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
           rc = autotune(ctx, A, cands, n, &cfg);
           if (rc != ITR_OK) return rc;
         }
-        if (ctx->autotune) {
+        if (ctx->autotune && !locked) {
           // the tiled HBM path as one more candidate, timed over the same probe steps
           PlainArgs T;
           CU(tiled_args(T));
@@ -1322,12 +1354,29 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
           CU(cudaEventElapsedTime(&t_ms, ctx->ev[1], ctx->ev[2]));
           if (t_ms < ctx->tune_ms) { cfg.tiled = true; ctx->tune_ms = t_ms; }
         }
-        ctx->tuned[key] = cfg;
+        if (!(locked && ctx->tuned.count(key))) ctx->tuned[key] = cfg;   // a locked run keeps a cached tiled choice
         tiled = cfg.tiled;
       }
     }
     if (!tiled) {
       A.C = cfg.C; A.W = cfg.W; A.S = cfg.S;
+      if (locked) {
+        const size_t nl = ctx->locked_dt.size();
+        CU(ctx->lDt.ensure(nl * 8));
+        CU(ctx->lS4.ensure((size_t)n * N * 16));
+        CU(ctx->lS2.ensure((size_t)n * N * 8));
+        CU(ctx->lSk.ensure((size_t)n * N * 4));
+        CU(ctx->lSs.ensure((size_t)n * cfg.C * sizeof(LockedSnap)));
+        CU(ctx->lFb.ensure((size_t)n * 8));
+        CU(cudaMemcpyAsync(ctx->lDt.p, ctx->locked_dt.data(), nl * 8, cudaMemcpyHostToDevice, ctx->stream));
+        A.locked_dt = ctx->lDt.as<double>();
+        A.n_locked = (unsigned long long)nl;
+        A.cfl_hard = ctx->cfl_hard;
+        A.snap4 = ctx->lS4.as<float4>(); A.snap2 = ctx->lS2.as<float2>(); A.snapk = ctx->lSk.as<float>();
+        A.snap_s = ctx->lSs.as<LockedSnap>();
+        A.fallback_t = ctx->lFb.as<double>();
+        ctx->locked_run = true;
+      }
       if (ctx->defer) {   // ladder group: the launch goes into the ladder's graph
         BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T), cfg.bnd);
         CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
@@ -1351,6 +1400,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
       ctx->last_was_tiled = false;
     }
   }
+  if (tiled && locked) return fail(ctx, ITR_UNSUPPORTED, "a %dx%d grid takes the tiled path, which has no baseline-locked dt", nx, ny);
   if (tiled) {
     const int nb = n_tiles;
     PlainArgs A;
@@ -1446,6 +1496,8 @@ extern "C" int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_g
                                   itr_result* results) {
   if (!ctx) return ITR_INVALID_ARG;
   if (n_groups < 1 || !groups || !results || !p) return fail(ctx, ITR_INVALID_ARG, "ladder: groups, params and results are required");
+  if (!ctx->locked_dt.empty())   // a schedule belongs to one grid (Problem::build records one per level, problem.rs:196-198)
+    return fail(ctx, ITR_UNSUPPORTED, "ladder: a baseline-locked dt schedule belongs to one grid; run each level with itr_gpu_run_batch");
   CU(cudaSetDevice(ctx->device));
   while ((int)ctx->children.size() < n_groups) {
     char err[256] = {0};

@@ -279,6 +279,7 @@ extern "C" int itr_gpu_run_plain_static(int device, const itr_params* p, const i
   res->volume_m3 = hc.volume;
   res->rel_residual = hc.rel_res;
   res->warm_start_steps = 0;
+  res->dt_fallback_t = -1.0;
   return ITR_OK;
 }
 

@@ -70,6 +70,7 @@ class Result(C.Structure):
         ("breach_sync", C.c_uint32), ("violation", C.c_double), ("lower_bound", C.c_double),
         ("j", C.c_double), ("feasible", C.c_int32), ("n_rows", C.c_int32),
         ("volume_m3", C.c_double), ("rel_residual", C.c_double), ("warm_start_steps", C.c_uint64),
+        ("dt_fallback_t", C.c_double),
     ]
 
 
@@ -103,6 +104,7 @@ SIGNATURES = {
     "itr_gpu_run_batch": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.c_int32, C.POINTER(Design),
                                     _u32p, C.c_int32, C.POINTER(Objective), C.POINTER(Result)]),
     "itr_gpu_set_option": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int64]),
+    "itr_gpu_set_locked_dt": (C.c_int, [C.c_void_p, _dp, C.c_uint64, C.c_double]),
     "itr_gpu_last_timing": (C.c_int, [C.c_void_p, _dp, _dp, C.POINTER(C.c_uint64), _i32p]),
     "itr_gpu_rerun_resident": (C.c_int, [C.c_void_p]),
     "itr_gpu_run_ladder": (C.c_int, [C.c_void_p, C.POINTER(Params), C.c_int32, C.POINTER(Group), C.POINTER(Result)]),

@@ -77,6 +77,10 @@ class SolverParams:
     initial_stage: float | None = None
     skip_dry: bool = True
     inflow_scale: float = 1.0
+    # Baseline-locked dt (solver.rs:42-46): the baseline's dt per step, each verified against
+    # cfl_hard; on a violation the run restarts adaptively from the last sync snapshot.
+    locked_dt: np.ndarray | None = None
+    cfl_hard: float = 0.5
 
     def vector(self) -> np.ndarray:
         """The 12-number parameter vector the CPU oracle takes."""
@@ -190,6 +194,7 @@ class GpuRun:
     warm_start_steps: int = 0           # steps taken over from the baseline record
     dj_ddzx2: np.ndarray | None = None  # itr_gpu_vjp_crest: dJ/d(second x-face jump)
     dj_ddzy2: np.ndarray | None = None
+    dt_fallback_t: float = -1.0         # locked dt: time of the snapshot the run fell back to (-1: none)
 
 
 @dataclass
@@ -286,6 +291,12 @@ class GpuSolver:
         return {"forward_ms": f.value, "backward_ms": b.value}
 
     def _params(self, p: SolverParams, keep: list):
+        # the locked dt schedule lives on the context: set (or clear) it for this call
+        sched = None if p.locked_dt is None else np.ascontiguousarray(p.locked_dt, dtype=np.float64)
+        keep.append(sched)
+        rc = self.lib.itr_gpu_set_locked_dt(self.ctx, _ptr(sched, C.c_double) if sched is not None and len(sched) else None,
+                                            0 if sched is None else len(sched), float(p.cfl_hard))
+        self._check(rc, "itr_gpu_set_locked_dt")
         rain_t = np.ascontiguousarray([q[0] for q in p.rain.pts] or [0.0], dtype=np.float64)
         rain_r = np.ascontiguousarray([q[1] for q in p.rain.pts] or [0.0], dtype=np.float64)
         keep += [rain_t, rain_r]
@@ -390,7 +401,7 @@ class GpuSolver:
                                breach_sync=int(r.breach_sync), violation=float(r.violation), lower_bound=float(r.lower_bound),
                                j=float(r.j), feasible=bool(r.feasible), sync_count=int(r.sync_count),
                                rel_residual=float(r.rel_residual), cell_updates=int(r.cell_updates),
-                               warm_start_steps=int(r.warm_start_steps),
+                               warm_start_steps=int(r.warm_start_steps), dt_fallback_t=float(r.dt_fallback_t),
                                dj_ddzx=gx[i] if gx is not None else None, dj_ddzy=gy[i] if gy is not None else None))
         return runs
 

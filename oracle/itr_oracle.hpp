@@ -622,6 +622,12 @@ struct Params {
   bool has_stage = false; double initial_stage = 0;
   bool skip_dry = true;
   double inflow_scale = 1.0;
+  // Baseline-locked dt (SolverParams::locked_dt / cfl_hard, solver.rs:42-46): the baseline's
+  // dt per step, each verified against cfl_hard; n_locked == 0 means adaptive dt.
+  const double* locked_dt = nullptr;
+  size_t n_locked = 0;
+  double cfl_hard = 0.5;
+  bool record_dts = false;   // keep the dt of every step (BaselineRecord::dts, solver.rs:508)
 };
 
 enum Kernel { K_ORACLE = 0, K_FUSED = 1 };
@@ -639,6 +645,8 @@ struct RunResult {
   uint64_t cell_updates = 0, rows_skipped = 0;
   std::vector<double> peak;      // per-cell running max of h (f64 compare), all cells
   std::vector<uint64_t> peak_step;
+  double dt_fallback_t = -1.0;   // locked dt: time at which the run fell back to adaptive dt
+  std::vector<double> dts;       // with Params::record_dts: the dt of every step, in order
 };
 
 // Optional observer config (GuardObserver, evaluator.rs:88-108).
@@ -1010,7 +1018,18 @@ template <class T> struct Solver {
     }
   }
 
-  // run_impl (solver.rs:346-660) without warm start, replay or locked dt.
+  // Sync snapshot of everything the run loop carries, for the locked-dt fallback
+  // (Checkpoint, solver.rs:78-92; taken at the start and at every sync, solver.rs:444-447,611-614).
+  struct Snap {
+    std::vector<T> h, qx, qy; std::vector<uint8_t> row_dry;
+    std::vector<double> mmax, mtmax, peak; std::vector<uint64_t> peak_step;
+    double t = 0, dt_cfl = 0, s_cur = 0; uint64_t step = 0; uint32_t sync_index = 0;
+    double acc[5] = {0, 0, 0, 0, 0}; double dmin = 0, dmax = 0, dsum = 0;
+    uint64_t cell_updates = 0, rows_skipped = 0; size_t n_rows = 0;
+  };
+
+  // run_impl (solver.rs:346-660) without warm start or replay; with locked dt when
+  // p.n_locked > 0 (solver.rs:436-483).
   // Optional custom start (the Ritter validation case builds a checkpoint by hand,
   // validation.rs:125-151): padded depth, all rows wet, given dt_next and v0.
   struct Start { std::vector<T> h; double dt_next = 0; double v0 = 0; };
@@ -1030,16 +1049,18 @@ template <class T> struct Solver {
     if (want_peak) { peak.assign(nx * ny, 0.0); peak_step.assign(nx * ny, 0); }
     double area = tb->dx * tb->dy;
     RunResult R;
-    double dt_cfl;
+    double dt_cfl, s_cur;
     if (start) {
       h = start->h;
       std::fill(row_dry.begin(), row_dry.end(), 0);
       R.v0 = start->v0;
       dt_cfl = start->dt_next;
+      s_cur = initial_smax();
     } else {
       init_state(h0);
       R.v0 = volume(area);
       double s0 = initial_smax();
+      s_cur = s0;
       dt_cfl = s0 > 0.0 ? fmin_num(p.cfl / s0, p.dt_max) : p.dt_max;
     }
     double t = 0.0; uint64_t step = 0; uint32_t sync_index = 0;
@@ -1047,14 +1068,43 @@ template <class T> struct Solver {
     double dmin = std::numeric_limits<double>::max(), dmax = 0, dsum = 0;
     uint64_t cells = (uint64_t)nx * ny;
     uint32_t n_sync = (uint32_t)std::ceil(p.duration / p.sync);
+    bool locked = p.n_locked > 0;
+    Snap snap;
+    auto save = [&]() {
+      snap.h = h; snap.qx = qx; snap.qy = qy; snap.row_dry = row_dry;
+      snap.mmax = mon.max; snap.mtmax = mon.tmax; snap.peak = peak; snap.peak_step = peak_step;
+      snap.t = t; snap.dt_cfl = dt_cfl; snap.s_cur = s_cur; snap.step = step; snap.sync_index = sync_index;
+      snap.acc[0] = acc_rain; snap.acc[1] = acc_in; snap.acc[2] = acc_out; snap.acc[3] = acc_infil; snap.acc[4] = acc_fix;
+      snap.dmin = dmin; snap.dmax = dmax; snap.dsum = dsum;
+      snap.cell_updates = R.cell_updates; snap.rows_skipped = R.rows_skipped; snap.n_rows = R.rows.size();
+    };
+    if (locked) save();
     while (t < p.duration && sync_index < n_sync) {
       double t_sync = fmin_num((double)(sync_index + 1) * p.sync, p.duration);
       double dt = fmin_num(dt_cfl, p.dt_max);
+      if (locked) {
+        // the recorded dt, verified against the hard CFL limit; otherwise restart adaptively
+        // from the last sync snapshot (solver.rs:452-482)
+        if (step < p.n_locked && p.locked_dt[step] * s_cur <= p.cfl_hard) {
+          dt = p.locked_dt[step];
+        } else {
+          h = snap.h; qx = snap.qx; qy = snap.qy; row_dry = snap.row_dry;
+          mon.max = snap.mmax; mon.tmax = snap.mtmax; peak = snap.peak; peak_step = snap.peak_step;
+          acc_rain = snap.acc[0]; acc_in = snap.acc[1]; acc_out = snap.acc[2]; acc_infil = snap.acc[3]; acc_fix = snap.acc[4];
+          dmin = snap.dmin; dmax = snap.dmax; dsum = snap.dsum;
+          R.cell_updates = snap.cell_updates; R.rows_skipped = snap.rows_skipped; R.rows.resize(snap.n_rows);
+          t = snap.t; step = snap.step; sync_index = snap.sync_index; dt_cfl = snap.dt_cfl; s_cur = snap.s_cur;
+          R.dt_fallback_t = t;
+          locked = false;
+          continue;
+        }
+      }
       bool hits = t + dt >= t_sync - 1e-9 * p.sync;
       if (hits) dt = t_sync - t;
       double rain = p.rain.integral(t, t + dt);
       double t_new = hits ? t_sync : t + dt;
       fill_ghosts(t);
+      if (p.record_dts) R.dts.push_back(dt);
       StepConsts<T> k = consts(dt, rain);
       step_no = step;
       StepStats<T> st = kern == K_ORACLE ? step_oracle(k, dt, t_new, hits) : step_fused(k, dt, t_new, hits);
@@ -1067,6 +1117,7 @@ template <class T> struct Solver {
       R.rows_skipped += st.rows_skipped;
       if (st.bad) { R.abort = AB_UNHEALTHY; break; }
       dt_cfl = st.smax > 0.0 ? p.cfl / st.smax : p.dt_max;
+      s_cur = st.smax;
       if (hits) {
         sync_index += 1;
         double v = volume(area);
@@ -1088,6 +1139,7 @@ template <class T> struct Solver {
             if (lb >= obs->incumbent) { R.abort = AB_INCUMBENT; R.abort_lb = lb; break; }
           }
         }
+        if (locked) save();
       }
     }
     R.t_end = t; R.steps = step; R.sync_count = sync_index;

@@ -152,8 +152,34 @@ struct ParamsIn {  // mirrors the 16-double params vector built by the Python si
   double duration, sync, cfl, dt_max, h_dry, h_eps, infil, initial_depth, has_stage, stage, skip_dry, inflow_scale;
 };
 
+// Baseline-locked dt of the next runs on the calling thread (SolverParams::locked_dt and
+// cfl_hard, solver.rs:42-46), and what the last run on that thread reported
+// (RunSummary::dt_fallback_t and, with record_dts, BaselineRecord::dts).
+static thread_local std::vector<double> g_locked;
+static thread_local double g_cfl_hard = 0.5;
+static thread_local bool g_record_dts = false;
+static thread_local double g_last_fallback = -1.0;
+static thread_local std::vector<double> g_last_dts;
+
+extern "C" void orc_set_locked_dt(const double* dts, int64_t n, double cfl_hard, int record_dts) {
+  g_locked.assign(dts ? dts : nullptr, dts ? dts + (n > 0 ? n : 0) : nullptr);
+  g_cfl_hard = cfl_hard;
+  g_record_dts = record_dts != 0;
+}
+
+// Returns the number of steps whose dt the last run recorded (copies up to cap of them).
+extern "C" int64_t orc_last_locked(double* fallback_t, double* dts, int64_t cap) {
+  if (fallback_t) *fallback_t = g_last_fallback;
+  for (int64_t i = 0; dts && i < cap && i < (int64_t)g_last_dts.size(); ++i) dts[i] = g_last_dts[(size_t)i];
+  return (int64_t)g_last_dts.size();
+}
+
 static Params make_params(const double* pv, const double* rain_t, const double* rain_r, int n_rain) {
   Params p;
+  p.locked_dt = g_locked.empty() ? nullptr : g_locked.data();
+  p.n_locked = g_locked.size();
+  p.cfl_hard = g_cfl_hard;
+  p.record_dts = g_record_dts;
   p.duration = pv[0]; p.sync = pv[1]; p.cfl = pv[2]; p.dt_max = pv[3]; p.h_dry = pv[4]; p.h_eps = pv[5];
   p.infil_capacity = pv[6]; p.initial_depth = pv[7]; p.has_stage = pv[8] != 0.0; p.initial_stage = pv[9];
   p.skip_dry = pv[10] != 0.0; p.inflow_scale = pv[11];
@@ -190,6 +216,8 @@ template <class T>
 static void write_result(const RunResult& R, const Solver<T>& S, double* out_s, double* mon_max, double* mon_tmax,
                          double* ledger, int max_rows, double* h_out, double* qx_out, double* qy_out,
                          double* peak, double* peak_step) {
+  g_last_fallback = R.dt_fallback_t;
+  g_last_dts = R.dts;
   out_s[0] = R.t_end; out_s[1] = (double)R.steps; out_s[2] = R.sync_count; out_s[3] = R.abort;
   out_s[4] = R.abort_cell; out_s[5] = R.abort_exceed; out_s[6] = R.abort_sync; out_s[7] = R.abort_lb;
   out_s[8] = R.v0; out_s[9] = R.rel_residual; out_s[10] = R.dt_min; out_s[11] = R.dt_max; out_s[12] = R.dt_mean;

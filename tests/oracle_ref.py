@@ -72,6 +72,9 @@ def lib():
                                  _d, C.c_int, C.c_int, _u32, _d, _d]
     L.orc_validation.argtypes = [C.c_int, C.c_int, _d]
     L.orc_render_map.argtypes = [C.c_int, C.c_int, C.c_double, _f, _f, _f, C.c_int, C.c_float, C.c_int, _u8]
+    L.orc_set_locked_dt.argtypes = [_d, C.c_int64, C.c_double, C.c_int]
+    L.orc_last_locked.restype = C.c_int64
+    L.orc_last_locked.argtypes = [_d, _d, C.c_int64]
     _lib = L
     return L
 
@@ -199,6 +202,27 @@ def _run(call, nx, ny, params, monitors, objective, baseline, incumbent, cut, fi
                 dt_min=out_s[10], dt_max=out_s[11], dt_mean=out_s[12], cell_updates=int(out_s[13]),
                 rows_skipped=int(out_s[14]), monitor_max=mm[:nm].copy(), monitor_tmax=mt[:nm].copy(),
                 ledger=led[:min(n_rows, max_rows)].copy(), h=h, qx=qx, qy=qy, peak=pk, peak_step=ps)
+
+
+def locked(run, locked_dt=None, cfl_hard=0.5, record_dts=False):
+    """Calls run() (one oracle run) with SolverParams::locked_dt / cfl_hard set (solver.rs:42-46), and
+    adds to its result dict dt_fallback_t (RunSummary::dt_fallback_t, -1 for none) and, with record_dts,
+    dts: the dt of every step (BaselineRecord::dts)."""
+    L = lib()
+    sched = None if locked_dt is None else np.ascontiguousarray(locked_dt, dtype=np.float64)
+    L.orc_set_locked_dt(P(sched, C.c_double), 0 if sched is None else len(sched), cfl_hard, 1 if record_dts else 0)
+    try:
+        r = run()
+    finally:
+        L.orc_set_locked_dt(None, 0, 0.5, 0)
+    fb = C.c_double(-1.0)
+    n = L.orc_last_locked(C.byref(fb), None, 0)
+    dts = np.zeros(n)
+    L.orc_last_locked(C.byref(fb), P(dts, C.c_double), n)
+    r["dt_fallback_t"] = fb.value
+    if record_dts:
+        r["dts"] = dts
+    return r
 
 
 def render_map(z, value, cell_size, mode=0, vex=1.0, scale=1, worse_dz=None):
