@@ -346,6 +346,38 @@ int itr_gpu_vjp_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g,
 int itr_gpu_render_map(itr_ctx* ctx, int32_t nx, int32_t ny, double cell_size, const float* z, const float* value,
                        const float* worse_dz, int32_t mode, float vex, int32_t scale, uint8_t* rgba);
 
+/* ---- Headless flood-scene render (presentation, not on the hot path). ----
+ * The reference's video renders each recorded frame with an SkSL ray marcher through Skia on
+ * Metal (video/src/shaders/terrain.sksl; uniforms from video/src/lib.rs:52-77; textures packed
+ * by video/src/data.rs:89-96). itr_gpu_render_scene runs the same shader on the device without
+ * a graphics stack: rgba receives width x height pixels, 4 bytes each, row 0 the top.
+ * Textures, 4 bytes per texel, row 0 the northern edge:
+ *   terrain  tw x th (the simulation grid refined by `up`): R, G = elevation code (16 bit,
+ *            R high) over z_span, B = material code (0 ground, 1-120 fill, 121-200 cut,
+ *            >= 250 building)
+ *   depth    nx x ny: R, G = depth code (16 bit) over depth_span, B = 255 where wet
+ *   vel      nx x ny: R, G = velocity u, v as 128 + 127 v / vel_max
+ * A texture read takes the texel under the coordinate, clamped to the image. */
+typedef struct itr_scene_view {   /* the shader's uniforms */
+  float cam_pos[3], cam_fwd[3], cam_right[3], cam_up[3];   /* camera frame (m; unit vectors) */
+  float focal;                /* focal length in image-height units */
+  float domain[3];            /* width, height, cell size (m) */
+  float z_lo, z_span;         /* elevation of code 0 (m, not used by the shader) and of the code span */
+  float up;                   /* terrain texels per simulation cell */
+  float depth_span;           /* depth of code 65535 (m) */
+  float ve;                   /* vertical exaggeration */
+  float time;                 /* simulated time (s) */
+  float rain, wet, overcast;  /* rain rate / peak rate, surface wetness, cloud cover, 0..1 */
+  float vel_max;              /* velocity of code 255 (m/s) */
+  float base;                 /* depth of the cut-away block below the lowest ground (m) */
+  int32_t ortho;              /* 1: top-down map over the whole domain */
+  int32_t debug;              /* 0 normal, 1 pixel coordinates, 2 elevation texture, 3 water texture */
+} itr_scene_view;
+
+int itr_gpu_render_scene(itr_ctx* ctx, const uint8_t* terrain, int32_t tw, int32_t th, const uint8_t* depth,
+                         const uint8_t* vel, int32_t nx, int32_t ny, const itr_scene_view* view, int32_t width,
+                         int32_t height, uint8_t* rgba);
+
 /* ---- Allocation-free plain forward. No reference counterpart. ----
  * For callers that cannot allocate device memory when they run a design: a process that
  * has committed the whole device to its own pool, a caller whose other streams must not be

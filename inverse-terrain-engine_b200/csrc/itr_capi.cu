@@ -25,6 +25,7 @@
 #include "itr_adjoint.cuh"
 #include "itr_design.cuh"
 #include "itr_render.cuh"
+#include "itr_raymarch.cuh"
 
 using namespace itr;
 
@@ -149,7 +150,7 @@ struct itr_ctx {
   std::vector<uint64_t> warm_steps;   // per design of the last batch
   DevBuf wsb;
   DevBuf mDz, mZe, mAux, mJp, mJob, mOut;
-  DevBuf rIn, rOut;   // map rendering
+  DevBuf rIn, rOut;   // map and scene rendering
   HostBuf mVol;
   // ladder: one child context per grid group; a deferred run stops before its launch
   std::vector<itr_ctx*> children;
@@ -1598,6 +1599,50 @@ extern "C" int itr_gpu_render_map(itr_ctx* ctx, int32_t nx, int32_t ny, double c
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(rgba, ctx->rOut.p, P * 4, cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
+  return ITR_OK;
+}
+
+extern "C" int itr_gpu_render_scene(itr_ctx* ctx, const uint8_t* terrain, int32_t tw, int32_t th, const uint8_t* depth,
+                                    const uint8_t* vel, int32_t nx, int32_t ny, const itr_scene_view* v, int32_t width,
+                                    int32_t height, uint8_t* rgba) {
+  if (!ctx) return ITR_INVALID_ARG;
+  if (!terrain || !depth || !vel || !v || !rgba) return fail(ctx, ITR_INVALID_ARG, "terrain, depth, vel, view and rgba are required");
+  if (tw < 1 || th < 1 || (int64_t)tw * th > (1ll << 28)) return fail(ctx, ITR_INVALID_ARG, "bad terrain texture size");
+  if (nx < 1 || ny < 1 || (int64_t)nx * ny > (1ll << 28)) return fail(ctx, ITR_INVALID_ARG, "bad grid size");
+  if (width < 1 || height < 1 || (int64_t)width * height > (1ll << 28)) return fail(ctx, ITR_INVALID_ARG, "bad image size");
+  if (!(v->domain[0] > 0.0f) || !(v->domain[1] > 0.0f) || !(v->domain[2] > 0.0f) || !(v->up > 0.0f) || !(v->ve > 0.0f))
+    return fail(ctx, ITR_INVALID_ARG, "domain, cell size, up and ve must be positive");
+  if (v->debug < 0 || v->debug > 3) return fail(ctx, ITR_INVALID_ARG, "debug must be 0..3");
+  CU(cudaSetDevice(ctx->device));
+  const size_t T = (size_t)tw * th, N = (size_t)nx * ny, P = (size_t)width * height;
+  CU(ctx->rIn.ensure((T + 2 * N) * 4));
+  CU(ctx->rOut.ensure(P * 4));
+  uchar4* din = ctx->rIn.as<uchar4>();
+  CU(cudaMemcpyAsync(din, terrain, T * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(din + T, depth, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(din + T + N, vel, N * 4, cudaMemcpyHostToDevice, ctx->stream));
+  SceneArgs A;
+  memset(&A, 0, sizeof(A));
+  A.terrain = din; A.depth = din + T; A.vel = din + T + N;
+  A.tw = tw; A.th = th; A.nx = nx; A.ny = ny; A.width = width; A.height = height;
+  for (int i = 0; i < 3; ++i) {
+    A.cam_pos[i] = v->cam_pos[i]; A.cam_fwd[i] = v->cam_fwd[i]; A.cam_right[i] = v->cam_right[i]; A.cam_up[i] = v->cam_up[i];
+  }
+  A.focal = v->focal; A.dom_w = v->domain[0]; A.dom_h = v->domain[1]; A.cell = v->domain[2];
+  A.z_span = v->z_span; A.up = v->up; A.depth_span = v->depth_span; A.ve = v->ve; A.time = v->time;
+  A.rain = v->rain; A.wet = v->wet; A.overcast = v->overcast; A.vel_max = v->vel_max; A.base = v->base;
+  A.ortho = v->ortho ? 1 : 0; A.debug = v->debug;
+  A.out = ctx->rOut.as<uchar4>();
+  const dim3 blk(16, 16), grd((unsigned)((width + 15) / 16), (unsigned)((height + 15) / 16));
+  CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+  k_render_scene<<<grd, blk, 0, ctx->stream>>>(A);
+  CU(cudaGetLastError());
+  CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+  CU(cudaMemcpyAsync(rgba, ctx->rOut.p, P * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  float k_ms = 0;
+  cudaEventElapsedTime(&k_ms, ctx->ev[1], ctx->ev[2]);
+  ctx->kernel_ms = k_ms; ctx->total_ms = k_ms; ctx->launches = 1; ctx->cell_updates = 0;
   return ITR_OK;
 }
 

@@ -88,6 +88,15 @@ class DesignSpace(C.Structure):
     ]
 
 
+class SceneView(C.Structure):
+    _fields_ = [
+        ("cam_pos", C.c_float * 3), ("cam_fwd", C.c_float * 3), ("cam_right", C.c_float * 3), ("cam_up", C.c_float * 3),
+        ("focal", C.c_float), ("domain", C.c_float * 3), ("z_lo", C.c_float), ("z_span", C.c_float), ("up", C.c_float),
+        ("depth_span", C.c_float), ("ve", C.c_float), ("time", C.c_float), ("rain", C.c_float), ("wet", C.c_float),
+        ("overcast", C.c_float), ("vel_max", C.c_float), ("base", C.c_float), ("ortho", C.c_int32), ("debug", C.c_int32),
+    ]
+
+
 class Group(C.Structure):
     _fields_ = [
         ("grid", C.POINTER(Grid)), ("n_designs", C.c_int32), ("designs", C.POINTER(Design)),
@@ -115,6 +124,8 @@ SIGNATURES = {
     "itr_gpu_last_vjp_timing": (C.c_int, [C.c_void_p, _dp, _dp]),
     "itr_gpu_render_map": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, _fp, _fp, _fp, C.c_int32, C.c_float,
                                      C.c_int32, _u8p]),
+    "itr_gpu_render_scene": (C.c_int, [C.c_void_p, _u8p, C.c_int32, C.c_int32, _u8p, _u8p, C.c_int32, C.c_int32,
+                                       C.POINTER(SceneView), C.c_int32, C.c_int32, _u8p]),
     "itr_gpu_record_baseline": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(Design), _u32p,
                                           C.c_int32, C.c_int32, C.POINTER(Result)]),
     "itr_gpu_run_primitives": (C.c_int, [C.c_void_p, C.POINTER(Params), C.POINTER(Grid), C.POINTER(DesignSpace), C.c_int32,

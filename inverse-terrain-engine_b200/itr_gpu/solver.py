@@ -497,6 +497,24 @@ class GpuSolver:
         self._check(rc, "itr_gpu_render_map")
         return out
 
+    def render_scene(self, terrain_rgba, depth_rgba, vel_rgba, view, width: int, height: int) -> np.ndarray:
+        """itr_gpu_render_scene: the video's ray-marched frame (video/src/shaders/terrain.sksl) of
+        the textures (itr_gpu.scene_render builds them) under `view` (a SceneView), as an RGBA
+        uint8 image of shape (height, width, 4), row 0 the top."""
+        t = np.ascontiguousarray(terrain_rgba, dtype=np.uint8)
+        d = np.ascontiguousarray(depth_rgba, dtype=np.uint8)
+        v = np.ascontiguousarray(vel_rgba, dtype=np.uint8)
+        th, tw = t.shape[:2]
+        ny, nx = d.shape[:2]
+        if v.shape[:2] != (ny, nx):
+            raise ValueError("depth and velocity textures must have the same size")
+        out = np.zeros((height, width, 4), dtype=np.uint8)
+        V = view.to_c()
+        rc = self.lib.itr_gpu_render_scene(self.ctx, _ptr(t, C.c_uint8), tw, th, _ptr(d, C.c_uint8), _ptr(v, C.c_uint8),
+                                           nx, ny, C.byref(V), int(width), int(height), _ptr(out, C.c_uint8))
+        self._check(rc, "itr_gpu_render_scene")
+        return out
+
     def record_baseline(self, p: SolverParams, terrain: PreparedTerrain, monitors: MonitorSet, checkpoint_interval: int = 64,
                         want_peak: bool = False, ledger_rows: int = 0) -> GpuRun:
         """itr_gpu_record_baseline: run the unedited terrain with checkpoints every

@@ -662,3 +662,27 @@ extern "C" void orc_validation(int prec, int id, double* out4) {
   out4[0] = o.value; out4[1] = o.threshold; out4[2] = o.passed; out4[3] = o.extra;
 }
 
+
+// The video's ray-marched frame (video/src/shaders/terrain.sksl) restated in f32: the checker
+// for itr_gpu_render_scene. vf: 27 floats in itr_scene_view order (cam_pos[3], cam_fwd[3],
+// cam_right[3], cam_up[3], focal, domain[3], z_lo, z_span, up, depth_span, ve, time, rain, wet,
+// overcast, vel_max, base); rgba gets width x height pixels, row 0 the top.
+#include "scene_oracle.hpp"
+extern "C" void orc_render_scene(const uint8_t* terrain, int tw, int th, const uint8_t* depth, const uint8_t* vel, int nx,
+                                 int ny, const float* vf, int ortho, int debug, int width, int height, uint8_t* rgba) {
+  orc_scene::Shader S;
+  orc_scene::View& u = S.u;
+  for (int i = 0; i < 3; ++i) {
+    u.cam_pos[i] = vf[i]; u.cam_fwd[i] = vf[3 + i]; u.cam_right[i] = vf[6 + i]; u.cam_up[i] = vf[9 + i];
+  }
+  u.focal = vf[12]; u.W = vf[13]; u.H = vf[14]; u.cell = vf[15]; u.z_lo = vf[16]; u.z_span = vf[17]; u.up = vf[18];
+  u.depth_span = vf[19]; u.ve = vf[20]; u.time = vf[21]; u.rain = vf[22]; u.wet = vf[23]; u.overcast = vf[24];
+  u.vel_max = vf[25]; u.base = vf[26]; u.ortho = ortho; u.debug = debug;
+  S.terrain = {terrain, tw, th};
+  S.depth = {depth, nx, ny};
+  S.vel = {vel, nx, ny};
+  for (int py = 0; py < height; ++py)
+    for (int px = 0; px < width; ++px) orc_scene::pixel(S, px, py, width, height, rgba + ((size_t)py * width + px) * 4);
+}
+extern "C" double orc_sin_ref(double x) { return itr_math::sin_ref(x); }
+extern "C" float orc_powf_ref(float x, float y) { return itr_math::powf_ref(x, y); }

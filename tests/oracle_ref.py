@@ -73,6 +73,12 @@ def lib():
     L.orc_validation.argtypes = [C.c_int, C.c_int, _d]
     L.orc_render_map.argtypes = [C.c_int, C.c_int, C.c_double, _f, _f, _f, C.c_int, C.c_float, C.c_int, _u8]
     L.orc_set_locked_dt.argtypes = [_d, C.c_int64, C.c_double, C.c_int]
+    L.orc_render_scene.argtypes = [_u8, C.c_int, C.c_int, _u8, _u8, C.c_int, C.c_int, _f, C.c_int, C.c_int, C.c_int,
+                                   C.c_int, _u8]
+    L.orc_sin_ref.restype = C.c_double
+    L.orc_sin_ref.argtypes = [C.c_double]
+    L.orc_powf_ref.restype = C.c_float
+    L.orc_powf_ref.argtypes = [C.c_float, C.c_float]
     L.orc_last_locked.restype = C.c_int64
     L.orc_last_locked.argtypes = [_d, _d, C.c_int64]
     _lib = L
@@ -223,6 +229,18 @@ def locked(run, locked_dt=None, cfl_hard=0.5, record_dts=False):
     if record_dts:
         r["dts"] = dts
     return r
+
+
+def render_scene(terrain_rgba, depth_rgba, vel_rgba, view, width, height):
+    """The video's ray-marched frame restated on the CPU (RGBA uint8, (height, width, 4))."""
+    t = np.ascontiguousarray(terrain_rgba, dtype=np.uint8)
+    d = np.ascontiguousarray(depth_rgba, dtype=np.uint8)
+    v = np.ascontiguousarray(vel_rgba, dtype=np.uint8)
+    vf = np.ascontiguousarray(view.floats(), dtype=np.float32)
+    out = np.zeros((height, width, 4), dtype=np.uint8)
+    lib().orc_render_scene(P(t, C.c_uint8), t.shape[1], t.shape[0], P(d, C.c_uint8), P(v, C.c_uint8), d.shape[1], d.shape[0],
+                           P(vf, C.c_float), 1 if view.ortho else 0, int(view.debug), width, height, P(out, C.c_uint8))
+    return out
 
 
 def render_map(z, value, cell_size, mode=0, vex=1.0, scale=1, worse_dz=None):
