@@ -208,11 +208,13 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value);
  * the first step where that fails, or when the schedule has run out, the design goes back to
  * its last sync snapshot (state, peaks, integrator, ledger) and continues with the adaptive dt;
  * itr_result.dt_fallback_t gets the snapshot's time. The clip to the next sync instant still
- * applies. The schedule is copied; n = 0 (or dt NULL) clears it. With a schedule set the
- * designs start cold (no warm start), and the paths that have no locked dt return
- * ITR_UNSUPPORTED: impl 1 and 2, grids that only fit the tiled path, the adjoint and the
- * ladder. itr_gpu_record_baseline runs adaptively, like the reference's baseline. Device
- * memory while a schedule is set: 28 B per cell per design for the snapshot. */
+ * applies. The schedule is copied; n = 0 (or dt NULL) clears it. Both batched paths take it
+ * (the cluster kernel, and the tiled path of impl 2 and of grids too large for a cluster);
+ * with a schedule set the designs start cold (no warm start), and the paths that have no
+ * locked dt return ITR_UNSUPPORTED: impl 1 (plain, one design per launch), the adjoint and
+ * the ladder. itr_gpu_record_baseline runs adaptively, like the reference's baseline.
+ * Device memory while a schedule is set: 28 B (cluster) or 16 B (tiled) per cell per design
+ * for the snapshot. */
 int itr_gpu_set_locked_dt(itr_ctx* ctx, const double* dt, uint64_t n, double cfl_hard);
 
 /* Timing of the last run_batch on the device, CUDA events on the context stream:

@@ -664,15 +664,29 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
   const cudaStream_t st = ctx->stream;
   Vjp* tape = ctx->vjp;
   const size_t N = (size_t)A.nx * A.ny;
+  // baseline-locked dt: the LOCKED finalize, each followed by the snapshot copy it may ask for
+  const bool locked = A.locked_dt != nullptr;
+  const dim3 cgrid(64, (unsigned)n);
   k_plain_init<<<n, 1024, 0, st>>>(A);
-  k_plain_finalize<<<n, 32, 0, st>>>(A, nb, 1);
+  if (locked) {
+    k_plain_finalize_locked<<<n, 32, 0, st>>>(A, nb, 1);
+    k_plain_locked_copy<<<cgrid, 256, 0, st>>>(A);
+    *launches += 1;
+  } else {
+    k_plain_finalize<<<n, 32, 0, st>>>(A, nb, 1);
+  }
   *launches += 2;
   const int K = tape ? tape->K : ctx->steps_per_submit;
   if (tape) { tape->dt.assign(n, std::vector<double>()); tape->blocks = 0; }
   auto block = [&]() {
     for (int s = 0; s < K; ++s) {
       launch_update(A, grid, st);
-      k_plain_finalize<<<n, kFinThreads, 0, st>>>(A, nb, 0);
+      if (locked) {
+        k_plain_finalize_locked<<<n, kFinThreads, 0, st>>>(A, nb, 0);
+        k_plain_locked_copy<<<cgrid, 256, 0, st>>>(A);
+      } else {
+        k_plain_finalize<<<n, kFinThreads, 0, st>>>(A, nb, 0);
+      }
     }
   };
   cudaGraphExec_t ge = nullptr;
@@ -713,7 +727,7 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
     }
     if (ge) { const cudaError_t e = cudaGraphLaunch(ge, st); if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "cudaGraphLaunch: %s", cudaGetErrorString(e)); break; } }
     else block();
-    *launches += 2 * K;
+    *launches += (locked ? 3 : 2) * K;
     cudaError_t e = cudaMemcpyAsync(hc, A.ctl, (size_t)n * sizeof(PlainCtl), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "tiled run: %s", cudaGetErrorString(e)); break; }
@@ -1211,9 +1225,9 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   // ---- baseline-locked dt: the batched cluster kernel only; the baseline record runs adaptively ----
   const bool locked = !ctx->locked_dt.empty() && !ctx->recording;
   ctx->locked_run = false;
-  if (locked && (ctx->impl != 0 || ctx->vjp || ctx->defer))
-    return fail(ctx, ITR_UNSUPPORTED, "a baseline-locked dt schedule runs on the batched cluster kernel only (impl 0, "
-                                      "no adjoint, no ladder)");
+  if (locked && (ctx->impl == 1 || ctx->vjp || ctx->defer))
+    return fail(ctx, ITR_UNSUPPORTED, "a baseline-locked dt schedule runs on the batched paths only (impl 0 and 2; "
+                                      "no plain one-design path, adjoint or ladder)");
   // ---- warm starts from the baseline record (a locked run starts cold: its snapshot is the start) ----
   ctx->warm_steps.assign((size_t)n, 0);
   const WarmStart* warm_dev = nullptr;
@@ -1285,6 +1299,21 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.max_rows = max_rows;
     A.max_steps = max_steps;
     A.warm = warm_dev;
+    if (locked && e == cudaSuccess) {
+      const size_t nl = ctx->locked_dt.size();
+      e = ctx->lDt.ensure(nl * 8);
+      if (e == cudaSuccess) e = ctx->lS4.ensure((size_t)n * 4 * N * 4);
+      if (e == cudaSuccess) e = ctx->lSs.ensure((size_t)n * sizeof(PlainCtl));
+      if (e == cudaSuccess) e = ctx->lFb.ensure((size_t)n * 8);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->lDt.p, ctx->locked_dt.data(), nl * 8, cudaMemcpyHostToDevice, ctx->stream);
+      A.locked_dt = ctx->lDt.as<double>();
+      A.n_locked = (unsigned long long)nl;
+      A.cfl_hard = ctx->cfl_hard;
+      A.snap = ctx->lS4.as<float>();
+      A.snapctl = ctx->lSs.as<PlainCtl>();
+      A.fallback_t = ctx->lFb.as<double>();
+      ctx->locked_run = true;
+    }
     return e;
   };
   if (ctx->impl == 0 && !tiled) {
@@ -1337,7 +1366,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
         if (ctx->autotune && !locked) {
           // the tiled HBM path as one more candidate, timed over the same probe steps
           PlainArgs T;
-          CU(tiled_args(T));
+          CU(tiled_args(T));   // (no locked schedule here: the tiled candidate is timed only unlocked)
           T.max_steps = (unsigned long long)ctx->probe_steps;
           T.warm = nullptr;
           T.obj.enabled = 0; T.ledger = nullptr; T.max_rows = 0;
@@ -1401,7 +1430,6 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
       ctx->last_was_tiled = false;
     }
   }
-  if (tiled && locked) return fail(ctx, ITR_UNSUPPORTED, "a %dx%d grid takes the tiled path, which has no baseline-locked dt", nx, ny);
   if (tiled) {
     const int nb = n_tiles;
     PlainArgs A;

@@ -391,6 +391,18 @@ ITR_DEV StepPlan plan_step_c(const RunParams& P, double t, uint32_t sync_index, 
   return s;
 }
 
+// plan_step for a step whose dt before the sync clip is given (the baseline-locked dt).
+ITR_DEV StepPlan plan_step_dt(const RunParams& P, double t, uint32_t sync_index, double dt) {
+  StepPlan s;
+  double t_sync = dmin_num((double)(sync_index + 1) * P.sync, P.duration);
+  s.hits = t + dt >= t_sync - 1e-9 * P.sync;
+  if (s.hits) dt = t_sync - t;
+  s.rain = rain_integral(P.rain, t, t + dt);
+  s.t_new = s.hits ? t_sync : t + dt;
+  s.dt = dt;
+  return s;
+}
+
 // plan_step_c for a step whose dt before the sync clip is given: the baseline-locked dt
 // (solver.rs:452-456 sets dt from the schedule, then :484-487 clip it to the sync instant).
 ITR_DEV StepPlan plan_step_dt_c(const RunParams& P, double t, uint32_t sync_index, double dt, RainCursor& cu) {

@@ -46,6 +46,12 @@ struct PlainCtl {
   StepPlan pl;
   StepK k;
   float2 inf[kMaxInflow];   // inflow groups at the step's start time (inflow_values)
+  // baseline-locked dt (k_plain_finalize_locked): smax of the current state, whether the
+  // schedule still holds, and the state copy the finalize asks of k_plain_locked_copy
+  // (1 save into the sync snapshot, 2 restore from it)
+  double s_cur;
+  int locked_live;
+  int copy_req;
 };
 
 struct PlainArgs {
@@ -80,6 +86,14 @@ struct PlainArgs {
   double* dt_log;     // optional, per design a ring of max_log (dt, rain, t): slot step % max_log
   int max_log;
   const WarmStart* warm;   // optional, per design (state NULL: cold)
+  // Baseline-locked dt (SolverParams::locked_dt / cfl_hard, solver.rs:42-46); read only by
+  // k_plain_finalize_locked and k_plain_locked_copy
+  const double* locked_dt;   // n_locked dts of the baseline, shared by every design
+  unsigned long long n_locked;
+  double cfl_hard;
+  float* snap;               // per design [4][nx*ny]: h, qx, qy, peaks at the last sync snapshot
+  PlainCtl* snapctl;         // per design: the control block at that snapshot
+  double* fallback_t;        // per design: time the run fell back to adaptive dt, -1 for none
 };
 
 // Pointers of design d inside a launch over n_designs designs.
@@ -248,12 +262,19 @@ constexpr int kFinThreads = 256;
 // Advance the integrator after a step (or plan the first step when `first`). Launched with
 // a block of warps per design: all of them sum the tile partials (one warp alone waits on
 // hundreds of dependent rounds of loads for a large grid), warp 0 does the rest.
-__global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
+// LOCKED: the baseline-locked dt (solver.rs:436-483): each step takes the schedule's dt while
+// dt * smax of the current state stays within cfl_hard; at the first step where it would not
+// (or the schedule has run out) the control block goes back to the last sync snapshot, which
+// the next k_plain_locked_copy completes with the state planes, and the run continues with the
+// adaptive dt. Snapshots: at the start and after every sync's abort tests.
+template <bool LOCKED>
+ITR_DEV void plain_finalize_body(const PlainArgs& A, int n_blocks, int first) {
   __shared__ double red[32][kPart];
   const PlainDesign D = plain_design(A, blockIdx.x, n_blocks);
   PlainCtl& c = *D.ctl;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const RunParams& P = A.P;
+  if constexpr (LOCKED) { if (threadIdx.x == 0) c.copy_req = 0; }   // the last request has been served
   if (c.done) return;
   double tot[kPart] = {0, 0, 0, 0, 0, 0, 0};
   if (!first) {
@@ -294,6 +315,7 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
     __syncwarp();
     if (badv) { if (lane == 0) { c.status = 3; c.done = 1; } return; }
     if (lane == 0) c.dt_cfl = smax > 0.0 ? P.cfl / smax : P.dt_max;
+    if constexpr (LOCKED) { if (lane == 0) c.s_cur = smax; }
     __syncwarp();
     if (c.pl.hits) {
       int decision = 0;
@@ -341,7 +363,43 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
       }
       __syncwarp();
       if (c.done) return;
+      if constexpr (LOCKED) {   // sync snapshot (solver.rs:611-614)
+        if (lane == 0 && c.locked_live) { A.snapctl[blockIdx.x] = c; c.copy_req = 1; }
+        __syncwarp();
+      }
     }
+  }
+  if constexpr (LOCKED) {
+    if (lane == 0) {
+      if (first) {   // the snapshot at the start (solver.rs:444-447)
+        c.locked_live = 1;
+        A.fallback_t[blockIdx.x] = -1.0;
+        A.snapctl[blockIdx.x] = c;
+        c.copy_req = 1;
+      }
+      if (!(c.t < P.duration && c.sync_index < P.n_sync)) {
+        c.done = 1;
+      } else if (c.step >= A.max_steps) {
+        c.status = 4; c.done = 1;
+      } else if (c.locked_live && !(c.step < A.n_locked && A.locked_dt[c.step] * c.s_cur <= A.cfl_hard)) {
+        // back to the last sync snapshot, adaptive from here on. A snapshot taken by this very
+        // finalize (save still pending) is the current state: nothing to copy back.
+        const int pending_save = c.copy_req;
+        c = A.snapctl[blockIdx.x];
+        c.locked_live = 0;
+        c.copy_req = pending_save == 1 ? 0 : 2;
+        A.fallback_t[blockIdx.x] = c.t;
+      }
+    }
+    __syncwarp();
+    if (c.done) return;
+    if (lane < P.inflow.n) c.inf[lane] = inflow_values(P.inflow, lane, c.t, P.g);
+    if (lane == 0) {
+      const double dt = c.locked_live ? A.locked_dt[c.step] : dmin_num(c.dt_cfl, P.dt_max);
+      c.pl = plan_step_dt(P, c.t, c.sync_index, dt);
+      c.k = step_consts(P, c.pl.dt, c.pl.rain);
+    }
+    return;
   }
   // inflow ghosts of the next step, at its start time c.t (fill_ghosts(t), solver.rs)
   if (lane < P.inflow.n) c.inf[lane] = inflow_values(P.inflow, lane, c.t, P.g);
@@ -354,6 +412,31 @@ __global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) {
       D.dt_log[3 * slot] = c.pl.dt; D.dt_log[3 * slot + 1] = c.pl.rain; D.dt_log[3 * slot + 2] = c.t;
     }
     c.k = step_consts(P, c.pl.dt, c.pl.rain);
+  }
+}
+
+__global__ void k_plain_finalize(const PlainArgs A, int n_blocks, int first) { plain_finalize_body<false>(A, n_blocks, first); }
+__global__ void k_plain_finalize_locked(const PlainArgs A, int n_blocks, int first) {
+  plain_finalize_body<true>(A, n_blocks, first);
+}
+
+// Baseline-locked dt: after a finalize that asked for it, copy each design's current state
+// plane and peaks into its sync snapshot (copy_req 1) or back from it (copy_req 2). A grid of
+// (blocks, designs); the control block is read only, so every block sees the same request.
+__global__ void k_plain_locked_copy(const PlainArgs A) {
+  const int d = blockIdx.y;
+  const PlainDesign D = plain_design(A, d, 0);
+  const PlainCtl& c = *D.ctl;
+  const int req = c.copy_req;
+  if (c.done || req == 0) return;
+  const size_t N = (size_t)A.nx * A.ny, pl = (size_t)c.par * N;
+  float* s = A.snap + (size_t)d * 4 * N;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    if (req == 1) {
+      s[i] = D.H[pl + i]; s[N + i] = D.QX[pl + i]; s[2 * N + i] = D.QY[pl + i]; s[3 * N + i] = D.PK[i];
+    } else {
+      D.H[pl + i] = s[i]; D.QX[pl + i] = s[N + i]; D.QY[pl + i] = s[2 * N + i]; D.PK[i] = s[3 * N + i];
+    }
   }
 }
 
@@ -405,6 +488,7 @@ __global__ void k_plain_init(const PlainArgs A) {
     memset(&c, 0, sizeof(c));
     c.v0 = v * P.area; c.volume = c.v0;
     c.dt_cfl = s > 0.0 ? dmin_num(P.cfl / s, P.dt_max) : P.dt_max;
+    c.s_cur = s;
     *D.ctl = c;
   }
 }

@@ -10,9 +10,9 @@ CPU: the oracle keeps the reference's own properties (crates/itr-hydro/tests/rep
 a zero edit under its own locked schedule is the baseline bit for bit with no fallback; an
 edit that speeds the flow up past a tight cfl_hard falls back and stays healthy, its ledger
 closing to 1e-4 (f32) and 1e-10 (f64) of the gross input.
-GPU: the batched cluster kernel under a locked schedule against the f32 oracle under the same
-schedule, bit for bit (steps, end time, depth, peaks, monitor maxima, fallback time), for a
-zero edit, an edit that stays locked and an edit that falls back.
+GPU: the batched cluster kernel and the tiled path under a locked schedule against the f32
+oracle under the same schedule, bit for bit (steps, end time, depth, peaks, monitor maxima,
+fallback time), for a zero edit, an edit that stays locked and an edit that falls back.
 """
 from __future__ import annotations
 
@@ -181,14 +181,43 @@ def test_gpu_locked_matches_oracle(gpu):
 
 
 @pytest.mark.gpu
+def test_gpu_locked_tiled_path(gpu):
+    """The tiled path (state in HBM; the path of grids too large for a cluster) under the same
+    schedules: the same bits as the oracle, fallback included, twice on one context."""
+    b = base()
+    zero = PreparedTerrain(b)
+    dts = run(b, zero, params(), 32, record=True)["dts"]
+    terrs = [zero, PreparedTerrain(b).apply_edit(small_edit()), PreparedTerrain(b).apply_edit(fast_edit())]
+    gpu.set_option("impl", 2)
+    try:
+        for cfl_hard in (0.5, 0.36, 0.36):
+            p = params(cfl_hard)
+            p.locked_dt = dts
+            runs = gpu.run_batch(p, terrs, monitors(), want_peak=True, want_depth=True, ledger_rows=64)
+            for i, t in enumerate(terrs):
+                o = run(b, t, params(cfl_hard), 32, locked=dts)
+                same(runs[i], o, f"tiled, cfl_hard {cfl_hard} design {i}")
+            if cfl_hard == 0.36:
+                assert runs[2].dt_fallback_t >= 0.0
+        # a schedule cut short falls back when it runs out
+        p = params()
+        p.locked_dt = dts[: len(dts) // 3]
+        r = gpu.run_batch(p, [zero], monitors(), want_peak=True, want_depth=True, ledger_rows=64)[0]
+        same(r, run(b, zero, params(), 32, locked=dts[: len(dts) // 3]), "tiled, short schedule")
+        assert r.dt_fallback_t >= 0.0
+    finally:
+        gpu.set_option("impl", 0)
+
+
+@pytest.mark.gpu
 def test_gpu_locked_unsupported_paths(gpu):
     """Paths without a locked schedule say so (ITR_UNSUPPORTED, the reference's Err from
-    run_batch, evaluator.rs:231-238) instead of running adaptively."""
+    run_batch, evaluator.rs:231-238) instead of running adaptively: the plain one-design path."""
     b = base()
     zero = PreparedTerrain(b)
     p = params()
     p.locked_dt = np.full(10, 0.1)
-    gpu.set_option("impl", 2)
+    gpu.set_option("impl", 1)
     try:
         with pytest.raises(UnsupportedError):
             gpu.run_batch(p, [zero], monitors())
