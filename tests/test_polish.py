@@ -1,0 +1,129 @@
+"""Gradient polishing of an incumbent (itr_gpu/polish.py): the adjoint proposes, the exact
+forward decides.
+
+CPU: the host logic against a stand-in solver with a known J and guard: steps follow the
+gradient inside the trust region, every proposal is snapped onto the quantisation grid
+(DesignSpace::q, crates/itr-core/src/design.rs:259-261) and the bounds, a step that breaks
+the guard or raises J is never kept, a berm whose height turns negative becomes a swale.
+GPU: a real incumbent on a small wet scene with assets and a guard area: J goes down, the
+result is feasible, its J is the exact forward's (a fresh itr_gpu_run_primitives gives the
+same bits), the f32 CPU oracle rerun of the polished design gives the same monitor maxima
+bit for bit, and the f64 oracle rerun agrees to 1e-3 relative in J.
+"""
+from __future__ import annotations
+
+import math
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+import oracle_ref as orc
+from helpers import base_arrays, design_dict
+from itr_gpu import (Asset, Hyetograph, MonitorSet, Objective, ObjectiveDef, PreparedTerrain, Segment, SolverParams,
+                     synthetic_terrain)
+from itr_gpu.design import BERM, SWALE, Primitive, materialize
+from itr_gpu.polish import polish
+
+
+class QuadSolver:
+    """J = sum_i (h_i - 0.22)^2 + (w_i - 6)^2 / 10 + (L_i - 47)^2 / 100; feasible while every
+    height stays <= 0.3 (a stand-in guard)."""
+
+    def __init__(self):
+        self.calls = 0
+
+    @staticmethod
+    def j(prims):
+        return sum((p.height - 0.22) ** 2 + (p.width - 6.0) ** 2 / 10 + (p.length - 47.0) ** 2 / 100 for p in prims)
+
+    def run_primitives(self, params, base, designs, monitors, editable, max_abs_dz, objective=None, baseline_max=None):
+        self.calls += 1
+        prims = designs[0]
+        ok = all(p.height <= 0.3 for p in prims)
+        return [SimpleNamespace(j=self.j(prims), feasible=ok, status=0)], [0.0], [0.0]
+
+    def vjp_primitives(self, params, base, designs, monitors, objective, editable, max_abs_dz, checkpoint_interval=128):
+        g = [[2 * (p.height - 0.22), (p.width - 6.0) / 5, (p.length - 47.0) / 50] for p in designs[0]]
+        return None, [np.array(g)]
+
+
+def quantised(v, step):
+    return abs(v / step - round(v / step)) < 1e-9
+
+
+def test_polish_host_logic():
+    s = QuadSolver()
+    obj = SimpleNamespace(monitors=MonitorSet())
+    start = [Primitive(SWALE, 10.0, 10.0, 80.0, 3.5, 30.0, -0.12), Primitive(BERM, 30.0, 20.0, 25.0, 7.5, 0.0, 0.05)]
+    res = polish(s, None, None, start, obj, None, 1.0, iters=40, radius=(0.1, 1.0, 10.0))
+    assert res.j < res.j_start and res.accepted > 0 and res.feasible
+    assert all(b <= a for a, b in zip([res.j_start] + res.history, res.history))   # J never goes up
+    for p in res.prims:
+        assert quantised(p.height, 0.01) and quantised(p.width, 0.5) and quantised(p.length, 0.5)
+        assert -0.5 <= p.height <= 0.3 and 3.0 <= p.width <= 8.0 and 20.0 <= p.length <= 100.0
+        assert (p.kind == BERM) == (p.height > 0.0)                 # the swale turned into a berm
+        assert abs(p.height - 0.22) <= 0.011 and abs(p.width - 6.0) <= 0.5 and abs(p.length - 47.0) <= 0.5
+    assert res.evaluations == s.calls
+
+
+def test_polish_never_keeps_an_infeasible_step():
+    """Optimum beyond the guard (h = 0.5 > 0.3): heights stop at or below 0.3."""
+    class Beyond(QuadSolver):
+        @staticmethod
+        def j(prims):
+            return sum((p.height - 0.5) ** 2 for p in prims)
+
+        def vjp_primitives(self, *a, **k):
+            return None, [np.array([[2 * (p.height - 0.5), 0.0, 0.0] for p in a[2][0]])]
+    s = Beyond()
+    obj = SimpleNamespace(monitors=MonitorSet())
+    res = polish(s, None, None, [Primitive(BERM, 0, 0, 40.0, 5.0, 0.0, 0.1)], obj, None, 1.0, iters=30)
+    assert res.feasible and res.accepted > 0
+    assert 0.25 <= res.prims[0].height <= 0.3
+
+
+# ---------------------------------------------------------------------------- GPU ----------
+
+def wet_scene():
+    nx, ny = 24, 16
+    base = synthetic_terrain(nx, ny, 5.0, lambda x, y: 2.0 - 0.01 * x + 0.2 * math.sin(y / 15.0) + 0.1 * math.cos(x / 20.0),
+                             n=0.03, segments=[Segment("transmissive", "east")])
+    p = SolverParams(180.0, 30.0, rain=Hyetograph.from_mm_h([(0, 50), (60, 120), (180, 0)]), initial_depth=0.3)
+    return base, p
+
+
+@pytest.mark.gpu
+def test_polish_incumbent_on_device():
+    from itr_gpu import GpuSolver
+    base, p = wet_scene()
+    nx, ny = base.nx, base.ny
+    assets = [5 * nx + 8, 9 * nx + 15, 12 * nx + 20]
+    guard = [3 * nx + 21, 4 * nx + 21]
+    probe = Objective(ObjectiveDef([Asset(f"a{i}", [c], 10.0) for i, c in enumerate(assets)], guard))
+    g = GpuSolver()
+    try:
+        r0 = g.run_batch(p, [PreparedTerrain(base)], probe.monitors)[0]
+        peaks = {c: float(r0.monitor_max[probe.monitors.position(c)]) for c in assets + guard}
+        odef = ObjectiveDef([Asset(f"a{i}", [c], peaks[c] - 0.004, 1.0 + i) for i, c in enumerate(assets)], guard,
+                            guard_tolerance_m=0.002, earth_weight=1e-4)
+        obj = Objective(odef)
+        baseline = np.array([peaks[int(c)] for c in obj.monitors.cells])
+        editable = np.ones((ny, nx), dtype=bool)
+        start = [Primitive(BERM, 55.0, 45.0, 40.0, 6.0, 30.0, 0.10), Primitive(SWALE, 85.0, 30.0, 30.0, 5.0, 110.0, -0.10)]
+        res = polish(g, p, base, start, obj, editable, 1.0, baseline_max=baseline, iters=6, checkpoint_interval=16)
+        assert res.feasible and res.accepted > 0 and res.j < res.j_start, (res.j_start, res.history)
+        # the exact forward: a fresh device run of the polished design gives the same J bits
+        runs, cut, fill = g.run_primitives(p, base, [res.prims], obj.monitors, editable, 1.0, objective=obj,
+                                           baseline_max=baseline)
+        assert runs[0].j == res.j and runs[0].feasible
+    finally:
+        g.close()
+    # the CPU oracle reruns of the polished design: f32 bit for bit, f64 to 1e-3 in J
+    e = materialize(res.prims, base.fine.geo, nx, ny, editable, 1.0)
+    t = PreparedTerrain(base).apply_edit(e)
+    o32 = orc.flat_run(base_arrays(base), design_dict(t, p), p, obj.monitors)
+    np.testing.assert_array_equal(o32["monitor_max"].astype(np.float32), runs[0].monitor_max.astype(np.float32))
+    o64 = orc.flat_run64(base_arrays(base), design_dict(t, p), p, obj.monitors)
+    j64 = obj.evaluate(o64["monitor_max"], e.cut_m3, e.fill_m3, baseline)["j"]
+    assert abs(j64 - res.j) <= 1e-3 * abs(j64), (j64, res.j)
