@@ -14,6 +14,9 @@ wall segment along a column; all edges closed. Seeded draws stand in for proptes
     ledger over f32 state; gpu.rs:41-53's rain-volume bound), device bitwise equal to f32.
   * Mirror: an east-west mirrored bed with walls only, 200 s of rain: mirrored depths within
     1e-9 (f64; the reference's bound) and 1e-6 (f32 and device).
+  * Crest lake at rest (equivalence.rs:245-268): a 1-cell berm kept by level-4 crest faces,
+    still water below its crest: |q| < 1e-10 and ledger residual < 1e-12 in f64; the device
+    keeps the depth to 1e-4 and equals the f32 oracle bit for bit.
 """
 from __future__ import annotations
 
@@ -143,3 +146,38 @@ def test_mirror_metamorphic_device(gpu):
         h = gpu.run_batch(p, [PreparedTerrain(base)], MonitorSet())[0].depth.astype(np.float64)
         hs.append(h[:, ::-1] if m else h)
     assert np.abs(hs[0] - hs[1]).max() < 1e-6
+
+
+def crest_case():
+    """equivalence.rs:245-268: 64 x 48 at 1 m, 0.2 sin(col / 9) plus a 1-cell berm of 1 m at
+    column 30, coarsened 4x (crest faces keep the berm); still water at stage 0.6 m, 120 s."""
+    from itr_gpu.terrain import FineTerrain, GeoTransform, TerrainBase
+    nx, ny = 64, 48
+    cols = np.arange(nx)
+    dem = np.tile(0.2 * np.sin(cols / 9.0) + np.where(cols == 30, 1.0, 0.0), (ny, 1))
+    geo = GeoTransform(0.0, float(ny), 1.0, 1.0)
+    walls = np.zeros((ny, nx), bool)
+    base = TerrainBase(FineTerrain(dem, walls, np.full((ny, nx), 0.03), geo), 4, [])
+    p = SolverParams(120.0, 30.0, initial_stage=0.6)
+    return dem, walls, geo, base, p
+
+
+def test_crest_level_lake_at_rest_oracle():
+    dem, walls, geo, base, p = crest_case()
+    s = orc.Scene(dem, walls, 0.03, geo, 4, [])
+    assert s.mode == 1   # crest faces at level 4
+    o = s.run(p, MonitorSet(), prec=1)
+    assert max(np.abs(o["qx"]).max(), np.abs(o["qy"]).max()) < 1e-10
+    assert o["rel_residual"] < 1e-12
+
+
+@pytest.mark.gpu
+def test_crest_level_lake_at_rest_device(gpu):
+    _, _, _, base, p = crest_case()
+    t = PreparedTerrain(base)
+    d = design_dict(t, p)
+    r = gpu.run_batch(p, [t], MonitorSet(), ledger_rows=8)[0]
+    assert np.abs(r.depth - d["h0"]).max() <= 1e-4
+    o = orc.flat_run(base_arrays(base), d, p, MonitorSet())
+    assert r.steps == o["steps"]
+    assert_bitwise(r.depth.ravel(), o["h"].ravel(), "crest lake")
