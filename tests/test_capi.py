@@ -38,7 +38,7 @@ def test_struct_layouts_match_header(tmp_path):
     from itr_gpu import _lib
     structs = {"itr_params": _lib.Params, "itr_grid": _lib.Grid, "itr_design": _lib.Design,
                "itr_objective": _lib.Objective, "itr_result": _lib.Result, "itr_group": _lib.Group,
-               "itr_primitive": _lib.Primitive, "itr_design_space": _lib.DesignSpace}
+               "itr_primitive": _lib.Primitive, "itr_design_space": _lib.DesignSpace, "itr_scene_view": _lib.SceneView}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
