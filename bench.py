@@ -436,6 +436,9 @@ def main():
                        "parallelism": f"designs sharded over {world} GPU(s), 1 design per thread-block cluster",
                        "l2": "flushed between timed iterations (256 MB write)"},
             "designs_per_s": designs_per_s,
+            "precision": ("device path bit-identical to the f32 CPU port (tests/test_gpu_parity.py); that port's "
+                          "per-cell peak depth within 2.0e-6 m of the f64 oracle on config 1, J within 3e-7 "
+                          "relative (tests/test_precision.py; bar 1e-4 m)"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_source": src,
                          "model": f"{BYTES_PER_CELL_STEP} B/cell-step x {cell_steps:.4g} cell-steps per launch"},
