@@ -271,3 +271,21 @@ def test_ledger_vs_f64_oracle(gpu):
     # storage and outflow against the f64 oracle (f32 state vs f64 state: 1e-3 relative)
     np.testing.assert_allclose(r.ledger[-1, 1], o64["ledger"][-1, 1], rtol=1e-3)
     np.testing.assert_allclose(r.ledger[-1, 2], o64["ledger"][-1, 2], rtol=1e-9)
+
+
+@pytest.mark.parametrize("impl", ["batched", "tiled"])
+def test_outputs_do_not_change_the_trajectory(gpu, impl):
+    """crates/itr-hydro/tests/equivalence.rs:177: asking for the per-cell peak, the final
+    depth and the ledger rows changes nothing of the run (steps, end time, monitor maxima)."""
+    sc = small_valley(900.0)
+    terrs = [t for _, _, t in sc.designs(3)]
+    gpu.set_option("impl", IMPL[impl])
+    try:
+        bare = gpu.run_batch(sc.params, terrs, sc.monitors, want_peak=False, want_depth=False, ledger_rows=0)
+        full = gpu.run_batch(sc.params, terrs, sc.monitors, want_peak=True, want_depth=True, ledger_rows=64)
+    finally:
+        gpu.set_option("impl", 0)
+    for a, b in zip(bare, full):
+        assert a.steps == b.steps and a.t_end == b.t_end and a.status == b.status
+        np.testing.assert_array_equal(a.monitor_max, b.monitor_max)
+        assert len(b.ledger) == b.sync_count
