@@ -108,7 +108,9 @@ typedef struct itr_design {
   const float* dzy;         /* (ny+1)*nx */
   const float* dzx2;        /* crest mode only, else NULL */
   const float* dzy2;        /* crest mode only, else NULL */
-  const float* h0;          /* nx*ny initial depth, or NULL for params.initial_depth on open cells */
+  const float* h0;          /* nx*ny initial depth, or NULL for params.initial_depth on open cells;
+                               infinite values or values above 1e4 m give ITR_INVALID_ARG (the first
+                               dt would vanish), NaN or negative ones an unhealthy run */
   double cut_m3, fill_m3;   /* earthwork volumes of the edit (J's earthwork term)      */
   const double* z_edge;     /* 2*nx+2*ny, indexed like grid.bc: z level above the datum of the
                                interior cell behind each boundary cell (PreparedTerrain::z_level,

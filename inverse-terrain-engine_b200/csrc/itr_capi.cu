@@ -336,6 +336,8 @@ static int autotune(itr_ctx* ctx, const BatchArgs& A0, const std::vector<LaunchC
 }
 
 // ------------------------------------------------------------------ input checks ------
+constexpr float kMaxInitialDepth = 1e4f;   // m
+
 static int check_inputs(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int32_t n, const itr_design* ds,
                         const uint32_t* mon, int32_t n_mon, const itr_objective* ob) {
   if (!p || !g) return fail(ctx, ITR_INVALID_ARG, "params and grid are required");
@@ -381,6 +383,14 @@ static int check_inputs(itr_ctx* ctx, const itr_params* p, const itr_grid* g, in
   for (int32_t d = 0; d < n && !ctx->mat; ++d) {
     if (!ds[d].dzx || !ds[d].dzy) return fail(ctx, ITR_INVALID_ARG, "design %d has no face jumps", d);
     if (g->mode == ITR_FACE_CREST && (!ds[d].dzx2 || !ds[d].dzy2)) return fail(ctx, ITR_INVALID_ARG, "design %d: crest mode needs dzx2/dzy2", d);
+    // An infinite or absurdly deep start makes the first CFL dt zero or vanishing, so the run
+    // would crawl towards its step limit; NaN and negative depths are left to the solver's
+    // health test (Unhealthy at the first step, numerics.rs:163, solver.rs:541-544).
+    if (ds[d].h0)
+      for (size_t i = 0; i < (size_t)g->nx * g->ny; ++i)
+        if (std::isinf(ds[d].h0[i]) || ds[d].h0[i] > kMaxInitialDepth)
+          return fail(ctx, ITR_INVALID_ARG, "design %d: initial depth %g at cell %zu is infinite or above %g m", d,
+                      (double)ds[d].h0[i], i, (double)kMaxInitialDepth);
   }
   if (ob) {
     if (ob->n_assets < 0 || ob->n_guard < 0) return fail(ctx, ITR_INVALID_ARG, "objective counts are negative");
