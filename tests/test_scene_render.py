@@ -82,6 +82,32 @@ def tone(c):
     return [u8(x) for x in v ** (1.0 / 2.2)]
 
 
+def test_texture_codes_and_camera():
+    """The packers invert as video/src/data.rs:94-96 decodes (16-bit codes within half a code
+    step), the velocity code as terrain.sksl:84-87 reads it, and look() builds Camera::look's
+    frame (video/src/lib.rs:35-42): unit forward, horizontal right, up = right x forward."""
+    rng = np.random.default_rng(3)
+    z = rng.uniform(3.0, 27.0, (20, 30))
+    t, lo, span = terrain_texture(z, np.full((20, 30), 60))
+    back = (t[..., 0].astype(np.float64) * 256 + t[..., 1]) / 65535.0 * span + lo
+    assert np.abs(back - z).max() <= 0.5 * span / 65535.0 + 1e-12 and np.all(t[..., 2] == 60)
+    d = rng.uniform(0.0, 3.0, (20, 30))
+    d[0, 0] = 0.0
+    dt_ = depth_texture(d, 4.0)
+    back = (dt_[..., 0].astype(np.float64) * 256 + dt_[..., 1]) / 65535.0 * 4.0
+    assert np.abs(back - d).max() <= 0.5 * 4.0 / 65535.0 + 1e-12
+    assert dt_[0, 0, 2] == 0 and np.all(dt_[d > 0][:, 2] == 255)
+    u, v = rng.uniform(-2, 2, (20, 30)), rng.uniform(-2, 2, (20, 30))
+    vt = velocity_texture(u, v, 2.0)
+    assert np.abs((vt[..., 0].astype(np.float64) - 128.0) / 127.0 * 2.0 - u).max() <= 0.5 * 2.0 / 127.0 + 1e-12
+    assert np.abs((vt[..., 1].astype(np.float64) - 128.0) / 127.0 * 2.0 - v).max() <= 0.5 * 2.0 / 127.0 + 1e-12
+    fwd, right, up, focal = look((-80.0, -60.0, 120.0), (225.0, 175.0, 10.0), 50.0)
+    f, r, w = np.array(fwd), np.array(right), np.array(up)
+    assert abs(np.linalg.norm(f) - 1) < 1e-6 and abs(np.linalg.norm(r) - 1) < 1e-6 and abs(r[2]) < 1e-7
+    assert np.allclose(w, np.cross(r, f), atol=1e-6) and w[2] > 0 and abs(f @ r) < 1e-6
+    assert abs(focal - 0.5 / math.tan(math.radians(25.0))) < 1e-6
+
+
 def test_deterministic_sin_and_pow():
     rng = np.random.default_rng(5)
     xs = np.concatenate([rng.uniform(-10, 10, 2000), rng.uniform(-4e6, 4e6, 2000), [0.0, math.pi / 2, -math.pi]])
