@@ -271,6 +271,55 @@ def boundary_summary(g):
     return out
 
 
+# The reference's own GPU throughput cases and its published numbers for them (wgpu on an
+# Apple M4 Pro through Metal, crates/itr-gpu/README.md:62-65): (label, n, designs, duration s,
+# useful cell-updates/s).
+GPUBENCH_CASES = (("512^2 x1", 512, 1, 120.0, 1.35e9), ("128^2 x16", 128, 16, 120.0, 0.66e9),
+                  ("128^2 x64", 128, 64, 120.0, 1.15e9), ("1024^2 x1", 1024, 1, 40.0, 1.40e9))
+
+
+def gpubench_summary(g):
+    """crates/itr-gpu/examples/gpubench.rs:17-33 on this operator: a plane 5 - 0.01 x +
+    0.3 sin(y / 40) at 2 m, closed walls, still water at stage 2 m, 100 mm/h of rain, sync every
+    quarter of the run; one warm-up call, then one run_batch call timed from the host as the
+    reference times it (packing, copies, kernels and results included): useful cell-updates/s
+    = steps x n^2 x designs / wall. Beside each, the reference's published number (other
+    hardware, for context)."""
+    import math
+
+    import numpy as np
+
+    from itr_gpu import Hyetograph, MonitorSet, PreparedTerrain, SolverParams, synthetic_terrain
+
+    def plane(x, y):
+        return 5.0 - 0.01 * x + 0.3 * np.sin(y / 40.0)
+    plane.vectorized = True
+    out = {}
+    for label, n, cands, dur, ref in GPUBENCH_CASES:
+        base = synthetic_terrain(n, n, 2.0, plane, n=0.03, segments=[])
+        p = SolverParams(dur, dur / 4.0, rain=Hyetograph.from_mm_h([(0.0, 100.0), (1e9, 100.0)]), initial_stage=2.0)
+        ts = [PreparedTerrain(base) for _ in range(cands)]
+        g.run_batch(p, ts, MonitorSet(), want_depth=False)
+        t0 = time.perf_counter()
+        runs = g.run_batch(p, ts, MonitorSet(), want_depth=False)
+        wall = time.perf_counter() - t0
+        upd = float(sum(r.steps for r in runs)) * n * n
+        out[label] = {"steps": int(runs[0].steps), "wall_s": wall, "cell_updates_per_s": upd / wall,
+                      "reference_m4pro_metal": ref, "over_reference": upd / wall / ref}
+        assert math.isfinite(out[label]["cell_updates_per_s"])
+    out["note"] = ("the reference's numbers are wgpu on an Apple M4 Pro (Metal); running them here is unavailable on "
+                   "this box. Ours: host-timed run_batch, as gpubench.rs times it")
+    return out
+
+
+def guarded(fn, *a):
+    """A side summary must not cost the bench line: its failure is reported in its place."""
+    try:
+        return fn(*a)
+    except Exception as e:  # noqa: BLE001
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def run_reference(args):
     rank, world, _ = dist_setup(args.gpus)
     if rank != 0:
@@ -419,6 +468,7 @@ def main():
         adj = None if args.no_adjoint or world > 1 or args.duration is not None else adjoint_summary(g)
         lad = None if args.no_ladder or world > 1 or args.duration is not None else ladder_summary(g)
         bnd = None if args.no_ladder or world > 1 or args.duration is not None else boundary_summary(g)
+        gpb = None if args.no_ladder or world > 1 or args.duration is not None else guarded(gpubench_summary, g)
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(sc, terrs)
@@ -448,6 +498,7 @@ def main():
             "adjoint": adj,
             "ladder": lad,
             "boundaries": bnd,
+            "reference_gpubench": gpb,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
             "clocks": clk.summary(),
