@@ -3,7 +3,7 @@
 // The reference's objective J uses softplus(x) = log1p(exp(x)) from the pure-Rust `libm`
 // crate 0.2.16 (crates/itr-core/src/objective.rs:70-75). That crate is not part of the
 // reference tree. The incumbent early abort (`lb >= incumbent`, evaluator.rs:100-104) runs on
-// the device, and the same decision must come out on the host checker, so both sides call
+// the device, and the same decision must come out of the host-side oracle, so both sides call
 // THIS one implementation, compiled without FMA contraction (nvcc -fmad=false,
 // gcc -ffp-contract=off): identical inputs give identical bits on the CPU and the GPU.
 //
@@ -20,7 +20,7 @@
 // correctly rounded, and the reference's libm values are matched only to that level.
 // The f32 wrappers (sinf_ref, expf_ref, powf_ref) serve the headless scene render, whose
 // shader leaves sin / exp / pow to the platform: with these the device image and the CPU
-// checker's agree bit for bit.
+// oracle's agree bit for bit.
 #pragma once
 #include <stdint.h>
 #include <string.h>

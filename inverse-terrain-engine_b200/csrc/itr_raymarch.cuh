@@ -19,7 +19,7 @@
 // below / above the first); the sRGB-ish result is rounded to 8 bits directly (the shader's
 // half4 output is not rounded to half first). The shader leaves sin, exp and pow to the
 // platform; here they are itr_math's deterministic sinf_ref / expf_ref / powf_ref, so the
-// image is the same bits on every device and on the CPU checker (which calls the same ones):
+// image is the same bits on every device and on the CPU oracle (which calls the same ones):
 // the procedural noise's fract(sin(.) * 43758.5) magnifies a last-bit difference in sin
 // into a different pattern.
 #pragma once

@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -50,7 +50,7 @@ class SceneView:
                               int(self.debug))
 
     def floats(self) -> np.ndarray:
-        """The 27 floats of the view in itr_scene_view order (the CPU checker's argument)."""
+        """The 27 floats of the view in itr_scene_view order (the CPU oracle's argument)."""
         return np.array(list(self.cam_pos) + list(self.cam_fwd) + list(self.cam_right) + list(self.cam_up) + [self.focal]
                         + list(self.domain) + [self.z_lo, self.z_span, self.up, self.depth_span, self.ve, self.time,
                                                self.rain, self.wet, self.overcast, self.vel_max, self.base],

@@ -1,4 +1,4 @@
-// itr_oracle.hpp — CPU restatement of the reference solver, used ONLY as a checker.
+// itr_oracle.hpp — CPU restatement of the reference solver, test infrastructure only: the results the tests compare with.
 //
 // TEST INFRASTRUCTURE. This header is the parity oracle for the B200 batched forward
 // operator. Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may

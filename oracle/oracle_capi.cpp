@@ -1,7 +1,7 @@
 // oracle_capi.cpp — C entry points over the CPU restatement, for ctypes.
 //
 // TEST INFRASTRUCTURE: loaded only by tests/, __graft_entry__.smoke() and the cpu_baseline
-// leg of bench.py, as the checker. Nothing in the product links this library.
+// leg of bench.py, as the oracle. Nothing in the product links this library.
 //
 // Two ways in:
 //  * scene runs: DEM + walls + Manning + boundary segments (+ a fine-resolution edit) are
@@ -406,7 +406,7 @@ extern "C" void orc_flat_run64(int kernel, int64_t nx, int64_t ny, double dx, do
 }
 
 // The result viewer's map (viewer/viewer.js:72-100, ramps :55-71), restated in f32 as the
-// fragment shader computes it, one pixel per (scale x scale) of a cell: the checker for the
+// fragment shader computes it, one pixel per (scale x scale) of a cell: the oracle for the
 // device image. rgba gets (scale nx) x (scale ny) pixels, row 0 north.
 static float orc_mix(float a, float b, float f) { return a * (1.0f - f) + b * f; }
 static void orc_ramp(const float (*C)[3], int n, float t, float* o) {
@@ -663,7 +663,7 @@ extern "C" void orc_validation(int prec, int id, double* out4) {
 }
 
 
-// The video's ray-marched frame (video/src/shaders/terrain.sksl) restated in f32: the checker
+// The video's ray-marched frame (video/src/shaders/terrain.sksl) restated in f32: the oracle
 // for itr_gpu_render_scene. vf: 27 floats in itr_scene_view order (cam_pos[3], cam_fwd[3],
 // cam_right[3], cam_up[3], focal, domain[3], z_lo, z_span, up, depth_span, ve, time, rain, wet,
 // overcast, vel_max, base); rgba gets width x height pixels, row 0 the top.

@@ -1,5 +1,5 @@
 // scene_oracle.hpp — CPU restatement of the video's height-field ray marcher
-// (video/src/shaders/terrain.sksl), the checker for itr_gpu_render_scene.
+// (video/src/shaders/terrain.sksl), the oracle for itr_gpu_render_scene.
 //
 // TEST INFRASTRUCTURE: included by oracle_capi.cpp only. f32 arithmetic in the shader's
 // operation order, compiled without FMA contraction (oracle/Makefile), with the GLSL

@@ -1,4 +1,4 @@
-"""ctypes wrapper of oracle/liboracle.so — the CPU checker (test infrastructure only).
+"""ctypes wrapper of oracle/liboracle.so — the CPU oracle (test infrastructure only).
 
 Builds the library on first use if it is missing (make -C oracle). Only tests/,
 __graft_entry__.smoke() and bench.py's cpu_baseline leg import this module.
