@@ -127,3 +127,13 @@ def test_polish_incumbent_on_device():
     o64 = orc.flat_run64(base_arrays(base), design_dict(t, p), p, obj.monitors)
     j64 = obj.evaluate(o64["monitor_max"], e.cut_m3, e.fill_m3, baseline)["j"]
     assert abs(j64 - res.j) <= 1e-3 * abs(j64), (j64, res.j)
+
+
+def test_quantize_rounds_half_away_from_zero():
+    """DesignSpace::q (crates/itr-core/src/design.rs:259-261) rounds with Rust's f64::round,
+    half-way cases away from zero (Python's round() would take the even neighbour)."""
+    from itr_gpu.design import quantize
+    assert quantize(0.125, 0.25) == 0.25 and quantize(-0.125, 0.25) == -0.25
+    assert quantize(0.375, 0.25) == 0.5 and quantize(0.625, 0.25) == 0.75
+    assert quantize(2.6, 0.5) == 2.5 and quantize(-2.76, 0.5) == -3.0
+    assert quantize(1.2345, 0.0) == 1.2345
