@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kTileThreads, 6) k_plain_update(const PlainArg
   const int par = cl.par;
   const StepK k = cl.k;
   const bool hits = cl.pl.hits;
-  const double dt_dx = cl.pl.dt * A.P.dx, dt_dy = cl.pl.dt * A.P.dy;
+  const double dt_dy = cl.pl.dt * A.P.dy;
   const int nx = A.nx, ny = A.ny;
   const int gx0 = blockIdx.x * kTile, gy0 = blockIdx.y * kTile;
   const int li = threadIdx.x;
