@@ -10,7 +10,11 @@ storm peaking at 100 mm/h at 20 min, 64 designs of 4 primitives each, run to com
            events on the launching stream, L2 flushed between iterations)
   e2e      the same metric through the public C ABI call (itr_gpu_run_batch) from host
            buffers: packing, host->device copies, kernel, device->host results
-  roofline the batched kernel against the measured HBM copy bandwidth at 32 B/cell-step
+  roofline the batched kernel's bound: instruction issue (its state stays in shared memory,
+           so DRAM carries only the inputs once). achieved = warp-instructions per
+           cell-step (ncu counters of the same kernel, profiles/) x cell-steps/s; peak = SMs x
+           4 schedulers x the median SM clock sampled during the timed region. The 32 B/cell-
+           step HBM model is reported beside it (roofline.hbm).
   cpu_baseline  the f32 CPU port of the reference's fused kernel (oracle/), candidate-parallel
            on the host cores, on a bounded sample of the same workload
 
@@ -97,6 +101,44 @@ class ClockSampler:
                         reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+COUNTERS = os.path.join(ROOT, "profiles", "k_batched_config2_counters.json")
+
+
+def kernel_counters():
+    """ncu counters of the batched kernel on this workload, committed under profiles/:
+    DRAM bytes per launch and warp-instructions issued per cell-step."""
+    try:
+        with open(COUNTERS) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def issue_roofline(cell_steps, avg_ms, counters, clocks, hbm_achieved, hbm_peak, hbm_src):
+    """The batched kernel keeps a design's state in shared memory for the whole storm, so it
+    is bound by instruction issue, not HBM: achieved warp-instructions/s = (warp-instructions
+    per cell-step, from ncu) x cell-steps/s; peak = SMs x 4 schedulers x 1 instruction per
+    clock at the median SM clock of the timed region. The HBM model rides along."""
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    ipc = counters.get("warp_inst_per_cell_step")
+    rate = cell_steps / (avg_ms / 1e3)
+    peak = sms * 4 * mhz * 1e6
+    line = {"bound": "issue", "unit": "warp-instr/s", "peak": peak,
+            "achieved": ipc * rate if ipc else None, "frac": ipc * rate / peak if ipc else None,
+            "traffic": counters.get("dram_bytes_per_launch"),
+            "model": (f"{ipc} warp-instructions per cell-step (ncu, {os.path.relpath(COUNTERS, ROOT)}) x "
+                      f"{rate:.4g} cell-steps/s; peak {sms} SMs x 4 issue slots x {mhz:.0f} MHz"),
+            "sms_used": counters.get("sms_used"),
+            "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_achieved / hbm_peak,
+                    "peak_source": hbm_src,
+                    "model": f"{BYTES_PER_CELL_STEP} B/cell-step x {cell_steps:.4g} cell-steps per launch"}}
+    if ipc and counters.get("sms_used"):
+        line["frac_of_used_sms"] = ipc * rate / (counters["sms_used"] * 4 * mhz * 1e6)
+    return line
 
 
 def dist_setup(n_gpus):
@@ -358,8 +400,9 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="pin the threads per CTA (profiling; 0 = autotune)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the config-4 adjoint summary")
     ap.add_argument("--no-ladder", action="store_true", help="skip the config-3 uneven-batch and stage/inflow summaries")
-    ap.add_argument("--workload", type=int, default=2, choices=[2, 5],
-                    help="2: the bench workload; 5: the 1024x1024 scene (16 designs; measurement / profiling only)")
+    ap.add_argument("--workload", type=int, default=2, choices=[2, 4, 5],
+                    help="2: the bench workload; 4: the 240x192 scene (32 designs); 5: the 1024x1024 scene (16 designs) "
+                         "(4 and 5: measurement / profiling only)")
     ap.add_argument("--impl-path", default="auto", choices=["auto", "tiled", "plain"],
                     help="profiling: run the main workload on the tiled or plain path instead of the autotuned one")
     ap.add_argument("--adjoint-only", action="store_true",
@@ -379,7 +422,7 @@ def main():
         print(json.dumps({"adjoint": adjoint_summary(g, duration=args.duration, which=4 if args.workload == 2 else 5)}))
         g.close()
         return 0
-    sc, terrs = workload(rank, args.designs if args.workload == 2 else 16, args.workload)
+    sc, terrs = workload(rank, {2: args.designs, 4: 32, 5: 16}[args.workload], args.workload)
     if args.duration is not None:
         sc.params.duration_s = float(args.duration)
     g = GpuSolver(local)
@@ -454,15 +497,8 @@ def main():
         per_launch_bytes = cell_steps * BYTES_PER_CELL_STEP
         avg_ms = sum(kern_ms) / len(kern_ms)
         achieved = per_launch_bytes / (avg_ms / 1e3) / 1e9
-        traffic = None
-        tp = os.path.join(ROOT, "profiles", "k_batched_config2_traffic.json")
-        if os.path.exists(tp):
-            try:
-                with open(tp) as f:
-                    tj = json.load(f)
-                traffic = float(tj["dram_bytes_per_launch"])
-            except Exception:
-                traffic = None
+        counters = kernel_counters()
+        clocks = clk.summary()
         # single-GPU only: the other ranks would wait on the closing barrier meanwhile
         plain = None if args.no_plain or world > 1 else plain_comparison(g, sc, terrs)
         adj = None if args.no_adjoint or world > 1 or args.duration is not None else adjoint_summary(g)
@@ -477,10 +513,12 @@ def main():
             "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": k_total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes and designs)",
-            "config": {"workload": ("config2: rolling hills 120x96 @5 m, 60 min storm (100 mm/h peak at 20 min), "
-                                    f"{len(terrs)} designs x 4 primitives per GPU, run to completion") if args.workload == 2 else
-                                   (f"config5: fractal 1024x1024 @2 m, {sc.params.duration_s:.0f} s of the 90 min double-peak storm, "
-                                    f"{len(terrs)} designs x 6 primitives"),
+            "config": {"workload": {2: ("config2: rolling hills 120x96 @5 m, 60 min storm (100 mm/h peak at 20 min), "
+                                        f"{len(terrs)} designs x 4 primitives per GPU, run to completion"),
+                                    4: (f"config4: rolling hills 240x192 @2.5 m, {sc.params.duration_s:.0f} s of the 60 min storm, "
+                                        f"{len(terrs)} designs x 4 primitives"),
+                                    5: (f"config5: fractal 1024x1024 @2 m, {sc.params.duration_s:.0f} s of the 90 min double-peak "
+                                        f"storm, {len(terrs)} designs x 6 primitives")}[args.workload],
                        "path": args.impl_path,
                        "designs_per_gpu": len(terrs), "cells": N, "steps_per_design_mean": sum(steps_per_design) / len(steps_per_design),
                        "parallelism": f"designs sharded over {world} GPU(s), 1 design per thread-block cluster",
@@ -489,9 +527,7 @@ def main():
             "precision": ("device path bit-identical to the f32 CPU port (tests/test_gpu_parity.py); that port's "
                           "per-cell peak depth within 2.0e-6 m of the f64 oracle on config 1, J within 3e-7 "
                           "relative (tests/test_precision.py; bar 1e-4 m)"),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": traffic, "peak_source": src,
-                         "model": f"{BYTES_PER_CELL_STEP} B/cell-step x {cell_steps:.4g} cell-steps per launch"},
+            "roofline": issue_roofline(cell_steps, avg_ms, counters, clocks, achieved, hbm, src),
             "cpu_baseline": cpu,
             "plain": plain,
             "batched_over_plain": (value / world / plain["value"]) if plain else None,
@@ -501,7 +537,7 @@ def main():
             "reference_gpubench": gpb,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "wall_s_timed": t_wall,
         }
         print(json.dumps(line))

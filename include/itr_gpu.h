@@ -388,8 +388,9 @@ int itr_gpu_render_scene(itr_ctx* ctx, const uint8_t* terrain, int32_t tw, int32
  * stalled by the device-wide synchronisation of cudaMalloc/cudaFree, a search loop that
  * must not fail mid-way on an out-of-memory error. It runs the plain path's kernels (same
  * bits as itr_gpu_run_batch) for ONE design on scratch held in a static device array of
- * fixed size, reserved when the library's module loads; the call allocates nothing, on the
- * device or the host. Inputs and results are host buffers with run_batch's meaning;
+ * fixed size. CUDA reserves that array when it loads the library's module on the device;
+ * under CUDA's default lazy loading that is the first call on the device, not the opening
+ * of the library. After that the call allocates nothing, on the device or the host. Inputs and results are host buffers with run_batch's meaning;
  * there is no objective (j = 0, no aborts), and boundaries are walls or transmissive
  * (stage and inflow cells, or inflow_scale other than 1, give ITR_UNSUPPORTED). Runs on
  * the device's legacy default stream and returns when the results are in the host buffers.
@@ -401,9 +402,10 @@ int itr_gpu_render_scene(itr_ctx* ctx, const uint8_t* terrain, int32_t tw, int32
 /* One static array per device, shared by every call, which finds it holding the previous
  * call's contents (the call clears what must start at zero). Calls on the same device that
  * overlap in time (several host threads or streams) race on it and corrupt each other's
- * results. The first call on a device does the set-up: with that device current it looks
- * up the array's device address (cudaGetSymbolAddress) and keeps it; make that first call
- * before any stream capture. */
+ * results. The first call on a device does the set-up: with that device current it loads the
+ * module and looks up the array's device address (cudaGetSymbolAddress) and keeps it; make
+ * that first call before any stream capture and before committing the device's memory to
+ * another pool. Boundaries: walls and transmissive edges only, inflow_scale 1. */
 int itr_gpu_run_plain_static(int device, const itr_params* p, const itr_grid* g, const itr_design* design,
                              const uint32_t* monitors, int32_t n_mon, itr_result* result, char* err, size_t errlen);
 

@@ -12,9 +12,13 @@
 //     on what else happens to be resident.
 // For them, itr_gpu_run_plain_static runs the same kernels as the plain path (k_plain_init,
 // k_plain_update, k_plain_finalize; bit-identical results) on scratch that lives in one
-// file-scope static device array of fixed size, reserved when the library's module is loaded.
-// The entry point calls no allocator (device or host): inputs are copied into the static
-// array, results are copied out of it.
+// file-scope static device array of fixed size. CUDA reserves that array on a device when it
+// loads the library's module there; under CUDA's default lazy module loading that happens at
+// the first use of the module on the device, i.e. inside the first itr_gpu_run_plain_static
+// call (its cudaGetSymbolAddress), not when the library is opened. A caller that commits the
+// device's memory to its own pool therefore makes one call first. After that the entry point
+// calls no allocator (device or host): inputs are copied into the static array, results are
+// copied out of it.
 //
 // Limits (rejected with ITR_INVALID_ARG and a message before any device work):
 //   (nx+1)*(ny+1) <= ITR_STATIC_MAX_POINTS, ceil(nx/16)*ceil(ny/16) <= ITR_STATIC_MAX_TILES,
@@ -22,8 +26,8 @@
 // One static array per device, kept from call to call: each call clears what must start at
 // zero. Calls on the same device that overlap in time (two host threads, or several
 // streams) race on it and corrupt each other's results; callers serialise them. The first
-// call on a device looks up the array's address (see static_scratch) and should come
-// before any stream capture.
+// call on a device loads the module and looks up the array's address (see static_scratch):
+// it should come before any stream capture and before the caller commits the device's memory.
 #pragma once
 
 namespace itr {
@@ -32,6 +36,7 @@ constexpr size_t kStaticPoints = ITR_STATIC_MAX_POINTS;
 constexpr size_t kStaticTiles = ITR_STATIC_MAX_TILES;
 constexpr size_t kStaticMon = ITR_STATIC_MAX_MONITORS;
 constexpr size_t kStaticRows = ITR_STATIC_MAX_LEDGER_ROWS;
+constexpr unsigned long long kStaticMaxSteps = 2000000000ull;   // device step limit (status 4 beyond it)
 
 // Fixed layout of the static array (byte offsets, each 256-aligned). Planes are sized for
 // kStaticPoints entries, which bounds nx*ny, ny*(nx+1) and (ny+1)*nx alike.
@@ -156,10 +161,13 @@ extern "C" int itr_gpu_run_plain_static(int device, const itr_params* p, const i
   if (g->mode != ITR_FACE_SIGNED && g->mode != ITR_FACE_CREST) return static_fail(err, errlen, ITR_INVALID_ARG, "unknown face mode %d", g->mode);
   for (int64_t i = 0; i < 2ll * nx + 2ll * ny; ++i) {
     if (g->bc[i] == ITR_BC_STAGE || g->bc[i] == ITR_BC_INFLOW)
-      return static_fail(err, errlen, ITR_UNSUPPORTED, "Stage and Inflow boundaries are not supported on the GPU backend");
+      return static_fail(err, errlen, ITR_UNSUPPORTED,
+                         "Stage and Inflow boundaries are not supported by itr_gpu_run_plain_static (use itr_gpu_run_batch)");
     if (g->bc[i] > ITR_BC_INFLOW) return static_fail(err, errlen, ITR_INVALID_ARG, "unknown boundary code %d", (int)g->bc[i]);
   }
-  if (p->inflow_scale != 1.0) return static_fail(err, errlen, ITR_UNSUPPORTED, "inflow scaling is not supported on the GPU backend");
+  if (p->inflow_scale != 1.0)
+    return static_fail(err, errlen, ITR_UNSUPPORTED,
+                       "inflow_scale other than 1 is not supported by itr_gpu_run_plain_static (use itr_gpu_run_batch)");
   if (!(p->duration_s >= 0.0) || !(p->sync_interval_s > 0.0) || !(p->cfl > 0.0) || !(p->dt_max_s > 0.0))
     return static_fail(err, errlen, ITR_INVALID_ARG, "duration, sync interval, cfl and dt_max must be positive");
   if (p->n_rain < 0 || p->n_rain > kMaxRain) return static_fail(err, errlen, ITR_INVALID_ARG, "hyetograph has %d points (max %d)", p->n_rain, kMaxRain);
@@ -169,6 +177,14 @@ extern "C" int itr_gpu_run_plain_static(int device, const itr_params* p, const i
   const bool crest = g->mode == ITR_FACE_CREST;
   if (!ds->dzx || !ds->dzy) return static_fail(err, errlen, ITR_INVALID_ARG, "design has no face jumps");
   if (crest && (!ds->dzx2 || !ds->dzy2)) return static_fail(err, errlen, ITR_INVALID_ARG, "crest mode needs dzx2/dzy2");
+  // The same start check as itr_gpu_run_batch: an infinite or absurdly deep start makes the
+  // first CFL dt zero or vanishing, so the run would crawl towards its step limit. NaN and
+  // negative depths are left to the solver's health test (Unhealthy at the first step).
+  if (ds->h0)
+    for (size_t i = 0; i < (size_t)nx * ny; ++i)
+      if (std::isinf(ds->h0[i]) || ds->h0[i] > kMaxInitialDepth)
+        return static_fail(err, errlen, ITR_INVALID_ARG, "initial depth %g at cell %zu is infinite or above %g m",
+                           (double)ds->h0[i], i, (double)kMaxInitialDepth);
 
   // ---- set-up: the static array of this device ----
   DeviceGuard dg;
@@ -236,7 +252,7 @@ extern "C" int itr_gpu_run_plain_static(int device, const itr_params* p, const i
   const int max_rows = res->ledger ? res->max_rows : 0;
   A.ledger = max_rows > 0 ? ledger : nullptr;
   A.max_rows = max_rows;
-  A.max_steps = 2000000000ull;
+  A.max_steps = kStaticMaxSteps;
   k_plain_init<<<1, 1024, 0, st>>>(A);
   k_plain_finalize<<<1, 32, 0, st>>>(A, nb, 1);
   constexpr int kStepsPerPoll = 64;
@@ -245,13 +261,15 @@ extern "C" int itr_gpu_run_plain_static(int device, const itr_params* p, const i
     for (int s = 0; s < kStepsPerPoll; ++s) {
       if (crest) k_plain_update<true><<<grid, kTileThreads, 0, st>>>(A);
       else k_plain_update<false><<<grid, kTileThreads, 0, st>>>(A);
-      k_plain_finalize<<<1, 32, 0, st>>>(A, nb, 0);
+      k_plain_finalize<<<1, kFinThreads, 0, st>>>(A, nb, 0);   // as run_plain_design: same summation order
     }
     SCU(cudaGetLastError());
     SCU(cudaMemcpyAsync(&hc, ctl, sizeof(PlainCtl), cudaMemcpyDeviceToHost, st));
     SCU(cudaStreamSynchronize(st));
     if (hc.done) break;
-    if (polls > 100000000ull) return static_fail(err, errlen, ITR_DEVICE_TIMEOUT, "plain run did not terminate");
+    // the device stops a run at max_steps (status 4), so this bound is never the one that ends it
+    if (polls > kStaticMaxSteps / kStepsPerPoll + 2)
+      return static_fail(err, errlen, ITR_DEVICE_TIMEOUT, "plain run did not terminate");
   }
   if (hc.status >= 4) return static_fail(err, errlen, ITR_DEVICE_TIMEOUT, "run exceeded its step limit (status %d)", hc.status);
 

@@ -74,8 +74,16 @@ def quantize(v: float, step: float) -> float:
 
 
 def round_half_away(x: float) -> float:
-    """Rust f64::round: half-way cases away from zero."""
-    return math.floor(x + 0.5) if x >= 0.0 else -math.floor(-x + 0.5)
+    """Rust f64::round: half-way cases away from zero. Rounds |x| through its exact
+    fractional part (|x| - floor(|x|) is exact in f64), so no x + 0.5 rounding step can
+    carry 0.49999999999999994 up to 1 or an odd integer above 2^52 to the next even one."""
+    if not math.isfinite(x):
+        return x
+    a = abs(x)
+    r = math.floor(a)
+    if a - r >= 0.5:
+        r += 1.0
+    return math.copysign(r, x)
 
 
 def materialize(prims: list[Primitive], geo: GeoTransform, nx: int, ny: int, editable: np.ndarray,

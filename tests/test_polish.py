@@ -137,3 +137,9 @@ def test_quantize_rounds_half_away_from_zero():
     assert quantize(0.375, 0.25) == 0.5 and quantize(0.625, 0.25) == 0.75
     assert quantize(2.6, 0.5) == 2.5 and quantize(-2.76, 0.5) == -3.0
     assert quantize(1.2345, 0.0) == 1.2345
+    from itr_gpu.design import round_half_away
+    # x + 0.5 would round these wrongly: 0.49999999999999994 + 0.5 rounds to 1.0, and an odd
+    # integer above 2^52 plus 0.5 rounds to the even neighbour
+    assert round_half_away(0.49999999999999994) == 0.0 and round_half_away(-0.49999999999999994) == 0.0
+    assert round_half_away(2.0 ** 52 + 1) == 2.0 ** 52 + 1 and round_half_away(-(2.0 ** 52 + 1)) == -(2.0 ** 52 + 1)
+    assert round_half_away(0.5) == 1.0 and round_half_away(-0.5) == -1.0 and round_half_away(-2.5) == -3.0

@@ -3,10 +3,13 @@
 Two consecutive calls must each reproduce the context entry point (itr_gpu_run_batch) bit
 for bit on the same design: everything, ledger included, against its plain path (the same
 kernels), and the state (depth, peaks, monitor maxima, steps) against its default batched
-path. The second call checks that nothing of the first survives in the static scratch.
-The size limit is checked on the host, before any device work. The entry point exists for
-callers that cannot allocate device memory when they run a design (a device committed to
-their own pool, other streams that cudaMalloc's device-wide synchronisation would stall).
+path and against the f32 oracle. The second call checks that nothing of the first survives
+in the static scratch, and that it takes no device memory: the device's free memory
+(cudaMemGetInfo) is the same before and after it. A grid of more than 32 tiles checks the
+ledger's summation order against the context path. The size limit and the start check are
+on the host, before any device work. The entry point exists for callers that cannot
+allocate device memory when they run a design (a device committed to their own pool,
+other streams that cudaMalloc's device-wide synchronisation would stall).
 This file sorts last so that it also runs after every other GPU test in one process.
 """
 from __future__ import annotations
@@ -16,7 +19,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from helpers import assert_bitwise
+import oracle_ref as orc
+from helpers import assert_bitwise, base_arrays, design_dict
 from itr_gpu import GpuSolver, _lib
 from itr_gpu.scenes import valley_scene
 
@@ -90,10 +94,32 @@ def test_oversize_grid_rejected_before_device_work():
     assert "600x600" in err and "static scratch" in err, err
 
 
+def test_infinite_initial_depth_rejected_before_device_work():
+    """An infinite or absurd start depth would make the first dt vanish and the run crawl
+    to its step limit: refused on the host like itr_gpu_run_batch refuses it."""
+    lib = _lib.load()
+    sc = valley_scene(10.0)
+    t = [t for _, _, t in sc.designs(1)][0]
+    h0 = np.zeros((sc.base.ny, sc.base.nx), np.float32)
+    for bad in (np.inf, 2e4):
+        h0[3, 4] = bad
+        rc, err, _, _ = static_call(lib, 0, sc.params, t.base, t, h0, sc.monitors)
+        assert rc == _lib.ITR_INVALID_ARG, (bad, rc, err)
+        assert "initial depth" in err, err
+
+
+def _free_bytes():
+    import torch
+    torch.cuda.synchronize(0)
+    return torch.cuda.mem_get_info(0)[0]
+
+
 @pytest.mark.gpu
-def test_static_entry_matches_run_batch_twice():
-    sc = valley_scene(10.0)   # 45 x 35, rain, transmissive outlet
-    sc.params.duration_s = 900.0
+@pytest.mark.parametrize("cell,duration", [(10.0, 900.0), (4.0, 600.0)])
+def test_static_entry_matches_run_batch_twice(cell, duration):
+    """45 x 35 (9 tiles) and 112 x 88 (42 tiles, more than one finalize warp's 32)."""
+    sc = valley_scene(cell)   # rain, transmissive outlet
+    sc.params.duration_s = duration
     terrs = [t for _, _, t in sc.designs(2)]
     g = GpuSolver(0)
     try:
@@ -103,13 +129,19 @@ def test_static_entry_matches_run_batch_twice():
     finally:
         g.close()
     lib = _lib.load()
+    orcs = [orc.flat_run(base_arrays(sc.base), design_dict(t, sc.params), sc.params, sc.monitors, want_peak=True)
+            for t in terrs]
     # two consecutive calls per design, designs alternating: each must equal run_batch
     for call in range(2):
-        for t, r, rb in zip(terrs, plain, batched):
+        for t, r, rb, o in zip(terrs, plain, batched, orcs):
             p = sc.params   # h0 as run_batch passes it: explicit only for an initial stage
             h0 = t.initial_depth(p.initial_depth, p.initial_stage) if p.initial_stage is not None else None
+            free0 = _free_bytes()
             rc, err, R, out = static_call(lib, 0, sc.params, t.base, t, h0, sc.monitors, ledger_rows=64)
+            free1 = _free_bytes()
             assert rc == _lib.ITR_OK, err
+            if call == 1:   # the first call may load the module (and with it the static array)
+                assert free1 == free0, f"the call changed free device memory by {free0 - free1} bytes"
             what = f"static call {call}"
             assert R.steps == r.steps, f"{what}: steps {R.steps} vs {r.steps}"
             assert R.t_end == r.t_end and R.sync_count == r.sync_count and R.status == r.status, what
@@ -124,3 +156,7 @@ def test_static_entry_matches_run_batch_twice():
             assert_bitwise(out["depth"], rb.depth, f"{what}: final depth vs batched")
             assert_bitwise(out["peak"], rb.peak, f"{what}: per-cell peak vs batched")
             np.testing.assert_array_equal(out["monitor_max"], rb.monitor_max, err_msg=f"{what}: monitor maxima vs batched")
+            assert R.steps == o["steps"] and R.t_end == o["t_end"], f"{what}: vs oracle"
+            assert_bitwise(out["depth"], o["h"], f"{what}: final depth vs oracle")
+            assert_bitwise(out["peak"], o["peak"], f"{what}: per-cell peak vs oracle")
+            np.testing.assert_array_equal(out["monitor_max"], o["monitor_max"], err_msg=f"{what}: monitor maxima vs oracle")
