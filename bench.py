@@ -236,7 +236,7 @@ def plain_comparison(g, sc, terrs, n_sample=2):
             "launches": tm["launches"], "kernel_ms": tm["kernel_ms"]}
 
 
-def adjoint_summary(g, K=128, duration=None, which=4):
+def adjoint_summary(g, K=128, duration=None, which=4, sweep=()):
     """Config 4 (rolling hills 240x192 @2.5 m, 60 min storm, 32 designs x 4 primitives), or
     config 5 (fractal 1024x1024 @2 m, 90 min storm, 16 designs x 6 primitives, K = 256): the
     batched forward against itr_gpu_vjp (taped forward + checkpointed backward), device time."""
@@ -251,17 +251,52 @@ def adjoint_summary(g, K=128, duration=None, which=4):
     g.run_batch(sc.params, terrs, sc.monitors, objective=sc.objective, want_depth=False)   # autotune
     g.rerun_resident()
     fwd = g.last_timing()["kernel_ms"]
-    # the first call sizes the context's checkpoint and tape buffers; a search loop reuses them
-    g.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=K)
-    runs = g.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=K)
-    v = g.last_vjp_timing()
-    cs = float(sum(r.steps for r in runs)) * sc.base.nx * sc.base.ny
+    N = sc.base.nx * sc.base.ny
+
+    def one(k):
+        # the first call sizes the context's checkpoint and tape buffers; a search loop reuses them
+        g.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=k)
+        runs = g.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=k)
+        v = g.last_vjp_timing()
+        steps = max(r.steps for r in runs)
+        # device memory of the adjoint: a checkpoint of (h, qx, qy) per design every k steps and
+        # two tapes of k states (replay of one segment beside the backward of the next)
+        ck = -(-steps // k) * n * 12 * N
+        tape = 2 * k * n * 12 * N
+        return runs, {"checkpoint_interval": k, "vjp_taped_forward_ms": v["forward_ms"], "vjp_backward_ms": v["backward_ms"],
+                      "adjoint_over_forward": (v["forward_ms"] + v["backward_ms"]) / fwd,
+                      "checkpoint_bytes": ck, "tape_bytes": tape}
+    runs, main = one(K)
+    cs = float(sum(r.steps for r in runs)) * N
     label = ("config4 rolling hills 240x192 @2.5 m" if which == 4 else "config5 fractal 1024x1024 @2 m")
-    return {"workload": f"{label}, {sc.params.duration_s:.0f} s storm, {n} designs x {sc.n_prims} primitives",
-            "forward_ms": fwd, "forward_cell_steps_per_s": cs / (fwd / 1e3), "checkpoint_interval": K,
-            "vjp_taped_forward_ms": v["forward_ms"], "vjp_backward_ms": v["backward_ms"],
-            "adjoint_over_forward": (v["forward_ms"] + v["backward_ms"]) / fwd,
-            "gradient": "dJ/d(face jump), f32 discrete adjoint with frozen dt; 0.1% vs f64 central differences (tests/test_adjoint.py)"}
+    out = {"workload": f"{label}, {sc.params.duration_s:.0f} s storm, {n} designs x {sc.n_prims} primitives",
+           "forward_ms": fwd, "forward_cell_steps_per_s": cs / (fwd / 1e3), **main,
+           "gradient": ("dJ/d(face jump), f32 discrete adjoint with frozen dt; within 1% of f64 central differences on "
+                        "config 4's grid, smooth sub-case (tests/test_adjoint.py)")}
+    if sweep:
+        out["interval_sweep"] = [one(k)[1] for k in sweep]
+    return out
+
+
+def polish_summary(g, duration=900.0, n_pop=16, iters=4):
+    """Config 5's search use of the adjoint (fractal 1024x1024 @2 m, the first `duration` s of
+    its double-peak storm): a generation of 16 seeded designs of 6 primitives evaluated on the
+    device, its best feasible design (the incumbent) polished with itr_gpu_vjp_primitives
+    gradients in a trust region, each proposal re-evaluated exactly with itr_gpu_run_primitives
+    (guard against the unedited baseline, volume limit). The f32 and f64 oracle reruns of the
+    polished incumbent are in tests/test_polish.py (about 2 CPU-minutes each)."""
+    from itr_gpu.polish import polish_population
+    from itr_gpu.scenes import config
+    sc = config(5)
+    sc.params.duration_s = float(duration)
+    designs = sc.primitive_designs(n_pop)
+    r = polish_population(g, sc.params, sc.base, designs, sc.objective, sc.editable, sc.max_abs_dz, max_volume=sc.max_volume,
+                          iters=iters)
+    res = r.result
+    return {"workload": f"config5 fractal 1024x1024 @2 m, first {duration:.0f} s of the storm, {n_pop} designs x 6 primitives",
+            "population_feasible": r.feasible, "j_incumbent": res.j_start, "j_polished": res.j, "delta_j": res.j - res.j_start,
+            "feasible": res.feasible, "accepted": res.accepted, "exact_evaluations": res.evaluations,
+            "history": res.history, "wall_s": r.wall_s}
 
 
 def ladder_summary(g):
@@ -310,6 +345,34 @@ def boundary_summary(g):
         out[name] = {"ms": t["kernel_ms"], "cell_steps_per_s": cs / (t["kernel_ms"] / 1e3),
                      "steps_per_design_mean": sum(r.steps for r in runs) / len(runs)}
     out["workload"] = "valley 90x70 @5 m, 2400 s storm, 64 designs x 2 primitives, batched path"
+    return out
+
+
+def dry_rows_summary(g):
+    """Dry-row skipping (kernel.rs:605-612) where it pays: the inflow-driven valley (90x70 @5 m,
+    inflow hydrographs on the west and south edges, stage on the east and north) with no rain,
+    the flood entering from the edges over 40 min, 64 designs on the batched path, once with
+    params.skip_dry on and once off (the same bits either way). Rows are skipped while their
+    neighbourhood is still dry; cell-steps/s counts the cells actually advanced."""
+    from itr_gpu import Hyetograph
+    from itr_gpu.scenes import inflow_valley_scene
+    sc = inflow_valley_scene(5.0)
+    sc.params.rain = Hyetograph.from_mm_h([(0, 0), (2400, 0)])
+    ts = [t for _, _, t in sc.designs(64)]
+    N = sc.base.nx * sc.base.ny
+    out = {"workload": "inflow valley 90x70 @5 m, no rain, 2400 s of inflow, 64 designs x 2 primitives, batched path"}
+    for skip in (True, False):
+        sc.params.skip_dry = skip
+        g.run_batch(sc.params, ts, sc.monitors, want_depth=False)
+        runs = g.run_batch(sc.params, ts, sc.monitors, want_depth=False)
+        ms = g.last_timing()["kernel_ms"]
+        steps = sum(r.steps for r in runs)
+        skipped = sum(r.rows_skipped for r in runs)
+        out["skip_on" if skip else "skip_off"] = {
+            "ms": ms, "rows_skipped_fraction": skipped * sc.base.nx / max(steps * N, 1),
+            "cell_steps_advanced_per_s": sum(r.cell_updates for r in runs) / (ms / 1e3),
+            "steps_x_cells_per_s": steps * N / (ms / 1e3)}
+    out["speedup"] = out["skip_off"]["ms"] / out["skip_on"]["ms"]
     return out
 
 
@@ -501,10 +564,13 @@ def main():
         clocks = clk.summary()
         # single-GPU only: the other ranks would wait on the closing barrier meanwhile
         plain = None if args.no_plain or world > 1 else plain_comparison(g, sc, terrs)
-        adj = None if args.no_adjoint or world > 1 or args.duration is not None else adjoint_summary(g)
+        adj = None if args.no_adjoint or world > 1 or args.duration is not None else guarded(adjoint_summary, g, 128, None, 4,
+                                                                                              (32, 512))
         lad = None if args.no_ladder or world > 1 or args.duration is not None else ladder_summary(g)
         bnd = None if args.no_ladder or world > 1 or args.duration is not None else boundary_summary(g)
         gpb = None if args.no_ladder or world > 1 or args.duration is not None else guarded(gpubench_summary, g)
+        pol = None if args.no_adjoint or world > 1 or args.duration is not None else guarded(polish_summary, g)
+        dry = None if args.no_ladder or world > 1 or args.duration is not None else guarded(dry_rows_summary, g)
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(sc, terrs)
@@ -535,6 +601,8 @@ def main():
             "ladder": lad,
             "boundaries": bnd,
             "reference_gpubench": gpb,
+            "polish": pol,
+            "dry_rows": dry,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
             "clocks": clocks,

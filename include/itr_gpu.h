@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define ITR_GPU_ABI_VERSION 3
+#define ITR_GPU_ABI_VERSION 4
 
 typedef struct itr_ctx itr_ctx;
 
@@ -67,7 +67,9 @@ typedef struct itr_params {
   int32_t n_rain;
   double infil_capacity;    /* constant infiltration capacity [m/s]                      */
   double initial_depth;     /* used for designs whose h0 is NULL (init_state, solver.rs:287) */
-  int32_t skip_dry;         /* dry-row skipping; bitwise-neutral (kernel.rs:605-612)     */
+  int32_t skip_dry;         /* dry-row skipping (kernel.rs:605-612): with no rain in a step, a row
+                               between dry rows (and dry ghosts) is not computed; results are
+                               the same bits. Done by the cluster kernel and the tiled path   */
   double inflow_scale;      /* factor on every inflow hydrograph (1.0 = as given)        */
 } itr_params;
 
@@ -148,7 +150,7 @@ typedef struct itr_result {
   int32_t max_rows;
   /* written by the library: */
   uint64_t steps;
-  uint64_t cell_updates;    /* steps * nx * ny (gpubench.rs:28) */
+  uint64_t cell_updates;    /* cells advanced: steps * nx * ny (gpubench.rs:28) less skipped dry rows */
   double t_end;
   uint32_t sync_count;
   int32_t status;           /* itr_run_status */
@@ -164,6 +166,9 @@ typedef struct itr_result {
   uint64_t warm_start_steps;/* steps taken over from the baseline record (RunSummary::warm_start_steps) */
   double dt_fallback_t;     /* locked dt: time of the sync snapshot the run fell back to, -1 if it
                                kept the schedule or ran adaptively (RunSummary::dt_fallback_t) */
+  uint64_t rows_skipped;    /* dry rows skipped (params.skip_dry; RunSummary::rows_skipped): rows
+                               that, with no rain in a step, lay between dry rows; their cells
+                               are left out of cell_updates = steps * nx * ny - rows_skipped * nx */
 } itr_result;
 
 /* GpuSolver::new (lib.rs:85). device < 0 selects the current device. Returns NULL on
@@ -199,6 +204,13 @@ int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int3
  *   "exact_special"     1 = the batched kernel computes every reciprocal and square root
  *                       with the IEEE-exact library routines instead of its own branch-free
  *                       ones (identical results; for checking, default 0)
+ *   "band"     tiled path update kernel: 1 = row-band sweep (default), 0 = 16x16 tiles with a
+ *              halo (identical results; for comparison)
+ *   "wait_limit"        try_wait rounds of the batched kernel's barrier wait in single-CTA
+ *                       designs before the run gives up with ITR_DEVICE_TIMEOUT (default 2^22)
+ *   "stall_wait_test"   1 = that barrier expects one arrival more than the CTA makes, so every
+ *                       such wait runs to its limit and the call returns ITR_DEVICE_TIMEOUT with
+ *                       the context still usable (test of the timeout path; default 0)
  * Returns ITR_INVALID_ARG for an unknown key. */
 int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value);
 
@@ -331,9 +343,11 @@ int itr_gpu_run_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g,
  * length) of every primitive, dj_dprim[3 * (k - prim_off[0]) + {0, 1, 2}] for primitive
  * prims[k], at fixed quantised centre and angle. The device runs itr_gpu_vjp's forward and backward on
  * the materialised designs, forms dJ/d(dz) per cell from the face-jump gradients, and
- * contracts it with central differences of the f64 materialisation (steps 1e-4 m in height,
- * 1e-3 m in width and length: the profile is linear in height and C1 in width and length),
- * adding the earthwork term's derivative earth_weight (cut_cost dV_cut + fill_cost dV_fill).
+ * contracts it with the derivative of the materialisation written out from the profile
+ * (Primitive::profile, design.rs:107-134: the (1 - s^2)^2 ridge and the flat-bottomed cut,
+ * differentiated through the distance to the segment and the half width, summed over the 4x4
+ * quadrature; cells clamped to +-max_abs_dz contribute nothing), adding the earthwork term's
+ * derivative earth_weight (cut_cost dV_cut + fill_cost dV_fill).
  * dj_ddzx / dj_ddzy (may be NULL) receive the face-jump gradients as itr_gpu_vjp gives them. */
 int itr_gpu_vjp_primitives(itr_ctx* ctx, const itr_params* p, const itr_grid* g, const itr_design_space* space,
                            int32_t n_designs, const int32_t* prim_off, const itr_primitive* prims,

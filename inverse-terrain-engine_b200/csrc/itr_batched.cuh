@@ -78,6 +78,8 @@ struct BatchArgs {
   DesignOut* out;     // n_designs
   unsigned long long max_steps;
   unsigned exact;     // 1: every paired reciprocal through the IEEE routine (checking)
+  unsigned wait_limit;   // try_wait rounds of a single-CTA design's barrier wait before status 5
+  unsigned stall_test;   // 1: that barrier expects one arrival more than the CTA makes (timeout test)
   const WarmStart* warm;   // optional, per design (state NULL: cold start)
   // Baseline-locked dt (SolverParams::locked_dt / cfl_hard, solver.rs:42-46); read only by the
   // LOCKED instantiation, which is launched when locked_dt is set.
@@ -98,14 +100,15 @@ ITR_DEV unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_sh
 // Shared-memory plan of one CTA. Every CTA of a cluster uses the plan of the largest band,
 // so an offset names the same array in every CTA (DSMEM maps local pointers to peers).
 struct SmemPlan {
-  size_t s4, s2, pk, bf, xb, bx, by, wsum, led, slot, red, mbar, inf, pf, total;
+  size_t s4, s2, pk, bf, xb, bx, by, wsum, led, slot, red, mbar, inf, pf, wf, gwf, nsk, total;
 };
 
 // Values staged per thread and row by the prefetch ring: south y-face jump, next row's
 // x-face jump, wet, g n^2 (+ the second jumps in crest mode).
 __host__ __device__ inline int prefetch_k(int crest) { return crest ? 6 : 4; }
 
-__host__ __device__ inline SmemPlan smem_plan(int nr_max, int nx, int S, int W, int nwarps, int crest = 0, int bnd = 0) {
+__host__ __device__ inline SmemPlan smem_plan(int nr_max, int nx, int S, int W, int nwarps, int crest = 0, int bnd = 0,
+                                               int ny = 0) {
   SmemPlan p;
   size_t n = (size_t)nr_max * nx, o = 0;
   p.s4 = o;   o += n * 16;                         // float4 h, qx, qy, u
@@ -127,12 +130,17 @@ __host__ __device__ inline SmemPlan smem_plan(int nr_max, int nx, int S, int W, 
   p.inf = o;  o += bnd ? (size_t)2 * kMaxInflow * 8 : 0;   // float2 inflow values [2 parity][groups]
   o = align_up(o, 16);
   p.pf = o;   o += (size_t)2 * S * prefetch_k(crest) * 64 * W * 4;   // [2 slot][S][K][64W] floats
+  p.wf = o;   o += (size_t)2 * nr_max * W;           // row wetness bytes [2 parity][nr_max][W]
+  p.gwf = o;  o += bnd ? (size_t)2 * (ny + 2) : 0;    // ghost wetness [2 parity][ny + 2 padded rows]
+  o = align_up(o, 8);
+  p.nsk = o;  o += 8;                                 // rows skipped by this CTA
   p.total = align_up(o, 16);
   return p;
 }
 
-__host__ __device__ inline size_t batched_smem_bytes(int nr_max, int nx, int S, int W, int nwarps, int crest = 0, int bnd = 0) {
-  return smem_plan(nr_max, nx, S, W, nwarps, crest, bnd).total;
+__host__ __device__ inline size_t batched_smem_bytes(int nr_max, int nx, int S, int W, int nwarps, int crest = 0, int bnd = 0,
+                                                     int ny = 0) {
+  return smem_plan(nr_max, nx, S, W, nwarps, crest, bnd, ny).total;
 }
 
 // 4-byte asynchronous global->shared copy (cp.async, cached in L1), commit and wait.
@@ -155,9 +163,10 @@ ITR_DEV void mbar_init(unsigned long long* bar, unsigned count) {
 ITR_DEV void mbar_arrive(unsigned long long* bar) {
   asm volatile("{ .reg .b64 st; mbarrier.arrive.release.cta.shared::cta.b64 st, [%0]; }" ::"r"(smem_u32(bar)) : "memory");
 }
-// Bounded wait on phase `parity`; returns false if the bound ran out.
-ITR_DEV bool mbar_wait(unsigned long long* bar, unsigned parity) {
-  for (unsigned it = 0; it < (1u << 28); ++it) {
+// Bounded wait on phase `parity`: at most `limit` try_wait rounds; returns false if the
+// bound ran out.
+ITR_DEV bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned limit) {
+  for (unsigned it = 0; it < limit; ++it) {
     unsigned ok;
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -206,6 +215,9 @@ struct Smem {
   unsigned long long* mbar;
   float2* INF;     // inflow group values [2 parity][kMaxInflow] (stage/inflow grids only)
   float* PF;       // prefetch ring, [2 slot][S][K][64W]
+  uint8_t* WF;     // [2 parity][nr_max][W]: the warp's columns of the row held water (state of that parity)
+  uint8_t* GWF;    // [2 parity][ny + 2]: a stage / inflow ghost of padded row j holds water (BND)
+  unsigned long long* NSK;
   int ncell, nbf, nxb;
 };
 
@@ -307,13 +319,14 @@ template <bool CLUSTERED>
 struct GroupSync {
   unsigned long long* mbar;
   unsigned phase;
+  unsigned limit;
   bool timed_out;
   ITR_DEV void b1_arrive() {
     if (CLUSTERED) cluster_arrive(); else mbar_arrive(mbar);
   }
   ITR_DEV void b1_wait() {
     if (CLUSTERED) cluster_wait();
-    else { if (!mbar_wait(mbar, phase & 1u)) timed_out = true; }
+    else { if (!mbar_wait(mbar, phase & 1u, limit)) timed_out = true; }
   }
   ITR_DEV void b1_done() { phase += 1; }
   ITR_DEV void full() {
@@ -381,6 +394,19 @@ ITR_DEV void locked_save(const BatchArgs& A, const Smem& sm, size_t base, int nc
   __syncthreads();
 }
 
+// Row wetness flags of the CTA's rows from the state in shared memory (init_state's rule: a
+// row is dry when every depth is 0), into parity slot `par`: warp-strided rows, entry 0 of a
+// row holds the flag, the other W - 1 entries are cleared.
+ITR_DEV void row_flags(const Smem& sm, int par, int nr, int nr_max, int nx, int W, int wid, int nwarps, int lane) {
+  for (int lr = wid; lr < nr; lr += nwarps) {
+    bool w = false;
+    for (int c = lane; c < nx; c += 32) w = w || sm.S4[lr * nx + c].x != 0.0f;
+    w = __any_sync(0xffffffffu, w);
+    uint8_t* e = sm.WF + ((size_t)par * nr_max + lr) * W;
+    for (int k = lane; k < W; k += 32) e[k] = (k == 0 && w) ? 1 : 0;
+  }
+}
+
 template <bool CREST, bool CLUSTERED, int MAXT, bool BND, bool LOCKED = false>
 __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -407,7 +433,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
 
   Smem sm;
   {
-    const SmemPlan pl = smem_plan(nr_max, nx, S, W, nwarps, CREST ? 1 : 0, BND ? 1 : 0);
+    const SmemPlan pl = smem_plan(nr_max, nx, S, W, nwarps, CREST ? 1 : 0, BND ? 1 : 0, ny);
     sm.S4 = reinterpret_cast<float4*>(smem_raw + pl.s4);
     sm.S2 = reinterpret_cast<float2*>(smem_raw + pl.s2);
     sm.PK = reinterpret_cast<float*>(smem_raw + pl.pk);
@@ -422,6 +448,9 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     sm.mbar = reinterpret_cast<unsigned long long*>(smem_raw + pl.mbar);
     sm.INF = reinterpret_cast<float2*>(smem_raw + pl.inf);
     sm.PF = reinterpret_cast<float*>(smem_raw + pl.pf);
+    sm.WF = reinterpret_cast<uint8_t*>(smem_raw + pl.wf);
+    sm.GWF = reinterpret_cast<uint8_t*>(smem_raw + pl.gwf);
+    sm.NSK = reinterpret_cast<unsigned long long*>(smem_raw + pl.nsk);
     sm.ncell = nr_max * nx; sm.nbf = (S + 1) * nx; sm.nxb = 2 * S * W * 2;
   }
   const RunParams& P = A.P;
@@ -507,10 +536,16 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   // that carry no cell compute on zeros (finite operands, no needless reciprocal fallbacks)
   for (int i = tid; i < 2 * S * K * vlanes; i += blockDim.x) sm.PF[i] = 0.0f;
   if (tid < 8) { sm.slot[tid] = 0u; sm.LED[tid] = 0.0; }
+  if (tid == 0) *sm.NSK = 0ull;
   if (WS && q == 0 && tid == 0) { sm.LED[0] = WS->tot_infil; sm.LED[1] = WS->tot_fix; sm.LED[2] = WS->tot_in; sm.LED[3] = WS->tot_out; }
-  if (tid == 0) mbar_init(sm.mbar, blockDim.x);
-  // inflow ghosts of step 0 (at t = 0); each later step's are written one step ahead
-  if (BND && wid == nwarps - 1 && lane < P.inflow.n) sm.INF[lane] = inflow_values(P.inflow, lane, t_start, P.g);
+  if (tid == 0) mbar_init(sm.mbar, blockDim.x + (A.stall_test ? 1u : 0u));
+  // inflow ghosts of step 0 (at t = 0), and the ghost wetness the dry-row test reads; each
+  // later step's are written one step ahead
+  if (BND && wid == nwarps - 1) {
+    if (lane < P.inflow.n) sm.INF[lane] = inflow_values(P.inflow, lane, t_start, P.g);
+    __syncwarp();
+    ghost_row_wet(A.bc, nx, ny, bh, sm.INF, sm.GWF, lane);
+  }
   {
     double sw = s0_l;
 #pragma unroll
@@ -519,6 +554,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     if (lane == 0) { sm.red[wid * 8 + 0] = sw; sm.red[wid * 8 + 1] = vw; }
   }
   if (CLUSTERED) { cluster_arrive(); cluster_wait(); } else __syncthreads();
+  row_flags(sm, 0, nr, nr_max, nx, W, wid, nwarps, lane);   // wetness of the initial state (parity 0)
   double s0 = 0.0, v0 = 0.0;
   for (int qq = 0; qq < C; ++qq) {
     const double* rr = CLUSTERED ? remote(sm.red, qq) : sm.red;
@@ -539,7 +575,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   double violation = 0.0, lower_bound = 0.0, volume = WS ? WS->volume : v0, rel_res = WS ? WS->rel_res : 0.0;
   int n_rows = WS ? WS->n_rows : 0;
   GroupSync<CLUSTERED> gs;
-  gs.mbar = sm.mbar; gs.phase = 0; gs.timed_out = false;
+  gs.mbar = sm.mbar; gs.phase = 0; gs.limit = A.wait_limit; gs.timed_out = false;
   const float heps2 = P.heps2_f;
   RainCursor rcur;
   rcur.seg = 0; rcur.brk = 0;
@@ -611,8 +647,13 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
           step = o.step; sync_index = o.sync_index; n_rows = o.n_rows;
           if (tid < 4) { sm.LED[tid] = o.led[tid]; sm.slot[tid] = 0u; }
           rcur.seg = 0; rcur.brk = 0;
-          if (BND && wid == nwarps - 1 && lane < P.inflow.n)
-            sm.INF[(int)(step & 1ull) * kMaxInflow + lane] = inflow_values(P.inflow, lane, t, P.g);
+          if (BND && wid == nwarps - 1) {
+            if (lane < P.inflow.n) sm.INF[(int)(step & 1ull) * kMaxInflow + lane] = inflow_values(P.inflow, lane, t, P.g);
+            __syncwarp();
+            ghost_row_wet(A.bc, nx, ny, bh, sm.INF + (int)(step & 1ull) * kMaxInflow, sm.GWF + (int)(step & 1ull) * (ny + 2), lane);
+          }
+          __syncthreads();   // the restored rows complete before their flags are taken
+          row_flags(sm, (int)(step & 1ull), nr, nr_max, nx, W, wid, nwarps, lane);
           if (q == 0 && tid == 0) A.fallback_t[d] = t;
           locked_live = false;
           gs.full();   // the restored state of every CTA visible before the next step
@@ -628,7 +669,11 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       inf_cur = sm.INF + sp * kMaxInflow;
       // the next step's inflow ghosts, at its start time (slot read after this step's
       // closing barrier; the other slot's readers finished before the previous one)
-      if (wid == nwarps - 1 && lane < P.inflow.n) sm.INF[(sp ^ 1) * kMaxInflow + lane] = inflow_values(P.inflow, lane, pl.t_new, P.g);
+      if (wid == nwarps - 1) {
+        if (lane < P.inflow.n) sm.INF[(sp ^ 1) * kMaxInflow + lane] = inflow_values(P.inflow, lane, pl.t_new, P.g);
+        __syncwarp();
+        ghost_row_wet(A.bc, nx, ny, bh, sm.INF + (sp ^ 1) * kMaxInflow, sm.GWF + (sp ^ 1) * (ny + 2), lane);
+      }
     }
     float smax_l = 0.0f, infil_l = 0.0f, fix_l = 0.0f;
     bool bad_l = false;
@@ -683,12 +728,43 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     if (in_strip) { if (W > 1) named_bar(1 + s, 32 * W); else __syncwarp(); }
     gs.b1_arrive();
 
+    // ---- dry-row skipping (kernel.rs:605-612) ----
+    // With no rain this step, grid row r is skipped when rows r - 1, r, r + 1 held no water in
+    // the old state (flags of parity sp, written during the previous step; the rows beside the
+    // CTA's band through DSMEM) and no stage or inflow ghost of theirs holds water. Its faces
+    // are exactly 0 and its cells keep their zero state: skipping changes no result. The
+    // decision depends only on shared flags, so every warp of a strip takes it alike.
+    const bool try_skip = P.skip_dry && !(k.rain > 0.0f);
+    auto row_dry = [&](int j) -> bool {   // grid row j in [-1, ny]
+      bool dr = !BND || sm.GWF[sp * (ny + 2) + j + 1] == 0;
+      if (j < 0 || j >= ny) return dr;
+      const uint8_t* wf = sm.WF;
+      int lj = j - ra;
+      if (CLUSTERED && (j < ra || j >= rb)) {
+        const int qq = j < ra ? q - 1 : q + 1;
+        wf = remote(sm.WF, qq);
+        lj = j - (int)((long long)qq * ny / C);
+      }
+      const uint8_t* e = wf + ((size_t)sp * nr_max + lj) * W;
+      for (int w = 0; w < W; ++w) dr = dr && e[w] == 0;
+      return dr;
+    };
+    bool d_m1 = false, d_0 = false, d_1 = false;
+    if (try_skip && L > 0) { d_m1 = row_dry(r0 - 1); d_0 = row_dry(r0); d_1 = row_dry(r0 + 1); }
+
     // ---- row sweep ----
 #pragma unroll 1
     for (int p = 0; p < L; ++p) {
       const int r = r0 + p;
       const int lr = lr0 + p;
       const bool last = (p == L - 1);
+      bool skip = false, skip_next = false;
+      if (try_skip) {
+        const bool d_2 = !last && row_dry(r + 2);
+        skip = d_m1 && d_0 && d_1;
+        skip_next = !last && d_0 && d_1 && d_2;
+        d_m1 = d_0; d_0 = d_1; d_1 = d_2;
+      }
       if (last) gs.b1_wait();
       if (!last) prefetch_row(r + 1, (p + 1) & 1);
       cp_async_commit();
@@ -701,8 +777,31 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       const float2 gn2_r = make_float2(pfv[3 * vlanes], pfv1[3 * vlanes]);
       const float2 d_s2 = CREST ? make_float2(pfv[4 * vlanes], pfv1[4 * vlanes]) : f2(0.0f);
       const float2 d_xn2 = CREST ? make_float2(pfv[5 * vlanes], pfv1[5 * vlanes]) : f2(0.0f);
+      const bool bottom = last && s + 1 >= S && q + 1 >= C;
       Cell2 nxt{};
       Face2 fS{}, fWn{};
+      if (skip) {   // a dry row between dry rows: zero faces, nothing to update
+        if (!last && !skip_next) {   // the next row's west faces
+          nxt = load_pair(lr + 1, r + 1);
+          const Cell2 left = left_pair(nxt, lr + 1, r + 1);
+          fWn = face2<true, CREST>(left.h, left.u, left.v, left.c, nxt.h, nxt.u, nxt.v, nxt.c, d_xn, d_xn2, k);
+          if (lane == 0) {
+            sm.XB[CK((((par ^ 1) * S + s) * W + wis) * 2 + 0, sm.nxb, 9)] = f4(fx_(fWn));
+            sm.XB[CK((((par ^ 1) * S + s) * W + wis) * 2 + 1, sm.nxb, 9)] = f4(fy_(fWn));
+          }
+        }
+        if (bottom) {
+          if (cell0) sm.BY[(sp * 2 + 1) * nx + col0] = 0.0f;
+          if (cell1) sm.BY[(sp * 2 + 1) * nx + col1] = 0.0f;
+        }
+        if (in_strip && col0 == 0) sm.BX[(sp * 2 + 0) * nr_max + lr] = 0.0f;
+        if (in_strip && (col0 == nx || col1 == nx)) sm.BX[(sp * 2 + 1) * nr_max + lr] = 0.0f;
+        if (lane == 0) sm.WF[((size_t)(sp ^ 1) * nr_max + lr) * W + wis] = 0;
+        if (lane == 0 && wis == 0) atomicAdd(sm.NSK, 1ull);   // once per skipped row (rain-free steps only)
+        cur = nxt; fN = Face2{}; fW = fWn; par ^= 1;
+        if (in_strip) { if (W > 1) named_bar(1 + s, 32 * W); else __syncwarp(); }
+        continue;
+      }
       // east faces: west faces of lane+1; lane 31 reads the published face of the lane
       // holding the next column
       Face2 fE = shfl_down_face2(fW);
@@ -716,7 +815,6 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       // strip's last row the next strip's / next CTA's top faces, or the south ghost row
       Cell2 left{}, below{};
       Face2 fS_in{};
-      const bool bottom = last && s + 1 >= S && q + 1 >= C;
       if (!last) {
         nxt = load_pair(lr + 1, r + 1);
         left = left_pair(nxt, lr + 1, r + 1);
@@ -742,6 +840,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       CellNew2 o;
       float2 uu, vv;
       if (!last) {
+        // (the next row's west faces are computed even when that row will be skipped: one
+        // straight-line body keeps both faces' instructions interleaved)
         fS = face2<false, CREST>(cur.h, cur.u, cur.v, cur.c, nxt.h, nxt.u, nxt.v, nxt.c, d_s, d_s2, k);
         fWn = face2<true, CREST>(left.h, left.u, left.v, left.c, nxt.h, nxt.u, nxt.v, nxt.c, d_xn, d_xn2, k);
       } else if (bottom) {
@@ -791,6 +891,10 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
         infil_l += o.infil.y;
         fix_l += o.fix.y;
       }
+      {   // the warp's columns of this row hold water in the new state (read next step)
+        const bool wet_any = __any_sync(0xffffffffu, (cell0 && o.h.x > 0.0f) || (cell1 && o.h.y > 0.0f));
+        if (lane == 0) sm.WF[((size_t)(sp ^ 1) * nr_max + lr) * W + wis] = wet_any ? 1 : 0;
+      }
       cur = nxt; fN = fS; fW = fWn; par ^= 1;
       if (in_strip) { if (W > 1) named_bar(1 + s, 32 * W); else __syncwarp(); }
     }
@@ -809,7 +913,13 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
         sm.WS[(sp * nwarps + wid) * 2 + 1] = wf;
       }
     }
-    gs.full();
+    if (CLUSTERED) {
+      gs.full();
+    } else if (__syncthreads_or(gs.timed_out ? 1 : 0)) {
+      // a barrier wait of this step ran out (bounded wait): the whole CTA leaves together
+      status = 5;
+      break;
+    }
     unsigned smax_bits = 0u, badv = 0u;
     for (int qq = 0; qq < C; ++qq) {
       const unsigned* sl = CLUSTERED ? remote(sm.slot, qq) : sm.slot;
@@ -969,6 +1079,9 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     o.breach_cell = breach_cell; o.breach_sync = breach_sync; o.violation = violation;
     o.lower_bound = lower_bound; o.v0 = v0; o.volume = volume; o.rel_residual = rel_res;
     o.n_rows = n_rows; o.pad = 0;
+    unsigned long long tot_skip = 0ull;
+    for (int qq = 0; qq < C; ++qq) tot_skip += CLUSTERED ? *remote(sm.NSK, qq) : *sm.NSK;
+    o.rows_skipped = tot_skip;
     A.out[d] = o;
   }
   // keep every CTA's shared memory alive until all remote reads are done

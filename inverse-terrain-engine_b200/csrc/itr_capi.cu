@@ -22,6 +22,7 @@
 #include "itr_device.cuh"
 #include "itr_batched.cuh"
 #include "itr_plain.cuh"
+#include "itr_band.cuh"
 #include "itr_adjoint.cuh"
 #include "itr_design.cuh"
 #include "itr_render.cuh"
@@ -68,6 +69,7 @@ struct LaunchCfg {
   size_t smem = 0;
   bool ok = false;
   bool tiled = false;   // the measured choice was the tiled HBM path
+  int band = 1;         // ... with the row-band kernel (1) or the 16x16 tiles (0)
   bool bnd = false;     // the grid has stage or inflow cells (k_batched<..., BND>)
 };
 
@@ -77,6 +79,7 @@ struct LaunchCfg {
 struct Collect {
   int n = 0, n_mon = 0, max_rows = 0;
   size_t N = 0;
+  int nx = 0;                        // cells per row (a skipped row's cell count)
   const itr_design* ds = nullptr;
   itr_result* res = nullptr;
   const itr_objective* ob = nullptr;
@@ -122,6 +125,9 @@ struct itr_ctx {
   int impl = 0, threads = 0, cluster = 0, graph = 1, steps_per_submit = 64;
   int autotune = 1, autotune_top = 6, probe_steps = 200;
   int exact_special = 0;
+  int band = 1;           // tiled path update kernel: 1 = row-band sweep (k_band), 0 = 16x16 tiles
+  unsigned wait_limit = 1u << 22;   // bounded barrier wait of single-CTA designs (try_wait rounds)
+  int stall_wait_test = 0;          // test of the timeout path: that wait never completes
   float tune_ms = 0.0f;
   // baseline-locked dt (itr_gpu_set_locked_dt): the schedule, its limit, the snapshot buffers
   // and, per design of the last batch, the fallback time (-1: none)
@@ -136,6 +142,7 @@ struct itr_ctx {
   DevBuf pH, pQX, pQY, pPK, ppart, pctl;
   // tiled batched path: state planes, tile partials, control blocks of all designs
   DevBuf tH, tQX, tQY, tpart, tctl;
+  DevBuf tRow, tGw, tSnapRow;   // row-band path: dry-row flags, ghost wetness, flags at the locked snapshot
   // adjoint: argmax states, (dt, rain) ring, checkpoints, tape, adjoint state, gradients
   DevBuf aTpk, aRing, aTape, aTape2, aLA, aLB, aGx, aGy, aGx2, aGy2, aSeg, aNst, aSeedC, aSeedS, aSeedW, aSeedN, aTmon;
   cudaStream_t stream2 = nullptr;   // adjoint: the replay of the next segment runs beside the backward steps
@@ -174,6 +181,7 @@ struct itr_ctx {
   bool last_was_tiled = false;
   PlainArgs last_tiled;
   dim3 last_tgrid;
+  int last_band = 1;   // the tiled update kernel of the last tiled batch (option band)
   // autotune cache: (nx, ny, n_designs, mode) -> cfg
   std::map<std::tuple<int, int, int, int>, LaunchCfg> tuned;
   cudaGraphExec_t gexec = nullptr;
@@ -194,6 +202,9 @@ static int fail(itr_ctx* c, int code, const char* fmt, ...) {
     cudaError_t e_ = (x);                                                                        \
     if (e_ != cudaSuccess) return fail(ctx, ITR_DEVICE_ERROR, "%s: %s", #x, cudaGetErrorString(e_)); \
   } while (0)
+
+// Step limit of every run on the device (status 4 beyond it).
+constexpr unsigned long long kMaxSteps = 2000000000ull;
 
 // ------------------------------------------------------------------ kernels table ----
 typedef void (*BatchedFn)(const BatchArgs);
@@ -234,7 +245,7 @@ static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_targe
   c.S = S;
   c.T = S * 32 * c.W;
   if (c.T > 1024) return c;
-  c.smem = batched_smem_bytes(nr_max, nx, S, c.W, c.T / 32, crest ? 1 : 0, bnd ? 1 : 0);
+  c.smem = batched_smem_bytes(nr_max, nx, S, c.W, c.T / 32, crest ? 1 : 0, bnd ? 1 : 0, ny);
   c.ok = c.smem <= ctx->smem_optin;
   return c;
 }
@@ -539,7 +550,7 @@ void itr_gpu_destroy(itr_ctx* ctx) {
   for (DevBuf* b : {&ctx->wet, &ctx->gn2, &ctx->bc, &ctx->dzx, &ctx->dzy, &ctx->dzx2, &ctx->dzy2, &ctx->h0, &ctx->cut, &ctx->fill,
                     &ctx->mon, &ctx->obj_i, &ctx->obj_d, &ctx->peak, &ctx->depth, &ctx->ledger, &ctx->out, &ctx->mmax,
                     &ctx->pH, &ctx->pQX, &ctx->pQY, &ctx->pPK, &ctx->ppart, &ctx->pctl, &ctx->tH, &ctx->tQX, &ctx->tQY,
-                    &ctx->tpart, &ctx->tctl, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aTape2, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy, &ctx->aGx2, &ctx->aGy2,
+                    &ctx->tpart, &ctx->tctl, &ctx->tRow, &ctx->tGw, &ctx->tSnapRow, &ctx->aTpk, &ctx->aRing, &ctx->aTape, &ctx->aTape2, &ctx->aLA, &ctx->aLB, &ctx->aGx, &ctx->aGy, &ctx->aGx2, &ctx->aGy2,
                     &ctx->aSeg, &ctx->aNst, &ctx->aSeedC, &ctx->aSeedS, &ctx->aSeedW, &ctx->aSeedN, &ctx->aTmon,
                     &ctx->mDz, &ctx->mZe, &ctx->mAux, &ctx->mJp, &ctx->mJob, &ctx->mOut, &ctx->wsb, &ctx->rIn, &ctx->rOut,
                     &ctx->lDt, &ctx->lS4, &ctx->lS2, &ctx->lSk, &ctx->lSs, &ctx->lFb})
@@ -589,6 +600,9 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   else if (k == "autotune") { ctx->autotune = value != 0; ctx->tuned.clear(); }
   else if (k == "exact_special") ctx->exact_special = value != 0;
   else if (k == "warm_start") ctx->warm_start = value != 0;
+  else if (k == "band") ctx->band = value != 0;
+  else if (k == "wait_limit") { if (value < 1 || value > 0x7fffffff) return fail(ctx, ITR_INVALID_ARG, "wait_limit out of range"); ctx->wait_limit = (unsigned)value; }
+  else if (k == "stall_wait_test") ctx->stall_wait_test = value != 0;
   else if (k == "probe_steps") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "probe_steps must be >= 1"); ctx->probe_steps = (int)value; }
   else return fail(ctx, ITR_INVALID_ARG, "unknown option '%s'", key);
   if (k == "threads" || k == "cluster") ctx->tuned.clear();
@@ -631,6 +645,29 @@ static void launch_update(const PlainArgs& A, dim3 grid, cudaStream_t st) {
   }
 }
 
+// One step's update of the tiled batched path: the row-band sweep (itr_band.cuh) over
+// (segment groups, bands, designs), or with option band = 0 the 16x16-tile kernel.
+static void launch_tiled_update(const itr_ctx* ctx, const PlainArgs& A, dim3 grid, cudaStream_t st) {
+  if (!ctx->band) { launch_update(A, grid, st); return; }
+  const bool bnd = A.bh != nullptr || A.P.inflow.n > 0;
+  const BandGeom bg = band_geom(A.nx, A.ny, A.band_rows);
+  const dim3 block((unsigned)(32 * bg.wpb));
+  if (A.mode == 1) {
+    if (bnd) k_band<true, true><<<grid, block, 0, st>>>(A);
+    else k_band<true, false><<<grid, block, 0, st>>>(A);
+  } else {
+    if (bnd) k_band<false, true><<<grid, block, 0, st>>>(A);
+    else k_band<false, false><<<grid, block, 0, st>>>(A);
+  }
+}
+
+// Blocks per design of the tiled path's update (the finalize's partials).
+static dim3 tiled_grid(const itr_ctx* ctx, int nx, int ny, int n) {
+  if (!ctx->band) return dim3((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile);
+  const BandGeom bg = band_geom(nx, ny, band_rows_for(nx, ny, n, ctx->sm_count));
+  return dim3((unsigned)bg.gx, (unsigned)bg.gy);
+}
+
 static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid, int* launches) {
   k_plain_init<<<1, 1024, 0, ctx->stream>>>(A);
   k_plain_finalize<<<1, 32, 0, ctx->stream>>>(A, n_blocks, 1);
@@ -647,7 +684,8 @@ static int run_plain_design(itr_ctx* ctx, PlainArgs& A, int n_blocks, dim3 grid,
     CU(cudaStreamSynchronize(ctx->stream));
     done = hctl->done;
     if (done) break;
-    if (guard > 100000000ull) return fail(ctx, ITR_DEVICE_TIMEOUT, "plain run did not terminate");
+    // the device stops a run at its step limit (status 4), so this bound never ends a run
+    if (guard > kMaxSteps / (uint64_t)ctx->steps_per_submit + 2) return fail(ctx, ITR_DEVICE_TIMEOUT, "plain run did not terminate");
   }
   return ITR_OK;
 }
@@ -690,7 +728,7 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
   if (tape) { tape->dt.assign(n, std::vector<double>()); tape->blocks = 0; }
   auto block = [&]() {
     for (int s = 0; s < K; ++s) {
-      launch_update(A, grid, st);
+      launch_tiled_update(ctx, A, grid, st);
       if (locked) {
         k_plain_finalize_locked<<<n, kFinThreads, 0, st>>>(A, nb, 0);
         k_plain_locked_copy<<<cgrid, 256, 0, st>>>(A);
@@ -757,7 +795,7 @@ static int run_tiled_batch(itr_ctx* ctx, PlainArgs& A, int n, dim3 tgrid, int* l
     bool all = true;
     for (int d = 0; d < n; ++d) all = all && hc[d].done;
     if (all) break;
-    if (polls > 100000000ull) { rc = fail(ctx, ITR_DEVICE_TIMEOUT, "tiled run did not terminate"); break; }
+    if (polls > kMaxSteps / (uint64_t)K + 2) { rc = fail(ctx, ITR_DEVICE_TIMEOUT, "tiled run did not terminate"); break; }
   }
   if (ge) cudaGraphExecDestroy(ge);
   return rc;
@@ -987,7 +1025,9 @@ static int collect_results(itr_ctx* ctx, const Collect& c) {
     itr_result& r = res[d];
     if (o.status >= 4) return fail(ctx, ITR_DEVICE_TIMEOUT, "design %d: run exceeded its step or wait limit (status %d)", d, o.status);
     r.steps = o.steps;
-    r.cell_updates = o.steps * (uint64_t)N;
+    r.rows_skipped = o.rows_skipped;
+    // cells actually advanced (RunSummary::cell_updates: steps x cells minus skipped dry rows)
+    r.cell_updates = o.steps * (uint64_t)N - o.rows_skipped * (uint64_t)c.nx;
     cu += r.cell_updates;
     r.t_end = o.t_end;
     r.sync_count = o.sync_count;
@@ -1275,17 +1315,20 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
       warm_dev = ctx->wsb.as<WarmStart>();
     }
   }
-  const unsigned long long max_steps = 2000000000ull;
+  const unsigned long long max_steps = kMaxSteps;
 
   // impl 2, or a grid no cluster shape can hold: the tiled batched path (state in HBM)
   bool tiled = ctx->impl == 2 || ctx->vjp != nullptr;
-  const dim3 tgrid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile);
-  const int n_tiles = (int)(tgrid.x * tgrid.y);
+  dim3 tgrid = tiled_grid(ctx, nx, ny, n);   // blocks per design of the tiled path's update
+  int n_tiles = (int)(tgrid.x * tgrid.y);
+  const int band0 = ctx->band;
+  const int max_tiles = std::max((nx + kTile - 1) / kTile * ((ny + kTile - 1) / kTile), n_tiles);
+  const bool bnd_grid = has_stage || P.inflow.n > 0;   // stage or inflow ghosts
   auto tiled_args = [&](PlainArgs& A) -> cudaError_t {
     cudaError_t e = ctx->tH.ensure((size_t)n * 2 * N * 4);
     if (e == cudaSuccess) e = ctx->tQX.ensure((size_t)n * 2 * N * 4);
     if (e == cudaSuccess) e = ctx->tQY.ensure((size_t)n * 2 * N * 4);
-    if (e == cudaSuccess) e = ctx->tpart.ensure((size_t)n * n_tiles * kPart * 8);
+    if (e == cudaSuccess) e = ctx->tpart.ensure((size_t)n * max_tiles * kPart * 8);
     if (e == cudaSuccess) e = ctx->tctl.ensure((size_t)n * sizeof(PlainCtl));
     memset(&A, 0, sizeof(A));
     A.P = P; A.nx = nx; A.ny = ny; A.mode = g->mode; A.n_designs = n;
@@ -1324,8 +1367,19 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
       A.fallback_t = ctx->lFb.as<double>();
       ctx->locked_run = true;
     }
+    A.band_rows = band_rows_for(nx, ny, n, ctx->sm_count);
+    if (ctx->band && e == cudaSuccess) {   // dry-row skipping on the row-band path
+      const size_t R = (size_t)ny + 2;
+      e = ctx->tRow.ensure((size_t)n * 2 * R * 4);
+      if (e == cudaSuccess && bnd_grid) e = ctx->tGw.ensure((size_t)n * R);
+      if (e == cudaSuccess && locked) e = ctx->tSnapRow.ensure((size_t)n * R * 4);
+      A.rowwet = ctx->tRow.as<unsigned>();
+      A.gwet = bnd_grid ? ctx->tGw.as<uint8_t>() : nullptr;
+      A.snaprow = locked ? ctx->tSnapRow.as<unsigned>() : nullptr;
+    }
     return e;
   };
+  int tiled_band = ctx->band;   // the tiled path's update kernel for this batch (the autotuner may pick)
   if (ctx->impl == 0 && !tiled) {
     BatchArgs A;
     memset(&A, 0, sizeof(A));
@@ -1351,6 +1405,8 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.out = ctx->out.as<DesignOut>();
     A.max_steps = max_steps;
     A.exact = ctx->exact_special ? 1u : 0u;
+    A.wait_limit = ctx->wait_limit;
+    A.stall_test = ctx->stall_wait_test ? 1u : 0u;
     A.warm = warm_dev;
     // launch configuration
     LaunchCfg cfg;
@@ -1361,6 +1417,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     } else if (ctx->tuned.count(key) && !(locked && ctx->tuned[key].tiled)) {
       cfg = ctx->tuned[key];
       tiled = cfg.tiled;
+      if (tiled) tiled_band = cfg.band;
     } else {
       std::vector<LaunchCfg> cands = candidates(ctx, nx, ny, n, crest, bnd);
       if (cands.empty()) {
@@ -1373,29 +1430,44 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
           rc = autotune(ctx, A, cands, n, &cfg);
           if (rc != ITR_OK) return rc;
         }
-        if (ctx->autotune && !locked) {
-          // the tiled HBM path as one more candidate, timed over the same probe steps
+        if (ctx->autotune && !locked && !ctx->defer) {
+          // the tiled HBM path as one more candidate, timed over the same probe steps (not for
+          // a ladder group: the ladder runs every group's cluster kernel in one graph launch)
           PlainArgs T;
           CU(tiled_args(T));   // (no locked schedule here: the tiled candidate is timed only unlocked)
           T.max_steps = (unsigned long long)ctx->probe_steps;
           T.warm = nullptr;
           T.obj.enabled = 0; T.ledger = nullptr; T.max_rows = 0;
           int dummy = 0;
-          float t_ms = 0.0f;
-          // direct launches and one poll: no graph build or host round trips in the timing
+          // both update kernels of the tiled path, row bands and 16x16 tiles; direct launches
+          // and one poll: no graph build or host round trips in the timing
           const int g0 = ctx->graph, k0 = ctx->steps_per_submit;
           ctx->graph = 0; ctx->steps_per_submit = ctx->probe_steps;
-          CU(cudaEventRecord(ctx->ev[1], ctx->stream));
-          rc = run_tiled_batch(ctx, T, n, tgrid, &dummy);
+          for (int bk = 1; bk >= 0 && rc == ITR_OK; --bk) {
+            ctx->band = bk;
+            const dim3 tg = tiled_grid(ctx, nx, ny, n);
+            float t_ms = 0.0f;
+            cudaError_t e = tiled_args(T);
+            T.max_steps = (unsigned long long)ctx->probe_steps;
+            T.warm = nullptr;
+            T.obj.enabled = 0; T.ledger = nullptr; T.max_rows = 0;
+            if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->stream);
+            if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "tiled probe: %s", cudaGetErrorString(e)); break; }
+            rc = run_tiled_batch(ctx, T, n, tg, &dummy);
+            if (rc != ITR_OK) break;
+            e = cudaEventRecord(ctx->ev[2], ctx->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(ctx->ev[2]);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t_ms, ctx->ev[1], ctx->ev[2]);
+            if (e != cudaSuccess) { rc = fail(ctx, ITR_DEVICE_ERROR, "tiled probe: %s", cudaGetErrorString(e)); break; }
+            if (t_ms < ctx->tune_ms) { cfg.tiled = true; cfg.band = bk; ctx->tune_ms = t_ms; }
+          }
           ctx->graph = g0; ctx->steps_per_submit = k0;
+          ctx->band = band0;
           if (rc != ITR_OK) return rc;
-          CU(cudaEventRecord(ctx->ev[2], ctx->stream));
-          CU(cudaEventSynchronize(ctx->ev[2]));
-          CU(cudaEventElapsedTime(&t_ms, ctx->ev[1], ctx->ev[2]));
-          if (t_ms < ctx->tune_ms) { cfg.tiled = true; ctx->tune_ms = t_ms; }
         }
         if (!(locked && ctx->tuned.count(key))) ctx->tuned[key] = cfg;   // a locked run keeps a cached tiled choice
         tiled = cfg.tiled;
+        if (tiled) tiled_band = cfg.band;
       }
     }
     if (!tiled) {
@@ -1423,7 +1495,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
         ctx->last_args = A; ctx->last_cfg = cfg; ctx->have_last = true;
         ctx->last_was_plain = false; ctx->last_was_tiled = false;
         Collect& c = ctx->pending;
-        c.n = n; c.n_mon = n_mon; c.max_rows = max_rows; c.N = N; c.ds = ds; c.res = res; c.ob = ob;
+        c.n = n; c.nx = nx; c.n_mon = n_mon; c.max_rows = max_rows; c.N = N; c.ds = ds; c.res = res; c.ob = ob;
         c.mon = mon; c.dmon = reinterpret_cast<const unsigned*>(dv + o_mon); c.launches = launches;
         ctx->pending_ok = true;
         return ITR_OK;
@@ -1441,6 +1513,13 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     }
   }
   if (tiled) {
+    struct BandScope {   // the tuned kernel choice for this batch; the option stays the caller's
+      itr_ctx* c; int v;
+      ~BandScope() { c->band = v; }
+    } band_scope{ctx, band0};
+    ctx->band = tiled_band;
+    tgrid = tiled_grid(ctx, nx, ny, n);
+    n_tiles = (int)(tgrid.x * tgrid.y);
     const int nb = n_tiles;
     PlainArgs A;
     CU(tiled_args(A));
@@ -1455,6 +1534,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     }
     CU(cudaEventRecord(ctx->ev[1], ctx->stream));
     rc = run_tiled_batch(ctx, A, n, tgrid, &launches);
+    ctx->last_band = ctx->band;
     if (rc != ITR_OK) return rc;
     k_plain_outputs<<<n, 256, 0, ctx->stream>>>(A, nb, ctx->out.as<DesignOut>(), ctx->depth.as<float>());
     launches += 1;
@@ -1521,7 +1601,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
   CU(cudaGetLastError());
 
   Collect col;
-  col.n = n; col.n_mon = n_mon; col.max_rows = max_rows; col.N = N; col.ds = ds; col.res = res; col.ob = ob;
+  col.n = n; col.nx = nx; col.n_mon = n_mon; col.max_rows = max_rows; col.N = N; col.ds = ds; col.res = res; col.ob = ob;
   col.mon = mon; col.dmon = reinterpret_cast<const unsigned*>(dv + o_mon); col.launches = launches;
   return collect_results(ctx, col);
 }
@@ -1551,6 +1631,7 @@ extern "C" int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_g
     c->impl = ctx->impl; c->threads = ctx->threads; c->cluster = ctx->cluster; c->graph = ctx->graph;
     c->steps_per_submit = ctx->steps_per_submit; c->autotune = ctx->autotune; c->autotune_top = ctx->autotune_top;
     c->probe_steps = ctx->probe_steps; c->exact_special = ctx->exact_special;
+    c->wait_limit = ctx->wait_limit; c->stall_wait_test = ctx->stall_wait_test;
     if (!c->ev_fork) CU(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     c->defer = true;
     c->pending_ok = false;
@@ -1560,6 +1641,21 @@ extern "C" int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_g
     if (rc != ITR_OK) return fail(ctx, rc, "ladder group %d: %s", gi, c->err.c_str());
     CU(cudaStreamSynchronize(c->stream));   // its inputs are on the device before the graph runs
     off += (size_t)(G.n_designs > 0 ? G.n_designs : 0);
+  }
+  // Groups whose launch shapes use the same kernel instantiation share its maximum dynamic
+  // shared-memory attribute: set it to the largest of their needs before the capture.
+  {
+    std::vector<std::pair<BatchedFn, size_t>> need;
+    for (int gi = 0; gi < n_groups; ++gi) {
+      itr_ctx* c = ctx->children[gi];
+      if (!c->pending_ok) continue;
+      const LaunchCfg& cf = c->last_cfg;
+      BatchedFn fn = batched_fn(c->last_args.mode == 1, cf.C > 1, maxt_bucket(cf.T), cf.bnd, c->last_args.locked_dt != nullptr);
+      bool found = false;
+      for (auto& e : need) if (e.first == fn) { e.second = std::max(e.second, cf.smem); found = true; }
+      if (!found) need.push_back({fn, cf.smem});
+    }
+    for (auto& e : need) CU(cudaFuncSetAttribute((const void*)e.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.second));
   }
   // one graph: fork from the context stream into every deferred group's stream, join back
   cudaGraph_t gr = nullptr;
@@ -1771,7 +1867,7 @@ extern "C" int itr_gpu_record_baseline(itr_ctx* ctx, const itr_params* p, const 
 static MatPrim mat_prim(const itr_primitive& q) {
   MatPrim m;
   memset(&m, 0, sizeof(m));
-  m.kind = q.kind; m.width = q.width; m.height = q.height;
+  m.kind = q.kind; m.width = q.width; m.height = q.height; m.length = q.length;
   if (q.kind == ITR_PRIM_MOUND) {
     m.x0 = m.x1 = q.cx; m.y0 = m.y1 = q.cy;
   } else {
@@ -1897,44 +1993,36 @@ extern "C" int itr_gpu_vjp_primitives(itr_ctx* ctx, const itr_params* p, const i
   rc = itr_gpu_vjp(ctx, p, g, n, M.ds.data(), mon, n_mon, ob, checkpoint_interval, res, dj_ddzx, dj_ddzy);
   ctx->mat = nullptr;
   if (rc != ITR_OK) return rc;
-  // central differences of the materialisation, one job per (primitive, parameter)
-  const double steps[3] = {1e-4, 1e-3, 1e-3};   // height, width, length
+  // the written-out derivative of the materialisation, one job per primitive over its own box
   std::vector<MatPrim> jp;
   std::vector<MatJob> jobs;
   for (int d = 0; d < n; ++d)
-    for (int k = prim_off[d]; k < prim_off[d + 1]; ++k)
-      for (int j = 0; j < 3; ++j) {
-        MatJob J;
-        memset(&J, 0, sizeof(J));
-        J.design = d;
-        J.out = 3 * (k - prim_off[0]) + j;
-        J.twoh = 2.0 * steps[j];
-        for (int sgn = 0; sgn < 2; ++sgn) {
-          const int b0 = (int)jp.size();
-          for (int q = prim_off[d]; q < prim_off[d + 1]; ++q) {
-            itr_primitive v = prims[q];
-            if (q == k) {
-              const double h = sgn == 0 ? steps[j] : -steps[j];
-              if (j == 0) v.height += h; else if (j == 1) v.width += h; else v.length += h;
-            }
-            jp.push_back(mat_prim(v));
-          }
-          MatDesign B = mat_box(jp.data(), b0, (int)jp.size(), sp, g);
-          (sgn == 0 ? J.up : J.dn) = B;
-        }
-        jobs.push_back(J);
-      }
+    for (int k = prim_off[d]; k < prim_off[d + 1]; ++k) {
+      MatJob J;
+      memset(&J, 0, sizeof(J));
+      J.design = d;
+      J.prim = (int)jp.size();
+      J.out = 3 * (k - prim_off[0]);
+      MatPrim one = M.prims[k];
+      one.height = 1.0;   // the box of this primitive alone, also when its height is 0
+      jp.push_back(M.prims[k]);
+      const MatDesign B = mat_box(&one, 0, 1, sp, g);
+      J.c0 = B.c0; J.r0 = B.r0; J.c1 = B.c1; J.r1 = B.r1;
+      jobs.push_back(J);
+    }
   const cudaStream_t st = ctx->stream;
   CU(ctx->mAux.ensure(2 * N));
   CU(ctx->mJp.ensure((jp.size() > 0 ? jp.size() : 1) * sizeof(MatPrim)));
   CU(ctx->mJob.ensure((jobs.size() > 0 ? jobs.size() : 1) * sizeof(MatJob)));
-  CU(ctx->mOut.ensure((jobs.size() > 0 ? jobs.size() : 1) * 8));
-  CU(ctx->mDz.ensure((size_t)n * N * 8));
+  CU(ctx->mOut.ensure((size_t)(3 * (jobs.size() > 0 ? jobs.size() : 1)) * 8));
+  CU(ctx->mZe.ensure((size_t)n * N * 8));
   CU(cudaMemcpyAsync(ctx->mAux.p, sp->editable, N, cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(ctx->mAux.as<uint8_t>() + N, sp->wall, N, cudaMemcpyHostToDevice, st));
   if (!jp.empty()) CU(cudaMemcpyAsync(ctx->mJp.p, jp.data(), jp.size() * sizeof(MatPrim), cudaMemcpyHostToDevice, st));
   if (!jobs.empty()) CU(cudaMemcpyAsync(ctx->mJob.p, jobs.data(), jobs.size() * sizeof(MatJob), cudaMemcpyHostToDevice, st));
-  double* gdz = ctx->mDz.as<double>();
+  // dz of the designs is still in mDz (the forward's materialisation); the edited levels in
+  // mZe are no longer needed and take dJ/d(dz)
+  double* gdz = ctx->mZe.as<double>();
   k_mat_gdz<<<dim3((unsigned)((N + 255) / 256), (unsigned)n), 256, 0, st>>>(nx, ny, ctx->aGx.as<double>(), ctx->aGy.as<double>(),
                                                                            ctx->mAux.as<uint8_t>() + N, gdz);
   if (!jobs.empty()) {
@@ -1944,9 +2032,9 @@ extern "C" int itr_gpu_vjp_primitives(itr_ctx* ctx, const itr_params* p, const i
     MA.ox = sp->origin_x; MA.oy = sp->origin_y; MA.dx = g->dx; MA.dy = g->dy;
     MA.z_wall = sp->z_wall; MA.max_abs_dz = sp->max_abs_dz;
     MA.editable = ctx->mAux.as<uint8_t>();
-    k_mat_grad<<<(unsigned)jobs.size(), 256, 0, st>>>(MA, ctx->mJp.as<MatPrim>(), ctx->mJob.as<MatJob>(), gdz, ob->earth_weight,
-                                                      ob->cut_cost, ob->fill_cost, ctx->mOut.as<double>());
-    CU(cudaMemcpyAsync(dj_dprim, ctx->mOut.p, jobs.size() * 8, cudaMemcpyDeviceToHost, st));
+    k_mat_dgrad<<<(unsigned)jobs.size(), 256, 0, st>>>(MA, ctx->mJp.as<MatPrim>(), ctx->mJob.as<MatJob>(), ctx->mDz.as<double>(),
+                                                       gdz, ob->earth_weight, ob->cut_cost, ob->fill_cost, ctx->mOut.as<double>());
+    CU(cudaMemcpyAsync(dj_dprim, ctx->mOut.p, 3 * jobs.size() * 8, cudaMemcpyDeviceToHost, st));
   }
   CU(cudaStreamSynchronize(st));
   return ITR_OK;
@@ -1981,7 +2069,10 @@ extern "C" int itr_gpu_rerun_resident(itr_ctx* ctx) {
   CU(cudaEventRecord(ctx->ev[1], ctx->stream));
   if (ctx->last_was_tiled) {
     PlainArgs A = ctx->last_tiled;
+    const int band = ctx->band;
+    ctx->band = ctx->last_band;   // the kernel its partials were laid out for
     int rc = run_tiled_batch(ctx, A, A.n_designs, ctx->last_tgrid, &launches);
+    ctx->band = band;
     if (rc != ITR_OK) return rc;
   } else if (!ctx->last_was_plain) {
     int rc = launch_batched(ctx, ctx->last_args, ctx->last_cfg, ctx->last_args.n_designs);

@@ -24,6 +24,7 @@ namespace itr {
 struct MatPrim {
   double x0, y0, x1, y1;   // segment end points (equal for a mound)
   double width, height;
+  double length;           // Primitive::length (the adjoint chain's d(end point)/dL)
   int kind;                // 0 berm, 1 swale, 2 cut, 3 mound
   int pad;
 };
@@ -163,8 +164,9 @@ __global__ void k_mat_volumes(const MatArgs M) {
 // ---- the design chain of the adjoint: dJ/d(height, width, length) per primitive ----
 // dJ/d(dz) per cell from the face-jump gradients (level 1: each interior jump is the
 // difference of its two cells' levels, the edge jumps stay 0, walls keep z_wall), then per
-// primitive parameter the central difference of the f64 materialisation contracted with it,
-// plus the earthwork term lambda (cut_cost dV_cut + fill_cost dV_fill) (objective.rs:95-128).
+// primitive the derivative of the materialisation, written out from Primitive::profile
+// (design.rs:107-134), contracted with it, plus the earthwork term lambda (cut_cost dV_cut +
+// fill_cost dV_fill) (objective.rs:95-128).
 
 // dJ/d(dz) of every cell of every design (grid: cells / 256 x designs).
 __global__ void k_mat_gdz(int nx, int ny, const double* gx, const double* gy, const uint8_t* wall, double* gdz) {
@@ -180,63 +182,94 @@ __global__ void k_mat_gdz(int nx, int ny, const double* gx, const double* gy, co
   gdz[(size_t)d * N + i] = wall[i] ? 0.0 : ((a - b) + e) - f;
 }
 
-// One central difference: the up and down perturbed primitive sets of one parameter of one
-// primitive of design `design`, each with its own box.
+// The profile at (x, y) and its derivatives with respect to the primitive's width and length
+// at fixed centre and angle. With s = d / (w / 2):
+//   ridge P = (1 - s^2)^2, dP/ds = -4 s (1 - s^2);
+//   cut   P = 1 for s <= 1/2, else (1 - u^2)^2 with u = 2 s - 1, dP/ds = -8 u (1 - u^2);
+//   ds/dw = -s / w;  ds/dL = (2 / w) dd/dL, dd/dL = 0 beside the segment and, beyond an end,
+//   the end's displacement (+-(cos a, sin a) / 2 per unit length) projected on the unit
+//   vector from the sample to it.
+__device__ __forceinline__ void mat_profile_d(const MatPrim& p, double x, double y, double& P, double& dw, double& dl) {
+  P = 0.0; dw = 0.0; dl = 0.0;
+  const double vx = p.x1 - p.x0, vy = p.y1 - p.y0;
+  const double l2 = vx * vx + vy * vy;
+  double t = 0.0;
+  int end = 0;
+  if (l2 > 0.0) {
+    t = ((x - p.x0) * vx + (y - p.y0) * vy) / l2;
+    if (t < 0.0) { t = 0.0; end = -1; }
+    else if (t > 1.0) { t = 1.0; end = 1; }
+  }
+  const double px = p.x0 + t * vx - x, py = p.y0 + t * vy - y;
+  const double d = sqrt(px * px + py * py);
+  const double half = 0.5 * p.width;
+  const double s = d / half;
+  if (s >= 1.0) return;
+  double dPds;
+  if (p.kind == 2) {
+    if (s <= 0.5) { P = 1.0; dPds = 0.0; }
+    else { const double u = (s - 0.5) / 0.5, w = 1.0 - u * u; P = w * w; dPds = -8.0 * u * w; }
+  } else {
+    const double w = 1.0 - s * s;
+    P = w * w; dPds = -4.0 * s * w;
+  }
+  dw = dPds * (-s / p.width);
+  if (end != 0 && d > 0.0 && p.kind != 3 && p.length > 0.0) {
+    const double ex = vx / (2.0 * p.length), ey = vy / (2.0 * p.length);
+    dl = dPds * ((double)end * (px * ex + py * ey) / d) / half;
+  }
+}
+
+// One primitive of one design: its own box of cells (materialize's box of that primitive).
 struct MatJob {
-  int design;
-  MatDesign up, dn;   // primitives [p0, p1) of the job's prim table, and the boxes
-  double twoh;        // 2 h
-  int out;            // output index (primitive * 3 + parameter)
+  int design, prim;           // prim indexes the job's primitive table
+  int c0, r0, c1, r1;
+  int out;                    // output index (3 per primitive: height, width, length)
+  int pad;
 };
 
-// dz of cell (r, c) for the primitives [p0, p1) inside box B (0 outside it or if not editable).
-__device__ __forceinline__ double mat_cell(const MatArgs& M, const MatPrim* ps, const MatDesign& B, int r, int c) {
-  if (!(c >= B.c0 && c < B.c1 && r >= B.r0 && r < B.r1) || !M.editable[(size_t)r * M.nx + c]) return 0.0;
-  double acc = 0.0;
-  for (int q = B.p0; q < B.p1; ++q) {
-    const MatPrim p = ps[q];
-    if (p.height == 0.0) continue;
-    double s = 0.0;
+// One block per primitive: over its box, d(dz)/d(height, width, length) of every editable cell
+// whose dz is not clamped, contracted with dJ/d(dz) plus the earthwork weight (the side of 0
+// the cell's dz lies on; the mean of both sides at 0, as a central difference would see it).
+__global__ void k_mat_dgrad(const MatArgs M, const MatPrim* jp, const MatJob* jobs, const double* dz, const double* gdz,
+                            double earth_w, double cut_cost, double fill_cost, double* out) {
+  const MatJob J = jobs[blockIdx.x];
+  const MatPrim p = jp[J.prim];
+  const int w = J.c1 - J.c0, h = J.r1 - J.r0;
+  const size_t N = (size_t)M.nx * M.ny;
+  const double area = M.dx * M.dy;
+  double s[3] = {0, 0, 0};
+  for (int k = threadIdx.x; w > 0 && h > 0 && k < w * h; k += blockDim.x) {
+    const int r = J.r0 + k / w, c = J.c0 + k % w;
+    const size_t i = (size_t)r * M.nx + c;
+    const double z = dz[(size_t)J.design * N + i];
+    if (!M.editable[i] || !(z > -M.max_abs_dz && z < M.max_abs_dz)) continue;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     for (int sy = 0; sy < 4; ++sy)
       for (int sx = 0; sx < 4; ++sx) {
         const double x = M.ox + ((double)c + ((double)sx + 0.5) / 4.0) * M.dx;
         const double y = M.oy - ((double)r + ((double)sy + 0.5) / 4.0) * M.dy;
-        s += mat_profile(p, x, y);
+        double P, dw, dl;
+        mat_profile_d(p, x, y, P, dw, dl);
+        a0 += P; a1 += dw; a2 += dl;
       }
-    acc += p.height * s * (1.0 / 16.0);
+    const double we = area * (z > 0.0 ? fill_cost : (z < 0.0 ? -cut_cost : 0.5 * (fill_cost - cut_cost)));
+    const double g = gdz[(size_t)J.design * N + i] + earth_w * we;
+    s[0] += g * a0 * (1.0 / 16.0);
+    s[1] += g * p.height * a1 * (1.0 / 16.0);
+    s[2] += g * p.height * a2 * (1.0 / 16.0);
   }
-  return acc < -M.max_abs_dz ? -M.max_abs_dz : (acc > M.max_abs_dz ? M.max_abs_dz : acc);
-}
-
-// One block per job: sum gdz * (dz_up - dz_dn) over the union of the two boxes, and the
-// cut / fill volumes of both sets; out = sum / 2h + lambda (cut_cost dcut + fill_cost dfill) / 2h.
-__global__ void k_mat_grad(const MatArgs M, const MatPrim* jp, const MatJob* jobs, const double* gdz, double earth_w,
-                           double cut_cost, double fill_cost, double* out) {
-  const MatJob J = jobs[blockIdx.x];
-  const int c0 = min(J.up.c0, J.dn.c0), r0 = min(J.up.r0, J.dn.r0);
-  const int c1 = max(J.up.c1, J.dn.c1), r1 = max(J.up.r1, J.dn.r1);
-  const int w = c1 - c0, h = r1 - r0;
-  const size_t N = (size_t)M.nx * M.ny;
-  const double a = M.dx * M.dy;
-  double s[5] = {0, 0, 0, 0, 0};   // contraction, cut up, fill up, cut down, fill down
-  for (int k = threadIdx.x; w > 0 && h > 0 && k < w * h; k += blockDim.x) {
-    const int r = r0 + k / w, c = c0 + k % w;
-    const double u = mat_cell(M, jp, J.up, r, c), v = mat_cell(M, jp, J.dn, r, c);
-    s[0] += gdz[(size_t)J.design * N + (size_t)r * M.nx + c] * (u - v);
-    if (u > 0.0) s[2] += u * a; else s[1] -= u * a;
-    if (v > 0.0) s[4] += v * a; else s[3] -= v * a;
-  }
-  __shared__ double red[32][5];
-  for (int j = 0; j < 5; ++j)
+  __shared__ double red[32][3];
+  for (int j = 0; j < 3; ++j)
     for (int o = 16; o > 0; o >>= 1) s[j] += __shfl_xor_sync(0xffffffffu, s[j], o);
   if ((threadIdx.x & 31) == 0)
-    for (int j = 0; j < 5; ++j) red[threadIdx.x >> 5][j] = s[j];
+    for (int j = 0; j < 3; ++j) red[threadIdx.x >> 5][j] = s[j];
   __syncthreads();
   if (threadIdx.x == 0) {
-    double t[5] = {0, 0, 0, 0, 0};
+    double t[3] = {0, 0, 0};
     for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
-      for (int j = 0; j < 5; ++j) t[j] += red[q][j];
-    out[J.out] = t[0] / J.twoh + earth_w * (cut_cost * (t[1] - t[3]) + fill_cost * (t[2] - t[4])) / J.twoh;
+      for (int j = 0; j < 3; ++j) t[j] += red[q][j];
+    for (int j = 0; j < 3; ++j) out[J.out + j] = t[j];
   }
 }
 

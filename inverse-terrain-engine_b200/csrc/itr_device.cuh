@@ -345,6 +345,28 @@ ITR_DEV void ghost_state(int code, float& h, float& qx, float& qy, float hstage,
   }
 }
 
+// Ghost wetness of the padded rows for a step whose inflow group values are `inf` (the dry-row
+// test of step_fused, kernel.rs:590-612, takes a row with a wet ghost as wet): a stage ghost
+// holds water when its depth is > 0, an inflow ghost when the group's critical depth is > 0;
+// wall and transmissive ghosts copy their interior cell, so they hold water only beside a wet
+// row and need no flag. gw[j], j = 0 .. ny + 1 (0 and ny + 1: the north and south ghost rows,
+// 1 .. ny: the west and east ghosts of grid row j - 1). bc: device codes (2 stage, 3 + group
+// inflow) north[nx], south[nx], west[ny], east[ny]; bh: stage depths indexed like bc (or NULL).
+// One warp, all 32 lanes.
+ITR_DEV void ghost_row_wet(const uint8_t* bc, int nx, int ny, const float* bh, const float2* inf, uint8_t* gw, int lane) {
+  auto wet = [&](int p) -> bool {
+    const int code = bc[p];
+    return (code == 2 && bh && bh[p] > 0.0f) || (code >= 3 && inf[code - 3].y > 0.0f);
+  };
+  for (int e = 0; e < 2; ++e) {   // the north and south ghost rows
+    bool w = false;
+    for (int c = lane; c < nx; c += 32) w = w || wet(e * nx + c);
+    w = __any_sync(0xffffffffu, w);
+    if (lane == 0) gw[e == 0 ? 0 : ny + 1] = w ? 1 : 0;
+  }
+  for (int j = 1 + lane; j <= ny; j += 32) gw[j] = (wet(2 * nx + j - 1) || wet(2 * nx + ny + j - 1)) ? 1 : 0;
+}
+
 // Run-wide scalars of one call.
 struct RunParams {
   double duration, sync, cfl, dt_max, h_dry, h_eps, infil, initial_depth;
@@ -492,6 +514,7 @@ struct DesignOut {
   double rel_residual;
   int n_rows;
   int pad;
+  unsigned long long rows_skipped;   // dry rows skipped (kernel.rs:605-612)
 };
 
 }  // namespace itr
@@ -579,7 +602,13 @@ ITR_DEV float2 rcp2f(float2 x, unsigned exact) {
   if (__any_sync(0xffffffffu, rcp_out(x.x) | rcp_out(x.y) | exact)) r = rcp2(x);
   return r;
 }
-ITR_DEV float2 canon2(float2 a) { return make_float2(canon(a.x), canon(a.y)); }
+// canon (a == 0 ? +0 : a) as one paired add of +0: x + 0 is x for every x except -0, which
+// rounds to +0; a NaN stays a NaN (its payload may differ, which no result depends on).
+ITR_DEV float2 canon2(float2 a) { return add2(a, f2(0.0f)); }
+// max(a, 0) with the reference's NaN rule (a > 0 ? a : 0): the hardware maximum with +0 gives
+// the same bits for all 2^32 inputs of each component (checked exhaustively on the B200,
+// NaN and -0 included), in one instruction per component instead of a compare and a select.
+ITR_DEV float2 max2z(float2 a) { return make_float2(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f)); }
 ITR_DEV float2 abs2(float2 a) { return make_float2(rabs(a.x), rabs(a.y)); }
 
 ITR_DEV float2 rcbrt2(float2 x, float nz) {
@@ -643,14 +672,14 @@ ITR_DEV Face2 face2(float2 hl, float2 ul, float2 vl, float2 cl, float2 hr, float
   float2 hsl, hsr, csl, csr;
   if (!CREST) {
     const B2 pos = gt2(d0, 0.0f);
-    hsl = max2(sub2(hl, max2(d0, f2(0.0f))), f2(0.0f));
-    hsr = max2(sub2(hr, max2(neg2(d0), f2(0.0f))), f2(0.0f));
+    hsl = max2z(sub2(hl, max2z(d0)));
+    hsr = max2z(sub2(hr, max2z(neg2(d0))));
     const float2 cred = sqrt2(mul2(f2(k.g), sel2(pos, hsl, hsr), NZ));
     csl = sel2(pos, cred, cl);
     csr = sel2(pos, cr, cred);
   } else {
-    hsl = max2(sub2(hl, d0), f2(0.0f));
-    hsr = max2(sub2(hr, d1), f2(0.0f));
+    hsl = max2z(sub2(hl, d0));
+    hsr = max2z(sub2(hr, d1));
     const B2 pl = gt2(d0, 0.0f), pr = gt2(d1, 0.0f);
     const float2 sl = sqrt2(mul2(f2(k.g), hsl, NZ)), sr = sqrt2(mul2(f2(k.g), hsr, NZ));
     csl = sel2(pl, sl, cl);
@@ -676,7 +705,7 @@ ITR_DEV CellNew2 update_cell2(float2 h, float2 qx, float2 qy, const Face2& w, co
   CellNew2 o;
   B2 bad = not2(B2{h1.x >= -k.h_dry, h1.y >= -k.h_dry});
   const B2 neg = lt2(h1, 0.0f);
-  o.fix = sel2(neg, neg2(h1), f2(0.0f));
+  o.fix = max2z(neg2(h1));   // h1 < 0 ? -h1 : 0, the same bits for every h1
   h1 = sel2(neg, f2(0.0f), h1);
   const float2 h2 = add2(h1, mul2(f2(k.rain), wet, NZ));
   o.infil = min2(mul2(f2(k.cap), wet, NZ), h2);

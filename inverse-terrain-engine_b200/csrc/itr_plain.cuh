@@ -52,6 +52,7 @@ struct PlainCtl {
   double s_cur;
   int locked_live;
   int copy_req;
+  unsigned long long rows_skipped;   // dry rows skipped so far (kernel.rs:605-612)
 };
 
 struct PlainArgs {
@@ -94,7 +95,26 @@ struct PlainArgs {
   float* snap;               // per design [4][nx*ny]: h, qx, qy, peaks at the last sync snapshot
   PlainCtl* snapctl;         // per design: the control block at that snapshot
   double* fallback_t;        // per design: time the run fell back to adaptive dt, -1 for none
+  // Dry-row skipping (kernel.rs:605-612), on the row-band path only (NULL elsewhere): per design
+  // [2][ny + 2] flags, padded row j (0 and ny + 1 the ghost rows) held water in the state of
+  // that parity (written by k_band, cleared by the finalize once read); the ghost wetness of
+  // the current step per padded row (stage / inflow grids only, else NULL); the flags at the
+  // locked-dt snapshot.
+  unsigned* rowwet;
+  uint8_t* gwet;
+  unsigned* snaprow;
+  int band_rows;             // row-band kernel: rows per band (1 .. 32)
 };
+
+// Padded row j is dry for the step about to run: no water in its state nor in its stage or
+// inflow ghosts (B.dry of step_fused, kernel.rs:590-612).
+ITR_DEV bool plain_row_dry(const unsigned* rw, const uint8_t* gw, int j) { return rw[j] == 0u && !(gw && gw[j]); }
+
+// Ghost wetness of every padded row for a step starting at the inflow values `inf`
+// (ghost_row_wet); one warp.
+ITR_DEV void plain_ghost_wet(const PlainArgs& A, const float* bh, const float2* inf, uint8_t* gw, int lane) {
+  ghost_row_wet(A.bc, A.nx, A.ny, bh, inf, gw, lane);
+}
 
 // Pointers of design d inside a launch over n_designs designs.
 struct PlainDesign {
@@ -106,6 +126,9 @@ struct PlainDesign {
   unsigned* tpk;
   double* dt_log;
   double cut, fill;
+  unsigned* rowwet;   // [2][ny + 2]
+  uint8_t* gwet;      // [ny + 2]
+  unsigned* snaprow;  // [ny + 2]
 };
 
 ITR_DEV PlainDesign plain_design(const PlainArgs& A, int d, int n_tiles) {
@@ -124,6 +147,10 @@ ITR_DEV PlainDesign plain_design(const PlainArgs& A, int d, int n_tiles) {
   v.dt_log = A.dt_log ? A.dt_log + (size_t)d * A.max_log * 3 : nullptr;
   v.cut = A.cut_d ? A.cut_d[d] : A.cut;
   v.fill = A.fill_d ? A.fill_d[d] : A.fill;
+  const size_t R = (size_t)A.ny + 2;
+  v.rowwet = A.rowwet ? A.rowwet + (size_t)d * 2 * R : nullptr;
+  v.gwet = A.gwet ? A.gwet + (size_t)d * R : nullptr;
+  v.snaprow = A.snaprow ? A.snaprow + (size_t)d * R : nullptr;
   return v;
 }
 
@@ -276,6 +303,24 @@ ITR_DEV void plain_finalize_body(const PlainArgs& A, int n_blocks, int first) {
   const RunParams& P = A.P;
   if constexpr (LOCKED) { if (threadIdx.x == 0) c.copy_req = 0; }   // the last request has been served
   if (c.done) return;
+  if (!first && D.rowwet) {
+    // dry rows the step just skipped (k_band's predicate on the flags it read: the state of
+    // parity c.par, not yet flipped), then clear those flags: the next step writes them
+    __shared__ unsigned s_skip;
+    if (threadIdx.x == 0) s_skip = 0u;
+    __syncthreads();
+    const int R = A.ny + 2;
+    unsigned* rw = D.rowwet + (size_t)c.par * R;
+    if (P.skip_dry && !(c.k.rain > 0.0f)) {
+      unsigned cnt = 0u;
+      for (int j = 1 + threadIdx.x; j <= A.ny; j += blockDim.x)
+        cnt += (plain_row_dry(rw, D.gwet, j - 1) && plain_row_dry(rw, D.gwet, j) && plain_row_dry(rw, D.gwet, j + 1)) ? 1u : 0u;
+      if (cnt) atomicAdd(&s_skip, cnt);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < R; j += blockDim.x) rw[j] = 0u;
+    if (threadIdx.x == 0) c.rows_skipped += s_skip;
+  }
   double tot[kPart] = {0, 0, 0, 0, 0, 0, 0};
   if (!first) {
     for (int b = threadIdx.x; b < n_blocks; b += blockDim.x)
@@ -394,6 +439,8 @@ ITR_DEV void plain_finalize_body(const PlainArgs& A, int n_blocks, int first) {
     __syncwarp();
     if (c.done) return;
     if (lane < P.inflow.n) c.inf[lane] = inflow_values(P.inflow, lane, c.t, P.g);
+    __syncwarp();
+    if (D.gwet) plain_ghost_wet(A, D.bh, c.inf, D.gwet, lane);
     if (lane == 0) {
       const double dt = c.locked_live ? A.locked_dt[c.step] : dmin_num(c.dt_cfl, P.dt_max);
       c.pl = plan_step_dt(P, c.t, c.sync_index, dt);
@@ -401,8 +448,11 @@ ITR_DEV void plain_finalize_body(const PlainArgs& A, int n_blocks, int first) {
     }
     return;
   }
-  // inflow ghosts of the next step, at its start time c.t (fill_ghosts(t), solver.rs)
+  // inflow ghosts of the next step, at its start time c.t (fill_ghosts(t), solver.rs), and
+  // the ghost wetness the row-band kernel's dry-row test reads
   if (lane < P.inflow.n) c.inf[lane] = inflow_values(P.inflow, lane, c.t, P.g);
+  __syncwarp();
+  if (D.gwet) plain_ghost_wet(A, D.bh, c.inf, D.gwet, lane);
   if (lane == 0) {
     if (!(c.t < P.duration && c.sync_index < P.n_sync)) { c.done = 1; return; }
     if (c.step >= A.max_steps) { c.status = 4; c.done = 1; return; }
@@ -431,6 +481,17 @@ __global__ void k_plain_locked_copy(const PlainArgs A) {
   if (c.done || req == 0) return;
   const size_t N = (size_t)A.nx * A.ny, pl = (size_t)c.par * N;
   float* s = A.snap + (size_t)d * 4 * N;
+  if (D.rowwet && blockIdx.x == 0) {   // the dry-row flags of the state (k_band's skipping)
+    const int R = A.ny + 2;
+    for (int j = threadIdx.x; j < R; j += blockDim.x) {
+      if (req == 1) {
+        D.snaprow[j] = D.rowwet[(size_t)c.par * R + j];
+      } else {
+        D.rowwet[(size_t)c.par * R + j] = D.snaprow[j];
+        D.rowwet[(size_t)(c.par ^ 1) * R + j] = 0u;
+      }
+    }
+  }
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
     if (req == 1) {
       s[i] = D.H[pl + i]; s[N + i] = D.QX[pl + i]; s[2 * N + i] = D.QY[pl + i]; s[3 * N + i] = D.PK[i];
@@ -446,10 +507,16 @@ __global__ void k_plain_init(const PlainArgs A) {
   const int nx = A.nx, ny = A.ny, n = nx * ny;
   const RunParams& P = A.P;
   const WarmStart* W = (A.warm && A.warm[blockIdx.x].state) ? &A.warm[blockIdx.x] : nullptr;
+  // dry-row flags of the initial state (init_state: a row is dry when all its depths are 0)
+  if (D.rowwet) {
+    for (int j = threadIdx.x; j < 2 * (ny + 2); j += blockDim.x) D.rowwet[j] = 0u;
+    __syncthreads();
+  }
   if (W) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       D.H[i] = W->state[i]; D.QX[i] = W->state[n + i]; D.QY[i] = W->state[2 * n + i]; D.PK[i] = W->state[3 * n + i];
       if (D.tpk) D.tpk[i] = 0u;
+      if (D.rowwet && W->state[i] != 0.0f) D.rowwet[1 + i / nx] = 1u;
     }
     if (threadIdx.x == 0) {
       PlainCtl c;
@@ -467,6 +534,7 @@ __global__ void k_plain_init(const PlainArgs A) {
     float h = D.h0[i];
     D.H[i] = h; D.QX[i] = 0.0f; D.QY[i] = 0.0f; D.PK[i] = 0.0f;
     if (D.tpk) D.tpk[i] = 0u;
+    if (D.rowwet && h != 0.0f) D.rowwet[1 + i / nx] = 1u;
     double hd = (double)h;
     v0 += hd;
     if (hd > P.h_dry) {
@@ -532,6 +600,7 @@ __global__ void k_plain_outputs(const PlainArgs A, int n_tiles, DesignOut* out, 
     o.steps = c.step; o.t_end = c.t; o.sync_count = c.sync_index; o.status = c.status;
     o.breach_cell = c.breach_cell; o.breach_sync = c.breach_sync; o.violation = c.violation;
     o.lower_bound = c.lower_bound; o.v0 = c.v0; o.volume = c.volume; o.rel_residual = c.rel_res; o.n_rows = c.n_rows;
+    o.rows_skipped = c.rows_skipped;
     out[blockIdx.x] = o;
   }
 }

@@ -70,7 +70,7 @@ class Result(C.Structure):
         ("breach_sync", C.c_uint32), ("violation", C.c_double), ("lower_bound", C.c_double),
         ("j", C.c_double), ("feasible", C.c_int32), ("n_rows", C.c_int32),
         ("volume_m3", C.c_double), ("rel_residual", C.c_double), ("warm_start_steps", C.c_uint64),
-        ("dt_fallback_t", C.c_double),
+        ("dt_fallback_t", C.c_double), ("rows_skipped", C.c_uint64),
     ]
 
 

@@ -10,18 +10,27 @@ dzy[r][c] = z[r][c] - z[r-1][c]; the domain-edge jumps stay 0), so
 dz comes from the design's primitives through DesignSpace::materialize (design.rs:316-385):
 a 4x4 sub-sample quadrature of each primitive's profile times its height, clamped to
 +-max_abs_dz and masked by the editable area. dJ/d(height, width, length) of a primitive at
-fixed quantized centre and angle is the dz gradient contracted with d(dz)/d(theta), taken
-by central differences of the f64 materialize (it is linear in height, and the (1 - s^2)^2
-profile is C1 in width and length), plus the earthwork term's derivative
-lambda (cut_cost dV_cut + fill_cost dV_fill) (objective.rs:95-128).
+fixed quantized centre and angle is the dz gradient contracted with d(dz)/d(theta), plus the
+earthwork term's derivative lambda (cut_cost dV_cut + fill_cost dV_fill) (objective.rs:95-128).
+d(dz)/d(theta) is the derivative of the quadrature, written out from Primitive::profile
+(design.rs:107-134): with s = d / (w / 2) the distance to the segment over the half width,
+  ridge P = (1 - s^2)^2           dP/ds = -4 s (1 - s^2)
+  cut   P = 1 (s <= 1/2), else (1 - u^2)^2 with u = 2 s - 1,   dP/ds = -8 u (1 - u^2)
+  ds/dw = -s / w,   ds/dL = (2 / w) dd/dL,
+where dd/dL is 0 beside the segment and (p - e) . de/dL / d beyond an end e, whose end points
+move by +-(cos a, sin a) / 2 per unit of length. The profile is C1 in w and L (its derivative
+vanishes at s = 1 and is continuous at s = 1/2), so the quadrature's derivative is the sum of
+the samples' derivatives; a cell whose dz is clamped to +-max_abs_dz has none.
+primitive_gradient_fd keeps the central differences of the f64 materialize as the check.
 """
 from __future__ import annotations
 
 import dataclasses
+import math
 
 import numpy as np
 
-from .design import Primitive, materialize
+from .design import CUT, MOUND, Primitive, materialize
 
 PARAMS = ("height", "width", "length")
 STEPS = {"height": 1e-4, "width": 1e-3, "length": 1e-3}
@@ -48,12 +57,92 @@ def _dz_full(prims, geo, nx, ny, editable, max_abs_dz):
     return full, e.cut_m3, e.fill_m3
 
 
+def profile_derivatives(p: Primitive, x: float, y: float):
+    """Primitive::profile at (x, y) and its derivatives with respect to width and length."""
+    (x0, y0), (x1, y1) = p.segment()
+    vx, vy = x1 - x0, y1 - y0
+    l2 = vx * vx + vy * vy
+    t, end = 0.0, 0
+    if l2 > 0.0:
+        t = ((x - x0) * vx + (y - y0) * vy) / l2
+        if t < 0.0:
+            t, end = 0.0, -1
+        elif t > 1.0:
+            t, end = 1.0, 1
+    px, py = x0 + t * vx - x, y0 + t * vy - y
+    d = math.sqrt(px * px + py * py)
+    half = 0.5 * p.width
+    s = d / half
+    if s >= 1.0:
+        return 0.0, 0.0, 0.0
+    if p.kind == CUT:
+        if s <= 0.5:
+            P, dPds = 1.0, 0.0
+        else:
+            u = (s - 0.5) / 0.5
+            w = 1.0 - u * u
+            P, dPds = w * w, -8.0 * u * w
+    else:
+        w = 1.0 - s * s
+        P, dPds = w * w, -4.0 * s * w
+    dP_dw = dPds * (-s / p.width)
+    dP_dL = 0.0
+    if end != 0 and d > 0.0 and p.kind != MOUND and p.length > 0.0:
+        ex, ey = vx / (2.0 * p.length), vy / (2.0 * p.length)   # d(end point)/dL at the far end
+        dP_dL = dPds * (end * (px * ex + py * ey) / d) / half
+    return P, dP_dw, dP_dL
+
+
+def _prim_box(p: Primitive, geo, nx, ny):
+    x0, y0, x1, y1 = p.bbox()
+    a = min(int(max(math.floor((x0 - geo.origin_x) / geo.dx), 0.0)), nx)
+    b = min(int(max(math.floor((geo.origin_y - y1) / geo.dy), 0.0)), ny)
+    c = min(int(max(math.ceil((x1 - geo.origin_x) / geo.dx), 0.0)), nx)
+    d = min(int(max(math.ceil((geo.origin_y - y0) / geo.dy), 0.0)), ny)
+    return a, b, c, d
+
+
 def primitive_gradient(base, geo, editable, max_abs_dz: float, prims: list[Primitive], gx: np.ndarray, gy: np.ndarray,
                        objective_def=None) -> np.ndarray:
-    """dJ/d(height, width, length) per primitive, shape (len(prims), 3). objective_def (an
-    ObjectiveDef) adds the earthwork term; without it only the asset term is differentiated."""
+    """dJ/d(height, width, length) per primitive, shape (len(prims), 3), from the written-out
+    derivative of the quadrature. objective_def (an ObjectiveDef) adds the earthwork term;
+    without it only the asset term is differentiated."""
     if base.level != 1:
         raise ValueError("the design chain is written for fidelity level 1 (signed faces)")
+    nx, ny = base.nx, base.ny
+    gdz = dz_gradient(base, gx, gy)
+    dz, _, _ = _dz_full(prims, geo, nx, ny, editable, max_abs_dz)
+    lam = 0.0 if objective_def is None else objective_def.earth_weight
+    cc = 0.0 if objective_def is None else objective_def.cut_cost
+    fc = 0.0 if objective_def is None else objective_def.fill_cost
+    area = geo.dx * geo.dy
+    out = np.zeros((len(prims), len(PARAMS)))
+    S = 4
+    for i, p in enumerate(prims):
+        a, b, c, d = _prim_box(p, geo, nx, ny)
+        acc = np.zeros(3)
+        for row in range(b, d):
+            for col in range(a, c):
+                z = dz[row, col]
+                if not editable[row, col] or not (-max_abs_dz < z < max_abs_dz):
+                    continue
+                s0 = s1 = s2 = 0.0
+                for sy in range(S):
+                    for sx in range(S):
+                        x = geo.origin_x + (col + (sx + 0.5) / S) * geo.dx
+                        y = geo.origin_y - (row + (sy + 0.5) / S) * geo.dy
+                        P, dw, dL = profile_derivatives(p, x, y)
+                        s0 += P; s1 += dw; s2 += dL
+                ddz = np.array([s0, p.height * s1, p.height * s2]) / (S * S)
+                we = area * (fc if z > 0.0 else (-cc if z < 0.0 else 0.5 * (fc - cc)))
+                acc += (gdz[row, col] + lam * we) * ddz
+        out[i] = acc
+    return out
+
+
+def primitive_gradient_fd(base, geo, editable, max_abs_dz: float, prims: list[Primitive], gx: np.ndarray, gy: np.ndarray,
+                          objective_def=None) -> np.ndarray:
+    """primitive_gradient by central differences of the f64 materialize (the check)."""
     nx, ny = base.nx, base.ny
     gdz = dz_gradient(base, gx, gy)
     lam = 0.0 if objective_def is None else objective_def.earth_weight

@@ -93,3 +93,42 @@ def polish(solver, params, base, prims, objective, editable, max_abs_dz: float, 
             r *= 0.5
         res.history.append(res.j)
     return res
+
+
+@dataclass
+class IncumbentPolish:
+    """One search generation's incumbent, polished: what polish_population() reports."""
+    population: int              # designs evaluated
+    feasible: int                # of which feasible (guard, volume limit)
+    incumbent: list              # the best feasible design of the population
+    result: PolishResult         # its polish
+    baseline_max: np.ndarray     # the unedited terrain's monitor maxima (guard reference)
+    wall_s: dict                 # wall time of the population run and of the polish
+
+
+def polish_population(solver, params, base, designs, objective, editable, max_abs_dz: float, max_volume=None,
+                      iters: int = 4, checkpoint_interval: int = 256, **kw) -> IncumbentPolish:
+    """The search loop's use of the adjoint for one generation: run the unedited terrain for
+    the guard baseline (Problem::build, crates/itr-opt/src/problem.rs:183-190), evaluate the
+    population of designs (given as primitives) exactly on the device, take the best feasible
+    one (lowest J with no guard violation and within the volume limit: the incumbent an
+    elitist method keeps, crates/itr-opt/src/driver.rs:169) and polish it (polish())."""
+    import time
+    from .terrain import PreparedTerrain
+    monitors = objective.monitors
+    t0 = time.perf_counter()
+    base_run = solver.run_batch(params, [PreparedTerrain(base)], monitors)[0]
+    baseline = np.asarray(base_run.monitor_max, dtype=np.float64)
+    runs, cut, fill = solver.run_primitives(params, base, designs, monitors, editable, max_abs_dz, objective=objective,
+                                            baseline_max=baseline, want_depth=False)
+    t1 = time.perf_counter()
+    ok = [i for i, r in enumerate(runs) if r.feasible and r.status == 0
+          and (max_volume is None or cut[i] + fill[i] <= max_volume)]
+    if not ok:
+        raise RuntimeError("no feasible design in the population")
+    best = min(ok, key=lambda i: runs[i].j)
+    res = polish(solver, params, base, designs[best], objective, editable, max_abs_dz, baseline_max=baseline, iters=iters,
+                 max_volume=max_volume, checkpoint_interval=checkpoint_interval, **kw)
+    t2 = time.perf_counter()
+    return IncumbentPolish(population=len(designs), feasible=len(ok), incumbent=designs[best], result=res,
+                           baseline_max=baseline, wall_s={"population": t1 - t0, "polish": t2 - t1})

@@ -88,6 +88,16 @@ class Scene:
         return out
 
 
+    def primitive_designs(self, n: int, seed: int | None = None, length=(20.0, 100.0), width=(3.0, 8.0),
+                          height=(-0.5, 0.5)):
+        """n seeded random designs as primitive lists, not materialised on the host (the
+        device does it, itr_gpu_run_primitives; the volume limit is applied to the volumes it
+        returns)."""
+        rng = np.random.default_rng(self.design_seed if seed is None else seed)
+        return [random_design(rng, self.n_prims, self.design_box, length=length, width=width, height=height)
+                for _ in range(n)]
+
+
 def _objective(geo, nx, ny, assets, guards, tol, thr=0.05):
     A = [Asset(f"asset{i}", _rect_cells(geo, nx, ny, *r), thr) for i, r in enumerate(assets)]
     G = sorted(set(c for g in guards for c in _rect_cells(geo, nx, ny, *g)))

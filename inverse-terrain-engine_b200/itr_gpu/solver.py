@@ -195,6 +195,7 @@ class GpuRun:
     dj_ddzx2: np.ndarray | None = None  # itr_gpu_vjp_crest: dJ/d(second x-face jump)
     dj_ddzy2: np.ndarray | None = None
     dt_fallback_t: float = -1.0         # locked dt: time of the snapshot the run fell back to (-1: none)
+    rows_skipped: int = 0               # dry rows skipped (RunSummary::rows_skipped)
 
 
 @dataclass
@@ -402,6 +403,7 @@ class GpuSolver:
                                j=float(r.j), feasible=bool(r.feasible), sync_count=int(r.sync_count),
                                rel_residual=float(r.rel_residual), cell_updates=int(r.cell_updates),
                                warm_start_steps=int(r.warm_start_steps), dt_fallback_t=float(r.dt_fallback_t),
+                               rows_skipped=int(r.rows_skipped),
                                dj_ddzx=gx[i] if gx is not None else None, dj_ddzy=gy[i] if gy is not None else None))
         return runs
 

@@ -98,6 +98,76 @@ def test_gradient_vs_f64_finite_differences_smooth(gpu):
     print(f"worst relative error vs f64 central differences: {worst:.3%}")
 
 
+def _fd_check_faces(base, p, t, obj, gx, gy, n_per_dir=3, threads=None):
+    """Central differences of the f64 oracle's J on the faces of largest |gradient| (interior
+    faces; n_per_dir per direction), the runs spread over the host threads. Returns
+    [(kind, index, adjoint, finite difference)]."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    nx, ny = base.nx, base.ny
+    dzx0 = np.asarray(t.dzx, np.float64).reshape(ny, nx + 1)
+    dzy0 = np.asarray(t.dzy, np.float64).reshape(ny + 1, nx)
+    gxi = np.abs(gx.copy()); gxi[:, 0] = 0; gxi[:, nx] = 0
+    gyi = np.abs(gy.copy()); gyi[0, :] = 0; gyi[ny, :] = 0
+    picks = [("x", np.unravel_index(i, gx.shape)) for i in np.argsort(gxi, axis=None)[-n_per_dir:]]
+    picks += [("y", np.unravel_index(i, gy.shape)) for i in np.argsort(gyi, axis=None)[-n_per_dir:]]
+    jobs = []
+    for kind, idx in picks:
+        for sgn in (1.0, -1.0):
+            a = (dzx0 if kind == "x" else dzy0).copy()
+            a[idx] += sgn * FD_STEP_M
+            jobs.append(dict(dzx=a) if kind == "x" else dict(dzy=a))
+    with ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as ex:
+        js = list(ex.map(lambda kw: j_f64(base, p, t, obj, **kw), jobs))
+    out = []
+    for k, (kind, idx) in enumerate(picks):
+        fd = (js[2 * k] - js[2 * k + 1]) / (2 * FD_STEP_M)
+        out.append((kind, idx, (gx if kind == "x" else gy)[idx], fd))
+    return out
+
+
+def config4_case(initial_depth, duration=300.0):
+    """Configuration 4's scene (rolling hills 240 x 192 at 2.5 m, its assets and storm) for the
+    first `duration` seconds of the storm, from `initial_depth` everywhere, one design."""
+    from itr_gpu.scenes import hills_scene
+    sc = hills_scene(2.5, seed=20261203 + 2, design_seed=7 + 4, initial_depth=initial_depth)
+    sc.params.duration_s = duration
+    return sc, sc.designs(1)[0][2]
+
+
+def test_gradient_vs_f64_finite_differences_config4_smooth(gpu):
+    """The required bar at the configured scale: configuration 4's grid (240 x 192), the fully
+    wet smooth sub-case (initial depth 0.3 m, no dry cells), the first 300 s of its storm
+    (3646 steps): dJ/d(face jump) on the six most sensitive faces within 1% of f64 central
+    differences."""
+    sc, t = config4_case(0.3)
+    run = gpu.vjp(sc.params, [t], sc.monitors, sc.objective, checkpoint_interval=128)[0]
+    assert run.status == 0 and run.steps > 3000
+    res = _fd_check_faces(sc.base, sc.params, t, sc.objective, run.dj_ddzx, run.dj_ddzy)
+    worst = 0.0
+    for kind, idx, ad, fd in res:
+        rel = abs(ad - fd) / abs(fd)
+        worst = max(worst, rel)
+        assert rel <= FD_REL_TOL, f"{kind}-face {idx}: adjoint {ad:.6e} vs finite difference {fd:.6e} (rel {rel:.3%})"
+    print(f"\nconfig 4 smooth (240x192, 300 s, {run.steps} steps): worst relative error vs f64 central "
+          f"differences on {len(res)} faces {worst:.3%}")
+
+
+def test_gradient_config4_mixed_wet_dry_reported(gpu):
+    """The mixed wet/dry case at configuration 4's scale (dry start, rain on dry hills, the
+    first 1200 s of the storm), reported beside the smooth one: through wetting fronts the
+    frozen-dt discrete adjoint and f64 finite differences of the adaptive-dt run may part, so
+    only finiteness and the sign on the dominant faces are asserted."""
+    sc, t = config4_case(0.0, 1200.0)
+    run = gpu.vjp(sc.params, [t], sc.monitors, sc.objective, checkpoint_interval=128)[0]
+    assert np.all(np.isfinite(run.dj_ddzx)) and np.all(np.isfinite(run.dj_ddzy))
+    res = _fd_check_faces(sc.base, sc.params, t, sc.objective, run.dj_ddzx, run.dj_ddzy, n_per_dir=2)
+    rels = [abs(ad - fd) / max(abs(fd), 1e-300) for _, _, ad, fd in res]
+    print(f"\nconfig 4 mixed wet/dry (1200 s, {run.steps} steps): relative errors vs f64 central differences "
+          + ", ".join(f"{r:.2%}" for r in rels))
+    assert sum(np.sign(ad) == np.sign(fd) for _, _, ad, fd in res) >= len(res) - 1
+
+
 def test_mixed_wet_dry_gradient_finite(gpu):
     """Dry start (rain on dry ground): the wet/dry branches still give a finite gradient."""
     base, p, t, obj = smooth_case(gpu, initial_depth=0.0, duration=240.0)

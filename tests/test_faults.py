@@ -6,6 +6,12 @@ A cell of NaN or negative initial depth makes its design unhealthy at the first 
 oracle and on the device; the device stops that design alone: the healthy designs of the same
 batch give the oracle's bits. An infinite initial depth (whose first CFL dt would be zero) is
 refused at the C boundary before any device work.
+
+A barrier wait that never completes (a single-CTA design's barrier expecting one arrival
+more than its CTA makes: option stall_wait_test) runs to its bounded limit; the kernel leaves
+its step loop with the whole CTA and the call returns ITR_DEVICE_TIMEOUT, after which the same
+context runs the batch again normally. No GPU fault is involved: the wait is a bounded
+try_wait loop.
 """
 from __future__ import annotations
 
@@ -82,3 +88,25 @@ def test_infinite_initial_depth_refused():
                          [(0.0, 0.0)], sc.monitors)
     finally:
         g.close()
+
+
+@pytest.mark.gpu
+def test_stalled_barrier_wait_times_out_and_context_recovers():
+    from itr_gpu import GpuSolver
+    sc = scene()
+    sc.params.duration_s = 300.0
+    terrs = [t for _, _, t in sc.designs(2)]
+    g = GpuSolver()
+    try:
+        for k, v in (("autotune", 0), ("cluster", 1), ("threads", 256), ("wait_limit", 2000), ("stall_wait_test", 1)):
+            g.set_option(k, v)
+        with pytest.raises(DeviceError, match="wait limit"):
+            g.run_batch(sc.params, terrs, sc.monitors, want_peak=True)
+        g.set_option("stall_wait_test", 0)
+        runs = g.run_batch(sc.params, terrs, sc.monitors, want_peak=True)
+    finally:
+        g.close()
+    for r, t in zip(runs, terrs):
+        o = orc.flat_run(base_arrays(sc.base), design_dict(t, sc.params), sc.params, sc.monitors, want_peak=True)
+        assert r.steps == o["steps"] and r.status == 0
+        assert_bitwise(r.peak.ravel(), o["peak"].ravel(), "after the timeout: per-cell peak")

@@ -129,6 +129,47 @@ def test_polish_incumbent_on_device():
     assert abs(j64 - res.j) <= 1e-3 * abs(j64), (j64, res.j)
 
 
+@pytest.mark.gpu
+def test_polish_config5_incumbent_exact_and_oracle_reruns():
+    """Configuration 5's polish workflow (fractal 1024 x 1024 at 2 m, 6 primitives per design,
+    the first 900 s of its storm, when the assets around their 0.05 m threshold are wet): the
+    best feasible design of a 16-design generation is polished with the device adjoint, every
+    proposal re-evaluated exactly on the device. Then the polished incumbent is rerun: a fresh
+    device run gives its J bits, the f32 oracle its monitor maxima bit for bit, the f64 oracle
+    its J to 1e-3 relative, and it is feasible against the baseline."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    from itr_gpu import GpuSolver
+    from itr_gpu.polish import polish_population
+    from itr_gpu.scenes import config
+    sc = config(5)
+    p = sc.params
+    p.duration_s = 900.0
+    g = GpuSolver()
+    try:
+        r = polish_population(g, p, sc.base, sc.primitive_designs(16), sc.objective, sc.editable, sc.max_abs_dz,
+                              max_volume=sc.max_volume, iters=4)
+        res = r.result
+        assert res.feasible and res.j <= res.j_start, (res.j_start, res.history)
+        runs, cut, fill = g.run_primitives(p, sc.base, [res.prims], sc.objective.monitors, sc.editable, sc.max_abs_dz,
+                                           objective=sc.objective, baseline_max=r.baseline_max)
+        assert runs[0].j == res.j and runs[0].feasible
+    finally:
+        g.close()
+    e = materialize(res.prims, sc.geo, sc.base.nx, sc.base.ny, sc.editable, sc.max_abs_dz)
+    t = PreparedTerrain(sc.base).apply_edit(e)
+    with ThreadPoolExecutor(max_workers=2) as ex:
+        f32 = ex.submit(orc.flat_run, base_arrays(sc.base), design_dict(t, p), p, sc.objective.monitors)
+        f64 = ex.submit(orc.flat_run64, base_arrays(sc.base), design_dict(t, p), p, sc.objective.monitors)
+        o32, o64 = f32.result(), f64.result()
+    np.testing.assert_array_equal(o32["monitor_max"].astype(np.float32), runs[0].monitor_max.astype(np.float32))
+    rep64 = sc.objective.evaluate(o64["monitor_max"], e.cut_m3, e.fill_m3, r.baseline_max)
+    assert abs(rep64["j"] - res.j) <= 1e-3 * abs(rep64["j"]), (rep64["j"], res.j)
+    assert rep64["guard_violation_m"] == 0.0
+    print(f"\nconfig 5 polish: J {res.j_start:.6g} -> {res.j:.6g} ({res.accepted} of {res.evaluations - 1} proposals kept), "
+          f"f64 rerun J {rep64['j']:.6g}; wall {r.wall_s}")
+
+
 def test_quantize_rounds_half_away_from_zero():
     """DesignSpace::q (crates/itr-core/src/design.rs:259-261) rounds with Rust's f64::round,
     half-way cases away from zero (Python's round() would take the even neighbour)."""
