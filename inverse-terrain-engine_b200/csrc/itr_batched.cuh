@@ -407,7 +407,11 @@ ITR_DEV void row_flags(const Smem& sm, int par, int nr, int nr_max, int nx, int 
   }
 }
 
-template <bool CREST, bool CLUSTERED, int MAXT, bool BND, bool LOCKED = false>
+// SKIP: the dry-row test of rain-free steps (kernel.rs:605-612) and the row wetness flags it
+// reads. The host launches the SKIP instantiation when params.skip_dry is set and the storm
+// has a rain-free interval inside the run; every other run has no rain-free step, where the
+// test never skips, and takes the instantiation without the bookkeeping (same results).
+template <bool CREST, bool CLUSTERED, int MAXT, bool BND, bool LOCKED = false, bool SKIP = false>
 __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int C = A.C;
@@ -544,7 +548,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
   if (BND && wid == nwarps - 1) {
     if (lane < P.inflow.n) sm.INF[lane] = inflow_values(P.inflow, lane, t_start, P.g);
     __syncwarp();
-    ghost_row_wet(A.bc, nx, ny, bh, sm.INF, sm.GWF, lane);
+    if (SKIP) ghost_row_wet(A.bc, nx, ny, bh, sm.INF, sm.GWF, lane);
   }
   {
     double sw = s0_l;
@@ -554,7 +558,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     if (lane == 0) { sm.red[wid * 8 + 0] = sw; sm.red[wid * 8 + 1] = vw; }
   }
   if (CLUSTERED) { cluster_arrive(); cluster_wait(); } else __syncthreads();
-  row_flags(sm, 0, nr, nr_max, nx, W, wid, nwarps, lane);   // wetness of the initial state (parity 0)
+  if (SKIP) row_flags(sm, 0, nr, nr_max, nx, W, wid, nwarps, lane);   // wetness of the initial state (parity 0)
   double s0 = 0.0, v0 = 0.0;
   for (int qq = 0; qq < C; ++qq) {
     const double* rr = CLUSTERED ? remote(sm.red, qq) : sm.red;
@@ -650,10 +654,13 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
           if (BND && wid == nwarps - 1) {
             if (lane < P.inflow.n) sm.INF[(int)(step & 1ull) * kMaxInflow + lane] = inflow_values(P.inflow, lane, t, P.g);
             __syncwarp();
-            ghost_row_wet(A.bc, nx, ny, bh, sm.INF + (int)(step & 1ull) * kMaxInflow, sm.GWF + (int)(step & 1ull) * (ny + 2), lane);
+            if (SKIP)
+              ghost_row_wet(A.bc, nx, ny, bh, sm.INF + (int)(step & 1ull) * kMaxInflow, sm.GWF + (int)(step & 1ull) * (ny + 2), lane);
           }
-          __syncthreads();   // the restored rows complete before their flags are taken
-          row_flags(sm, (int)(step & 1ull), nr, nr_max, nx, W, wid, nwarps, lane);
+          if (SKIP) {
+            __syncthreads();   // the restored rows complete before their flags are taken
+            row_flags(sm, (int)(step & 1ull), nr, nr_max, nx, W, wid, nwarps, lane);
+          }
           if (q == 0 && tid == 0) A.fallback_t[d] = t;
           locked_live = false;
           gs.full();   // the restored state of every CTA visible before the next step
@@ -671,8 +678,10 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       // closing barrier; the other slot's readers finished before the previous one)
       if (wid == nwarps - 1) {
         if (lane < P.inflow.n) sm.INF[(sp ^ 1) * kMaxInflow + lane] = inflow_values(P.inflow, lane, pl.t_new, P.g);
-        __syncwarp();
-        ghost_row_wet(A.bc, nx, ny, bh, sm.INF + (sp ^ 1) * kMaxInflow, sm.GWF + (sp ^ 1) * (ny + 2), lane);
+        if (SKIP) {
+          __syncwarp();
+          ghost_row_wet(A.bc, nx, ny, bh, sm.INF + (sp ^ 1) * kMaxInflow, sm.GWF + (sp ^ 1) * (ny + 2), lane);
+        }
       }
     }
     float smax_l = 0.0f, infil_l = 0.0f, fix_l = 0.0f;
@@ -734,7 +743,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     // CTA's band through DSMEM) and no stage or inflow ghost of theirs holds water. Its faces
     // are exactly 0 and its cells keep their zero state: skipping changes no result. The
     // decision depends only on shared flags, so every warp of a strip takes it alike.
-    const bool try_skip = P.skip_dry && !(k.rain > 0.0f);
+    const bool try_skip = SKIP && !(k.rain > 0.0f);
     auto row_dry = [&](int j) -> bool {   // grid row j in [-1, ny]
       bool dr = !BND || sm.GWF[sp * (ny + 2) + j + 1] == 0;
       if (j < 0 || j >= ny) return dr;
@@ -749,8 +758,18 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       for (int w = 0; w < W; ++w) dr = dr && e[w] == 0;
       return dr;
     };
-    bool d_m1 = false, d_0 = false, d_1 = false;
-    if (try_skip && L > 0) { d_m1 = row_dry(r0 - 1); d_0 = row_dry(r0); d_1 = row_dry(r0 + 1); }
+    // Bit i of dmask: grid row r0 - 1 + mbase + i is dry, for the rows up to r0 + L, one row
+    // per lane and ballot (64 rows per fill; a strip longer than 61 rows refills as it goes).
+    unsigned long long dmask = 0ull;
+    int mbase = 0;
+    auto fill_mask = [&](int from) {
+      const int ja = r0 - 1 + from + lane, jb = ja + 32, jmax = r0 + L;
+      const bool da = ja <= jmax && row_dry(ja);
+      const bool db = jb <= jmax && row_dry(jb);
+      dmask = (unsigned long long)__ballot_sync(0xffffffffu, da) | ((unsigned long long)__ballot_sync(0xffffffffu, db) << 32);
+      mbase = from;
+    };
+    if (try_skip && L > 0) fill_mask(0);
 
     // ---- row sweep ----
 #pragma unroll 1
@@ -760,10 +779,10 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       const bool last = (p == L - 1);
       bool skip = false, skip_next = false;
       if (try_skip) {
-        const bool d_2 = !last && row_dry(r + 2);
-        skip = d_m1 && d_0 && d_1;
-        skip_next = !last && d_0 && d_1 && d_2;
-        d_m1 = d_0; d_0 = d_1; d_1 = d_2;
+        if (p - mbase > 60) fill_mask(p);
+        const int i = p - mbase;   // bits i, i + 1, i + 2: rows r - 1, r, r + 1
+        skip = ((dmask >> i) & 7ull) == 7ull;
+        skip_next = !last && ((dmask >> (i + 1)) & 7ull) == 7ull;
       }
       if (last) gs.b1_wait();
       if (!last) prefetch_row(r + 1, (p + 1) & 1);
@@ -780,7 +799,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
       const bool bottom = last && s + 1 >= S && q + 1 >= C;
       Cell2 nxt{};
       Face2 fS{}, fWn{};
-      if (skip) {   // a dry row between dry rows: zero faces, nothing to update
+      if (SKIP && skip) {   // a dry row between dry rows: zero faces, nothing to update
         if (!last && !skip_next) {   // the next row's west faces
           nxt = load_pair(lr + 1, r + 1);
           const Cell2 left = left_pair(nxt, lr + 1, r + 1);
@@ -891,7 +910,7 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
         infil_l += o.infil.y;
         fix_l += o.fix.y;
       }
-      {   // the warp's columns of this row hold water in the new state (read next step)
+      if (SKIP) {   // the warp's columns of this row hold water in the new state (read next step)
         const bool wet_any = __any_sync(0xffffffffu, (cell0 && o.h.x > 0.0f) || (cell1 && o.h.y > 0.0f));
         if (lane == 0) sm.WF[((size_t)(sp ^ 1) * nr_max + lr) * W + wis] = wet_any ? 1 : 0;
       }
@@ -1080,7 +1099,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_batched(const BatchArgs A) {
     o.lower_bound = lower_bound; o.v0 = v0; o.volume = volume; o.rel_residual = rel_res;
     o.n_rows = n_rows; o.pad = 0;
     unsigned long long tot_skip = 0ull;
-    for (int qq = 0; qq < C; ++qq) tot_skip += CLUSTERED ? *remote(sm.NSK, qq) : *sm.NSK;
+    if (SKIP)
+      for (int qq = 0; qq < C; ++qq) tot_skip += CLUSTERED ? *remote(sm.NSK, qq) : *sm.NSK;
     o.rows_skipped = tot_skip;
     A.out[d] = o;
   }

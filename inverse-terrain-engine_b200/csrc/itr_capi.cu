@@ -21,6 +21,7 @@
 #include "../../include/itr_gpu.h"
 #include "itr_device.cuh"
 #include "itr_batched.cuh"
+#include "itr_batched_table.cuh"
 #include "itr_plain.cuh"
 #include "itr_band.cuh"
 #include "itr_adjoint.cuh"
@@ -207,25 +208,19 @@ static int fail(itr_ctx* c, int code, const char* fmt, ...) {
 constexpr unsigned long long kMaxSteps = 2000000000ull;
 
 // ------------------------------------------------------------------ kernels table ----
-typedef void (*BatchedFn)(const BatchArgs);
+#ifdef ITR_CHECKED
+namespace itr {
+ITR_BATCHED_TABLE(batched_fn_00, false, false)
+ITR_BATCHED_TABLE(batched_fn_01, false, true)
+ITR_BATCHED_TABLE(batched_fn_10, true, false)
+ITR_BATCHED_TABLE(batched_fn_11, true, true)
+}  // namespace itr
+#endif
 
-static BatchedFn batched_fn(bool crest, bool clustered, int maxt, bool bnd, bool locked = false) {
-#define PICK(CR, CL, BD, LK)                                          \
-  if (maxt <= 256) return k_batched<CR, CL, 256, BD, LK>;             \
-  if (maxt <= 512) return k_batched<CR, CL, 512, BD, LK>;             \
-  if (maxt <= 768) return k_batched<CR, CL, 768, BD, LK>;             \
-  return k_batched<CR, CL, 1024, BD, LK>;
-#define PICK4(LK)                                                                                  \
-  if (bnd) {                                                                                       \
-    if (crest) { if (clustered) { PICK(true, true, true, LK) } else { PICK(true, false, true, LK) } } \
-    else { if (clustered) { PICK(false, true, true, LK) } else { PICK(false, false, true, LK) } }    \
-  }                                                                                                \
-  if (crest) { if (clustered) { PICK(true, true, false, LK) } else { PICK(true, false, false, LK) } } \
-  else { if (clustered) { PICK(false, true, false, LK) } else { PICK(false, false, false, LK) } }
-  if (locked) { PICK4(true) }
-  PICK4(false)
-#undef PICK4
-#undef PICK
+// skip: the dry-row instantiation (RunParams::skip_dry, set only when a rain-free step can occur)
+static BatchedFn batched_fn(bool crest, bool clustered, int maxt, bool bnd, bool locked = false, bool skip = false) {
+  if (crest) return bnd ? batched_fn_11(clustered, maxt, locked, skip) : batched_fn_10(clustered, maxt, locked, skip);
+  return bnd ? batched_fn_01(clustered, maxt, locked, skip) : batched_fn_00(clustered, maxt, locked, skip);
 }
 
 static int maxt_bucket(int T) { return T <= 256 ? 256 : T <= 512 ? 512 : T <= 768 ? 768 : 1024; }
@@ -252,7 +247,7 @@ static LaunchCfg make_cfg(const itr_ctx* ctx, int nx, int ny, int C, int T_targe
 
 static int launch_batched(itr_ctx* ctx, const BatchArgs& A, const LaunchCfg& cfg, int n_designs, bool set_attr = true) {
   const bool crest = A.mode == 1, clustered = cfg.C > 1;
-  BatchedFn fn = batched_fn(crest, clustered, maxt_bucket(cfg.T), cfg.bnd, A.locked_dt != nullptr);
+  BatchedFn fn = batched_fn(crest, clustered, maxt_bucket(cfg.T), cfg.bnd, A.locked_dt != nullptr, A.P.skip_dry != 0);
   if (set_attr) CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   cudaLaunchConfig_t lc;
   memset(&lc, 0, sizeof(lc));
@@ -418,6 +413,23 @@ static int check_inputs(itr_ctx* ctx, const itr_params* p, const itr_grid* g, in
   return ITR_OK;
 }
 
+// The storm's rate (linear between breakpoints, constant before the first and after the last)
+// is 0 over an interval of positive length inside [0, duration], so a step of the run can be
+// rain-free. Unsorted breakpoints: conservatively true. (A step inside a storm that is positive
+// almost everywhere has a mean rate > 0 unless it is shorter than about 1e-30 s.)
+static bool rain_free_stretch(const RunParams& P) {
+  const Rain& R = P.rain;
+  const double T = P.duration;
+  if (R.n == 0 || !P.rain_sorted) return true;
+  if (R.r[0] <= 0.0 && R.t[0] > 0.0) return true;
+  if (R.r[R.n - 1] <= 0.0 && R.t[R.n - 1] < T) return true;
+  for (int k = 0; k + 1 < R.n; ++k) {
+    const double a = R.t[k] > 0.0 ? R.t[k] : 0.0, b = R.t[k + 1] < T ? R.t[k + 1] : T;
+    if (R.r[k] <= 0.0 && R.r[k + 1] <= 0.0 && a < b) return true;
+  }
+  return false;
+}
+
 static RunParams make_run_params(const itr_params* p, const itr_grid* g) {
   RunParams P;
   memset(&P, 0, sizeof(P));
@@ -430,6 +442,10 @@ static RunParams make_run_params(const itr_params* p, const itr_grid* g) {
   for (int i = 0; i < p->n_rain; ++i) { P.rain.t[i] = p->rain_t[i]; P.rain.r[i] = p->rain_rate[i]; }
   P.rain_sorted = 1;
   for (int i = 1; i < p->n_rain; ++i) if (!(p->rain_t[i] >= p->rain_t[i - 1])) P.rain_sorted = 0;
+  // Dry-row skipping can act only on a step without rain: keep it on only when the storm has
+  // a rain-free stretch inside the run (no skipping is possible otherwise, and the kernels
+  // then leave out its bookkeeping; the results are the same either way).
+  if (P.skip_dry && !rain_free_stretch(P)) P.skip_dry = 0;
   P.g_f = (float)g->g; P.g_half_f = (float)(0.5 * g->g);
   P.inv_dx_f = (float)(1.0 / g->dx); P.inv_dy_f = (float)(1.0 / g->dy);
   P.h_dry_f = (float)p->h_dry; P.heps2_f = (float)(p->h_eps * p->h_eps); P.q_min_f = (float)1e-30;
@@ -1490,7 +1506,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
         ctx->locked_run = true;
       }
       if (ctx->defer) {   // ladder group: the launch goes into the ladder's graph
-        BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T), cfg.bnd);
+        BatchedFn fn = batched_fn(crest, cfg.C > 1, maxt_bucket(cfg.T), cfg.bnd, A.locked_dt != nullptr, A.P.skip_dry != 0);
         CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
         ctx->last_args = A; ctx->last_cfg = cfg; ctx->have_last = true;
         ctx->last_was_plain = false; ctx->last_was_tiled = false;
@@ -1650,7 +1666,8 @@ extern "C" int itr_gpu_run_ladder(itr_ctx* ctx, const itr_params* p, int32_t n_g
       itr_ctx* c = ctx->children[gi];
       if (!c->pending_ok) continue;
       const LaunchCfg& cf = c->last_cfg;
-      BatchedFn fn = batched_fn(c->last_args.mode == 1, cf.C > 1, maxt_bucket(cf.T), cf.bnd, c->last_args.locked_dt != nullptr);
+      BatchedFn fn = batched_fn(c->last_args.mode == 1, cf.C > 1, maxt_bucket(cf.T), cf.bnd, c->last_args.locked_dt != nullptr,
+                                c->last_args.P.skip_dry != 0);
       bool found = false;
       for (auto& e : need) if (e.first == fn) { e.second = std::max(e.second, cf.smem); found = true; }
       if (!found) need.push_back({fn, cf.smem});

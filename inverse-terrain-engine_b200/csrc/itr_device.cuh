@@ -593,13 +593,15 @@ ITR_DEV float2 fma2(float2 a, float2 b, float2 c) {
 // kernel's reciprocals (HLL denominator, friction, velocity) are in range for every
 // healthy state: the fallback is for NaN/infinite states and for checking.
 ITR_DEV float rcp_est(float x) { float r; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
-ITR_DEV unsigned rcp_out(float x) { return (((__float_as_uint(x) >> 23) & 0xffu) - 2u) > 250u ? 1u : 0u; }
+// In range: |x| in [2^-125, 2^126), i.e. biased exponent 2 .. 252. Two compares of |x| (the
+// absolute value is an operand modifier); NaN, zero and infinity fail them.
+ITR_DEV bool rcp_in(float x) { return fabsf(x) >= 0x1p-125f && fabsf(x) < 0x1p126f; }
 
 ITR_DEV float2 rcp2f(float2 x, unsigned exact) {
   const float2 y = make_float2(rcp_est(x.x), rcp_est(x.y));
   const float2 e = fma2(neg2(x), y, f2(1.0f));
   float2 r = fma2(y, e, y);
-  if (__any_sync(0xffffffffu, rcp_out(x.x) | rcp_out(x.y) | exact)) r = rcp2(x);
+  if (__any_sync(0xffffffffu, !(rcp_in(x.x) && rcp_in(x.y)) || exact)) r = rcp2(x);
   return r;
 }
 // canon (a == 0 ? +0 : a) as one paired add of +0: x + 0 is x for every x except -0, which
