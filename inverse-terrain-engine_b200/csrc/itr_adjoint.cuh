@@ -58,6 +58,7 @@ struct AdjArgs {
   const float* seed_w;                //   w_k sigmoid((P_k - eta_k) / tau)
   const int* seed_n;                  // per design
   int max_seeds;
+  int band_rows;                      // k_adj_band: rows per band (1 .. 32)
 };
 
 // Padded cell (gx, gy) of a state [3][N] with ghost cells (boundary.rs:36-87), as plain_load:

@@ -23,6 +23,8 @@
 //     block barrier is the final reduction of the per-block partials.
 // Outputs are k_plain_update's: the new plane, PK (and the argmax state index tpk), the
 // per-block partials [kPart] in the finalize's layout, and the atomic smax / bad words.
+// TAPE: the adjoint's replay of a recorded step (itr_adjoint_band.cuh): the same update, writing
+// only the new plane (no peaks, partials, CFL maximum, health word or row flags).
 #pragma once
 #include <cmath>
 #include "itr_plain.cuh"
@@ -141,7 +143,7 @@ ITR_DEV Raw2 band_row(const PlainArgs& A, const PlainDesign& D, const float2* in
 // jumps of row r + 1, wet and g n^2 of row r.
 struct RowIn { float2 dys, dys2, dxn, dxn2, wet, gn2, pk; };
 
-template <bool CREST, bool BND>
+template <bool CREST, bool BND, bool TAPE = false>
 __global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) {
   __shared__ float4 edge_w[kBandWarps][kBandRows], edge_e[kBandWarps][kBandRows];
   __shared__ float wmax[kBandWarps];
@@ -156,7 +158,8 @@ __global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) 
   const bool hits = cl.pl.hits;
   const double dt_dy = cl.pl.dt * A.P.dy;
   const int nx = A.nx, ny = A.ny, nxp1 = nx + 1;
-  const size_t N = (size_t)nx * ny, pin = (size_t)par * N, pout = (size_t)(par ^ 1) * N;
+  const size_t N = (size_t)nx * ny, plane = A.plane_stride ? A.plane_stride : N;
+  const size_t pin = (size_t)par * plane, pout = (size_t)(par ^ 1) * plane;
   const float2* inf = cl.inf;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const int ns = (nx + 63) / 64;
@@ -178,12 +181,33 @@ __global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) 
   bool bad_l = false;
 
   if (seg) {
-    // ---- pre-pass: the segment's two edge x-faces of every row of the band ----
+    // Dry-row skipping (kernel.rs:605-612): with no rain this step, grid row r is skipped when
+    // padded rows r, r + 1, r + 2 (grid rows r - 1, r, r + 1 and their ghosts) held no water
+    // in the old state. Its faces are then exactly 0 and its cells keep their (zero) state, so
+    // skipping changes no result. Bit p of skipm: grid row r0 + p; bit i of m: padded row r0 + i.
+    unsigned long long skipm = 0ull;
+    const unsigned* rw_old = D.rowwet ? D.rowwet + (size_t)par * (ny + 2) : nullptr;
+    unsigned* rw_new = D.rowwet ? D.rowwet + (size_t)(par ^ 1) * (ny + 2) : nullptr;
+    if (!TAPE && rw_old && A.P.skip_dry && !(k.rain > 0.0f)) {
+      const int ja = r0 + lane, jb = r0 + 32 + lane;
+      const bool da = ja <= ny + 1 && plain_row_dry(rw_old, D.gwet, ja);
+      const bool db = lane < 2 && jb <= ny + 1 && plain_row_dry(rw_old, D.gwet, jb);
+      const unsigned long long m =
+          (unsigned long long)__ballot_sync(0xffffffffu, da) | ((unsigned long long)__ballot_sync(0xffffffffu, db) << 32);
+      skipm = m & (m >> 1) & (m >> 2);
+    }
+    // Rows the sweep needs: row p is updated unless skipped, and its state and inputs are also
+    // read for the next row's west faces; need(p) is false when rows p and p + 1 (or the band's
+    // end) are both skipped, and then nothing of row p is loaded.
+    auto skipped = [&](int p) -> bool { return p >= L || ((skipm >> p) & 1ull); };
+    auto need = [&](int p) -> bool { return !(skipped(p) && skipped(p + 1)); };
+    // ---- pre-pass: the segment's two edge x-faces of every row of the band (skipped rows:
+    //      zero faces, which they are) ----
     {
       const int r = r0 + lane;
       Raw2 lf, rt;
       float2 d0 = f2(0.0f), d1 = f2(0.0f);
-      if (r < r1) {
+      if (r < r1 && !skipped(lane)) {
         band_cell<BND>(A, D, inf, pin, r, cw - 1, lf.h.x, lf.qx.x, lf.qy.x);
         band_cell<BND>(A, D, inf, pin, r, cw, rt.h.x, rt.qx.x, rt.qy.x);
         if (ce <= nx) {
@@ -204,11 +228,11 @@ __global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) 
       edge_w[wid][lane] = f4(fx_(f));
       edge_e[wid][lane] = f4(fy_(f));
       // x_boundary (kernel.rs:435-450): the west domain face of every row, per face
-      if (s == 0 && r < r1) {
+      if (!TAPE && s == 0 && r < r1) {
         const double vw = (double)f.m.x * dt_dy;
         if (vw > 0.0) acc_in += vw; else acc_out -= vw;
       }
-      if (ce == nx && r < r1) {   // the east domain face is this segment's edge
+      if (!TAPE && ce == nx && r < r1) {   // the east domain face is this segment's edge
         const double ve = (double)f.m.y * dt_dy;
         if (ve > 0.0) acc_out += ve; else acc_in -= ve;
       }
@@ -232,13 +256,13 @@ __global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) 
       if (vec) {   // 8-byte aligned pairs (even nx, both columns in the grid)
         q.wet = *reinterpret_cast<const float2*>(A.wet + ci);
         q.gn2 = *reinterpret_cast<const float2*>(A.gn2 + ci);
-        q.pk = *reinterpret_cast<const float2*>(D.PK + ci);
+        q.pk = TAPE ? f2(0.0f) : *reinterpret_cast<const float2*>(D.PK + ci);
         q.dys = *reinterpret_cast<const float2*>(dzy + fy);
       } else {
         q.dys = make_float2(v0 ? dzy[fy] : 0.0f, v1 ? dzy[fy + 1] : 0.0f);
         q.wet = make_float2(v0 ? A.wet[ci] : 0.0f, v1 ? A.wet[ci + 1] : 0.0f);
         q.gn2 = make_float2(v0 ? A.gn2[ci] : 0.0f, v1 ? A.gn2[ci + 1] : 0.0f);
-        q.pk = make_float2(v0 ? D.PK[ci] : 0.0f, v1 ? D.PK[ci + 1] : 0.0f);
+        q.pk = TAPE ? f2(0.0f) : make_float2(v0 ? D.PK[ci] : 0.0f, v1 ? D.PK[ci + 1] : 0.0f);
       }
       return q;
     };
@@ -260,9 +284,9 @@ __global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) 
     };
     // the row above the band (old state; the north ghost row at the domain edge) and row r0
     const bool int_lane = interior;
-    Cell2 cur, nxt;
-    Face2 fN, fW;
-    {
+    Cell2 cur{}, nxt{};
+    Face2 fN{}, fW{};
+    if (!skipped(0)) {
       const Raw2 ta = band_row<BND>(A, D, inf, pin, r0 - 1, c0, int_lane && r0 > 0);
       const Raw2 ca = band_row<BND>(A, D, inf, pin, r0, c0, int_lane);
       const Cell2 top = cells_of(ta.h, ta.qx, ta.qy, k);
@@ -274,44 +298,38 @@ __global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) 
       const float2 dx1 = CREST ? make_float2(c0 <= nx ? D.dzx2[c0 + fx] : 0.0f, c1 <= nx ? D.dzx2[c0 + fx + 1] : 0.0f) : f2(0.0f);
       fN = face2<false, CREST>(top.h, top.u, top.v, top.c, cur.h, cur.u, cur.v, cur.c, dy0, dy1, k);
       fW = xfaces(cur, dx0, dx1, 0);
-      if (r0 == 0) {   // y_boundary top (kernel.rs:452-472): summed over the row first
+      if (!TAPE && r0 == 0) {   // y_boundary top (kernel.rs:452-472): summed over the row first
         ytop += (v0 ? (double)fN.m.x : 0.0) + (v1 ? (double)fN.m.y : 0.0);
       }
     }
-    // Dry-row skipping (kernel.rs:605-612): with no rain this step, grid row r is skipped when
-    // padded rows r, r + 1, r + 2 (grid rows r - 1, r, r + 1 and their ghosts) held no water
-    // in the old state. Its faces are then exactly 0 and its cells keep their (zero) state, so
-    // skipping changes no result. Bit p of skipm: grid row r0 + p; bit i of m: padded row r0 + i.
-    unsigned long long skipm = 0ull;
-    const unsigned* rw_old = D.rowwet ? D.rowwet + (size_t)par * (ny + 2) : nullptr;
-    unsigned* rw_new = D.rowwet ? D.rowwet + (size_t)(par ^ 1) * (ny + 2) : nullptr;
-    if (rw_old && A.P.skip_dry && !(k.rain > 0.0f)) {
-      const int ja = r0 + lane, jb = r0 + 32 + lane;
-      const bool da = ja <= ny + 1 && plain_row_dry(rw_old, D.gwet, ja);
-      const bool db = lane < 2 && jb <= ny + 1 && plain_row_dry(rw_old, D.gwet, jb);
-      const unsigned long long m =
-          (unsigned long long)__ballot_sync(0xffffffffu, da) | ((unsigned long long)__ballot_sync(0xffffffffu, db) << 32);
-      skipm = m & (m >> 1) & (m >> 2);
+    RowIn in{};
+    Raw2 raw{};
+    if (need(0)) {
+      in = load_in(r0);
+      raw = band_row<BND>(A, D, inf, pin, r0 + 1, c0, int_lane && r0 + 1 < ny);
     }
-    RowIn in = load_in(r0);
-    Raw2 raw = band_row<BND>(A, D, inf, pin, r0 + 1, c0, int_lane && r0 + 1 < ny);
 #pragma unroll 1
     for (int p = 0; p < L; ++p) {
       const int r = r0 + p;
       const RowIn q = in;
-      const bool skip = (skipm >> p) & 1ull;
-      const bool skip_next = p + 1 >= L || ((skipm >> (p + 1)) & 1ull);
-      if (!(skip && skip_next)) nxt = cells_of(raw.h, raw.qx, raw.qy, k);
-      if (p + 1 < L) {   // next row's operands, in flight while this row is updated
+      const bool skip = skipped(p);
+      if (need(p)) nxt = cells_of(raw.h, raw.qx, raw.qy, k);
+      if (p + 1 < L && need(p + 1)) {   // next row's operands, in flight while this row is updated
         in = load_in(r + 1);
         raw = band_row<BND>(A, D, inf, pin, r + 2, c0, int_lane && r + 2 < ny);
       }
       Face2 fWn{};
-      if (p + 1 < L && !((skipm >> (p + 1)) & 1ull)) fWn = xfaces(nxt, q.dxn, q.dxn2, p + 1);
+      if (!skipped(p + 1)) fWn = xfaces(nxt, q.dxn, q.dxn2, p + 1);
       if (skip) {   // a dry row between dry rows: zero faces, the (zero) state carried over
         const size_t ci = (size_t)r * nx + c0;
-        if (v0) { D.H[pout + ci] = 0.0f; D.QX[pout + ci] = 0.0f; D.QY[pout + ci] = 0.0f; }
-        if (v1) { D.H[pout + ci + 1] = 0.0f; D.QX[pout + ci + 1] = 0.0f; D.QY[pout + ci + 1] = 0.0f; }
+        if (vec) {
+          *reinterpret_cast<float2*>(D.H + pout + ci) = f2(0.0f);
+          *reinterpret_cast<float2*>(D.QX + pout + ci) = f2(0.0f);
+          *reinterpret_cast<float2*>(D.QY + pout + ci) = f2(0.0f);
+        } else {
+          if (v0) { D.H[pout + ci] = 0.0f; D.QX[pout + ci] = 0.0f; D.QY[pout + ci] = 0.0f; }
+          if (v1) { D.H[pout + ci + 1] = 0.0f; D.QX[pout + ci + 1] = 0.0f; D.QY[pout + ci + 1] = 0.0f; }
+        }
         cur = nxt; fN = Face2{}; fW = fWn;
         continue;
       }
@@ -337,30 +355,33 @@ __global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) 
         if (v0) { D.H[pout + ci] = o.h.x; D.QX[pout + ci] = o.qx.x; D.QY[pout + ci] = o.qy.x; }
         if (v1) { D.H[pout + ci + 1] = o.h.y; D.QX[pout + ci + 1] = o.qx.y; D.QY[pout + ci + 1] = o.qy.y; }
       }
-      if (v0) {
-        if (o.h.x > q.pk.x) { D.PK[ci] = o.h.x; if (D.tpk) D.tpk[ci] = (unsigned)(cl.step + 1); }
-        smax_l = rmax(smax_l, o.s.x);
-        bad_l = bad_l || o.bad.x;
+      if constexpr (!TAPE) {
+        if (v0) {
+          if (o.h.x > q.pk.x) { D.PK[ci] = o.h.x; if (D.tpk) D.tpk[ci] = (unsigned)(cl.step + 1); }
+          smax_l = rmax(smax_l, o.s.x);
+          bad_l = bad_l || o.bad.x;
+        }
+        if (v1) {
+          if (o.h.y > q.pk.y) { D.PK[ci + 1] = o.h.y; if (D.tpk) D.tpk[ci + 1] = (unsigned)(cl.step + 1); }
+          smax_l = rmax(smax_l, o.s.y);
+          bad_l = bad_l || o.bad.y;
+        }
+        // row partials: f32 over the lane's pair, f64 across rows
+        infil_l += (double)((v0 ? o.infil.x : 0.0f) + (v1 ? o.infil.y : 0.0f));
+        fix_l += (double)((v0 ? o.fix.x : 0.0f) + (v1 ? o.fix.y : 0.0f));
+        if (hits) vol += (v0 ? (double)o.h.x : 0.0) + (v1 ? (double)o.h.y : 0.0);
+        if (last_seg) {   // x_boundary: the east domain face inside this segment (kernel.rs:435-450)
+          if (c0 == nx - 1) { const double ve = (double)fE.m.x * dt_dy; if (ve > 0.0) acc_out += ve; else acc_in -= ve; }
+          if (c1 == nx - 1) { const double ve = (double)fE.m.y * dt_dy; if (ve > 0.0) acc_out += ve; else acc_in -= ve; }
+        }
+        if (r == ny - 1) ybot += (v0 ? (double)fS.m.x : 0.0) + (v1 ? (double)fS.m.y : 0.0);
+        if (rw_new && __any_sync(0xffffffffu, (v0 && o.h.x > 0.0f) || (v1 && o.h.y > 0.0f)) && lane == 0)
+          rw_new[r + 1] = 1u;   // the row holds water in the new state (every writer stores 1)
       }
-      if (v1) {
-        if (o.h.y > q.pk.y) { D.PK[ci + 1] = o.h.y; if (D.tpk) D.tpk[ci + 1] = (unsigned)(cl.step + 1); }
-        smax_l = rmax(smax_l, o.s.y);
-        bad_l = bad_l || o.bad.y;
-      }
-      // row partials: f32 over the lane's pair, f64 across rows
-      infil_l += (double)((v0 ? o.infil.x : 0.0f) + (v1 ? o.infil.y : 0.0f));
-      fix_l += (double)((v0 ? o.fix.x : 0.0f) + (v1 ? o.fix.y : 0.0f));
-      if (hits) vol += (v0 ? (double)o.h.x : 0.0) + (v1 ? (double)o.h.y : 0.0);
-      if (last_seg) {   // x_boundary: the east domain face inside this segment (kernel.rs:435-450)
-        if (c0 == nx - 1) { const double ve = (double)fE.m.x * dt_dy; if (ve > 0.0) acc_out += ve; else acc_in -= ve; }
-        if (c1 == nx - 1) { const double ve = (double)fE.m.y * dt_dy; if (ve > 0.0) acc_out += ve; else acc_in -= ve; }
-      }
-      if (r == ny - 1) ybot += (v0 ? (double)fS.m.x : 0.0) + (v1 ? (double)fS.m.y : 0.0);
-      if (rw_new && __any_sync(0xffffffffu, (v0 && o.h.x > 0.0f) || (v1 && o.h.y > 0.0f)) && lane == 0)
-        rw_new[r + 1] = 1u;   // the row holds water in the new state (every writer stores 1)
       cur = nxt; fN = fS; fW = fWn;
     }
   }
+  if constexpr (TAPE) return;
   // ---- block reduction into the finalize's partials (fixed order) ----
   const float m = warp_max_f(smax_l);
   const unsigned b = __any_sync(0xffffffffu, bad_l) ? 1u : 0u;

@@ -25,6 +25,7 @@
 #include "itr_plain.cuh"
 #include "itr_band.cuh"
 #include "itr_adjoint.cuh"
+#include "itr_adjoint_band.cuh"
 #include "itr_design.cuh"
 #include "itr_render.cuh"
 #include "itr_raymarch.cuh"
@@ -127,6 +128,7 @@ struct itr_ctx {
   int autotune = 1, autotune_top = 6, probe_steps = 200;
   int exact_special = 0;
   int band = 1;           // tiled path update kernel: 1 = row-band sweep (k_band), 0 = 16x16 tiles
+  int adj_band = 1;       // adjoint replay and backward step: 1 = row-band sweeps, 0 = 16x16 tiles
   unsigned wait_limit = 1u << 22;   // bounded barrier wait of single-CTA designs (try_wait rounds)
   int stall_wait_test = 0;          // test of the timeout path: that wait never completes
   float tune_ms = 0.0f;
@@ -146,6 +148,7 @@ struct itr_ctx {
   DevBuf tRow, tGw, tSnapRow;   // row-band path: dry-row flags, ghost wetness, flags at the locked snapshot
   // adjoint: argmax states, (dt, rain) ring, checkpoints, tape, adjoint state, gradients
   DevBuf aTpk, aRing, aTape, aTape2, aLA, aLB, aGx, aGy, aGx2, aGy2, aSeg, aNst, aSeedC, aSeedS, aSeedW, aSeedN, aTmon;
+  DevBuf aPlan[2];   // row-band replay: the control blocks of each tape's segment, [K][n]
   cudaStream_t stream2 = nullptr;   // adjoint: the replay of the next segment runs beside the backward steps
   cudaEvent_t ev_rep[2] = {nullptr, nullptr}, ev_adj[2] = {nullptr, nullptr}, ev_bwd = nullptr;
   HostBuf aRingH;
@@ -617,6 +620,7 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   else if (k == "exact_special") ctx->exact_special = value != 0;
   else if (k == "warm_start") ctx->warm_start = value != 0;
   else if (k == "band") ctx->band = value != 0;
+  else if (k == "adj_band") ctx->adj_band = value != 0;
   else if (k == "wait_limit") { if (value < 1 || value > 0x7fffffff) return fail(ctx, ITR_INVALID_ARG, "wait_limit out of range"); ctx->wait_limit = (unsigned)value; }
   else if (k == "stall_wait_test") ctx->stall_wait_test = value != 0;
   else if (k == "probe_steps") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "probe_steps must be >= 1"); ctx->probe_steps = (int)value; }
@@ -935,6 +939,23 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   const cudaStream_t s2 = ctx->stream2;
   CU(cudaEventRecord(ctx->ev_bwd, st));   // the set-up above, before the first replay
   CU(cudaStreamWaitEvent(s2, ctx->ev_bwd, 0));
+  // Row-band replay: k_band<..., TAPE> over the tape, slot j to slot j + 1, with the control
+  // blocks k_adj_plan writes for the segment (one buffer per tape).
+  const bool adj_band = ctx->adj_band != 0;
+  PlainArgs T;
+  memset(&T, 0, sizeof(T));
+  T.P = F.P; T.nx = nx; T.ny = ny; T.mode = F.mode; T.n_designs = n;
+  T.wet = F.wet; T.gn2 = F.gn2; T.bc = F.bc; T.bh = F.bh;
+  T.dzx = F.dzx; T.dzy = F.dzy; T.dzx2 = F.dzx2; T.dzy2 = F.dzy2;
+  T.state_stride = 3 * N; T.plane_stride = S3;
+  T.band_rows = band_rows_for(nx, ny, n, ctx->sm_count);
+  const BandGeom tg = band_geom(nx, ny, T.band_rows);
+  const dim3 tgrid((unsigned)tg.gx, (unsigned)tg.gy, (unsigned)n), tblock((unsigned)(32 * tg.wpb));
+  A.band_rows = adj_rows_for(nx, ny, n, ctx->sm_count);
+  const AdjGeom ag = adj_geom(nx, ny, A.band_rows);
+  const dim3 agrid((unsigned)ag.gx, (unsigned)ag.gy, (unsigned)n), ablock(32 * kAdjWarps);
+  if (adj_band)
+    for (int i = 0; i < 2; ++i) CU(ctx->aPlan[i].ensure((size_t)K * n * sizeof(PlainCtl)));
   auto replay = [&](uint64_t b) -> int {
     const int slot = (int)(b & 1u);
     if (b + 2 < nblocks) CU(cudaStreamWaitEvent(s2, ctx->ev_adj[slot], 0));   // segment b + 2's backward is done with it
@@ -943,6 +964,24 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
     R.tape = tapes[slot];
     R.step0 = b * K;
     R.seg = ctx->aSeg.as<double>() + b * seg_elems;
+    if (adj_band) {
+      PlainCtl* plan = ctx->aPlan[slot].as<PlainCtl>();
+      k_adj_plan<<<dim3((unsigned)K, (unsigned)n), 32, 0, s2>>>(R, plan);
+      for (int j = 0; j + 1 < K; ++j) {
+        PlainArgs Tj = T;
+        Tj.H = tapes[slot] + (size_t)j * S3; Tj.QX = Tj.H + N; Tj.QY = Tj.H + 2 * N;
+        Tj.ctl = plan + (size_t)j * n;
+        if (crest) {
+          if (bnd) k_band<true, true, true><<<tgrid, tblock, 0, s2>>>(Tj);
+          else k_band<true, false, true><<<tgrid, tblock, 0, s2>>>(Tj);
+        } else {
+          if (bnd) k_band<false, true, true><<<tgrid, tblock, 0, s2>>>(Tj);
+          else k_band<false, false, true><<<tgrid, tblock, 0, s2>>>(Tj);
+        }
+      }
+      CU(cudaEventRecord(ctx->ev_rep[slot], s2));
+      return ITR_OK;
+    }
     for (int j = 0; j + 1 < K; ++j) {
       if (crest) {
         if (bnd) k_adj_replay<true, true><<<grid, kTileThreads, 0, s2>>>(R, j);
@@ -965,7 +1004,15 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
     A.seg = ctx->aSeg.as<double>() + b * seg_elems;
     for (int j = K - 1; j >= 0; --j) {
       A.lin = lin; A.lout = lout;
-      if (crest) {
+      if (adj_band) {
+        if (crest) {
+          if (bnd) k_adj_band<true, true><<<agrid, ablock, 0, st>>>(A, j);
+          else k_adj_band<false, true><<<agrid, ablock, 0, st>>>(A, j);
+        } else {
+          if (bnd) k_adj_band<true, false><<<agrid, ablock, 0, st>>>(A, j);
+          else k_adj_band<false, false><<<agrid, ablock, 0, st>>>(A, j);
+        }
+      } else if (crest) {
         if (bnd) k_adj_step<true, true><<<grid, kTileThreads, 0, st>>>(A, j);
         else k_adj_step<false, true><<<grid, kTileThreads, 0, st>>>(A, j);
       } else {

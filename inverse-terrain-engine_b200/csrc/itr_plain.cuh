@@ -104,6 +104,11 @@ struct PlainArgs {
   uint8_t* gwet;
   unsigned* snaprow;
   int band_rows;             // row-band kernel: rows per band (1 .. 32)
+  // State layout (0: the ping-pong default, design d's planes at H + d 2 N, plane p at + p N).
+  // The adjoint's replay (k_band with TAPE) reads and writes its tape through these: design
+  // stride 3 N, and plane 1 = the next step's slot.
+  size_t state_stride;
+  size_t plane_stride;
 };
 
 // Padded row j is dry for the step about to run: no water in its state nor in its stage or
@@ -138,7 +143,8 @@ ITR_DEV PlainDesign plain_design(const PlainArgs& A, int d, int n_tiles) {
   v.dzx2 = A.dzx2 ? A.dzx2 + d * SX : nullptr; v.dzy2 = A.dzy2 ? A.dzy2 + d * SY : nullptr;
   v.h0 = A.h0 + d * N;
   v.bh = A.bh ? A.bh + (size_t)d * (2 * A.nx + 2 * A.ny) : nullptr;
-  v.H = A.H + d * 2 * N; v.QX = A.QX + d * 2 * N; v.QY = A.QY + d * 2 * N;
+  const size_t ss = A.state_stride ? A.state_stride : 2 * N;
+  v.H = A.H + d * ss; v.QX = A.QX + d * ss; v.QY = A.QY + d * ss;
   v.PK = A.PK + d * N;
   v.part = A.part + (size_t)d * n_tiles * kPart;
   v.ctl = A.ctl + d;

@@ -245,6 +245,23 @@ def fractal_scene(n: int = 1024, cell: float = 2.0, seed: int = 20261203 + 5, de
                  design_seed)
 
 
+def river_scene(n: int = 1024, cell: float = 2.0, duration_s: float = 900.0) -> Scene:
+    """Rain-free and inflow-driven: configuration 5's fractal terrain fed by a river that enters
+    through 60 m of the north edge at the head of the terrain's channel (0 to 40 m^3/s over the
+    first 10 min, then steady) and leaves through the transmissive south and east edges. Rows
+    far from the river stay dry for the whole run (the case dry-row skipping is for)."""
+    sc = fractal_scene(n, cell)
+    L = n * cell
+    x0 = 0.1 * L
+    segs = [Segment("inflow", "north", (x0 - 30.0, x0 + 30.0), hydrograph=[(0.0, 0.0), (600.0, 40.0), (duration_s, 40.0)]),
+            Segment("transmissive", "south"), Segment("transmissive", "east")]
+    sc.base = TerrainBase(sc.base.fine, 1, segs)
+    sc.params.rain = Hyetograph.from_mm_h([(0.0, 0.0), (duration_s, 0.0)])
+    sc.params.duration_s = duration_s
+    sc.name = "river"
+    return sc
+
+
 def config(i: int) -> Scene:
     """Scene of configuration i (1-based) at its native resolution."""
     if i == 1:
