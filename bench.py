@@ -484,6 +484,80 @@ def run_reference(args):
     return 0
 
 
+def _case_tiled5(g):
+    """Config 5 on the tiled path (row bands): 1024^2 x 16 designs as primitives, first 300 s."""
+    from itr_gpu.scenes import config
+    sc = config(5)
+    sc.params.duration_s = 300.0
+    ds = sc.primitive_designs(16)
+    for _ in range(2):
+        g.run_primitives(sc.params, sc.base, ds, sc.monitors, sc.editable, sc.max_abs_dz, want_depth=False)
+
+
+def _case_mat4(g):
+    """Config 4's design chain: device materialisation and its adjoint, 32 designs, first 120 s."""
+    from itr_gpu.scenes import config
+    sc = config(4)
+    sc.params.duration_s = 120.0
+    ds = sc.primitive_designs(32)
+    for _ in range(2):
+        g.vjp_primitives(sc.params, sc.base, ds, sc.monitors, sc.objective, sc.editable, sc.max_abs_dz, checkpoint_interval=64)
+
+
+def _case_plain2(g):
+    """Config 2 on the plain one-design-per-launch path, 2 designs, first 300 s."""
+    from itr_gpu.scenes import config
+    sc = config(2)
+    sc.params.duration_s = 300.0
+    ts = [t for _, _, t in sc.designs(2)]
+    g.set_option("impl", 1)
+    for _ in range(2):
+        g.run_batch(sc.params, ts, sc.monitors, want_depth=False)
+
+
+def _case_adj4(g):
+    """Config 4's adjoint: 32 designs, first 300 s of the storm, checkpoint interval 64."""
+    from itr_gpu.scenes import config
+    sc = config(4)
+    sc.params.duration_s = 300.0
+    ts = [t for _, _, t in sc.designs(32)]
+    for _ in range(2):
+        g.vjp(sc.params, ts, sc.monitors, sc.objective, checkpoint_interval=64)
+
+
+def _case_render(g):
+    """The presentation kernels: a 1920x1080 perspective frame of the 45x35 valley scene at 10 m
+    (terrain refined twice, water, flow), and a map image of a seeded 1024^2 field at scale 2."""
+    import numpy as np
+    from itr_gpu.scene_render import SceneView, depth_texture, look, terrain_texture, velocity_texture
+    from itr_gpu.scenes import valley_field
+    nx, ny, cell, up = 45, 35, 10.0, 2
+    zf = valley_field(20261203 + 1)
+    x = (np.arange(nx * up) + 0.5) * cell / up
+    y = ny * cell - (np.arange(ny * up) + 0.5) * cell / up
+    trgba, z_lo, z_span = terrain_texture(zf(*np.meshgrid(x, y)), np.zeros((ny * up, nx * up), np.uint8))
+    zc = zf(*np.meshgrid((np.arange(nx) + 0.5) * cell, ny * cell - (np.arange(ny) + 0.5) * cell))
+    depth = np.clip(zc.min() + 1.4 - zc, 0.0, None)
+    drgba = depth_texture(depth, 4.0)
+    vrgba = velocity_texture(np.where(depth > 0, 0.7, 0.0), np.where(depth > 0, 0.15, 0.0), 2.0)
+    top = z_span * 2.0
+    fwd, right, upv, focal = look((520.0, 420.0, top + 60.0), (200.0, 160.0, 0.2 * top), 60.0)
+    view = SceneView(cam_pos=(520.0, 420.0, top + 60.0), cam_fwd=fwd, cam_right=right, cam_up=upv, focal=focal,
+                     domain=(nx * cell, ny * cell, cell), z_lo=z_lo, z_span=z_span, up=float(up), depth_span=4.0, ve=2.0,
+                     vel_max=2.0, time=1200.0, rain=1.0, wet=1.0, overcast=0.98)
+    for _ in range(2):
+        g.render_scene(trgba, drgba, vrgba, view, 1920, 1080)
+    rng = np.random.default_rng(3)
+    z = (rng.random((1024, 1024)) * 10.0).astype(np.float32)
+    val = rng.random((1024, 1024)).astype(np.float32)
+    for _ in range(2):
+        g.render_map(z, val, 2.0, mode=0, vex=3.0, scale=2)
+
+
+PROFILE_CASES = {"tiled5": _case_tiled5, "mat4": _case_mat4, "plain2": _case_plain2, "adj4": _case_adj4,
+                 "render": _case_render}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -504,6 +578,8 @@ def main():
                     help="profiling: run the main workload on the tiled or plain path instead of the autotuned one")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="profiling: only the config-4 adjoint (forward + VJP) for --duration seconds of storm; prints its summary")
+    ap.add_argument("--profile-case", default=None, choices=sorted(PROFILE_CASES),
+                    help="profiling: run one small case of one path twice (the second run is the one to capture) and exit")
     ap.add_argument("--duration", type=float, default=None,
                     help="simulate only the first DURATION s of the storm (profiling case; not a bench line)")
     args = ap.parse_args()
@@ -514,6 +590,12 @@ def main():
     import torch
     torch.cuda.set_device(local)
     from itr_gpu import GpuSolver
+    if args.profile_case:
+        g = GpuSolver(local)
+        PROFILE_CASES[args.profile_case](g)
+        g.close()
+        print(json.dumps({"profile_case": args.profile_case, "ok": True}))
+        return 0
     if args.adjoint_only:
         g = GpuSolver(local)
         print(json.dumps({"adjoint": adjoint_summary(g, duration=args.duration, which=4 if args.workload == 2 else 5)}))

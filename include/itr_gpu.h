@@ -69,7 +69,9 @@ typedef struct itr_params {
   double initial_depth;     /* used for designs whose h0 is NULL (init_state, solver.rs:287) */
   int32_t skip_dry;         /* dry-row skipping (kernel.rs:605-612): with no rain in a step, a row
                                between dry rows (and dry ghosts) is not computed; results are
-                               the same bits. Done by the cluster kernel and the tiled path   */
+                               the same bits. Done by the cluster kernel and the tiled path;
+                               a storm without a rain-free stretch inside the run has no step
+                               to skip, and such runs leave the bookkeeping out             */
   double inflow_scale;      /* factor on every inflow hydrograph (1.0 = as given)        */
 } itr_params;
 
@@ -206,6 +208,8 @@ int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int3
  *                       ones (identical results; for checking, default 0)
  *   "band"     tiled path update kernel: 1 = row-band sweep (default), 0 = 16x16 tiles with a
  *              halo (identical results; for comparison)
+ *   "adj_band" adjoint replay and backward step: 1 = row-band sweeps (default), 0 = 16x16
+ *              tiles with a halo (identical gradients; for comparison)
  *   "wait_limit"        try_wait rounds of the batched kernel's barrier wait in single-CTA
  *                       designs before the run gives up with ITR_DEVICE_TIMEOUT (default 2^22)
  *   "stall_wait_test"   1 = that barrier expects one arrival more than the CTA makes, so every
