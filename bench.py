@@ -578,6 +578,8 @@ def main():
                     help="profiling: run the main workload on the tiled or plain path instead of the autotuned one")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="profiling: only the config-4 adjoint (forward + VJP) for --duration seconds of storm; prints its summary")
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                    help="profiling: itr_gpu_set_option(KEY, VALUE) on the context before the run (repeatable)")
     ap.add_argument("--profile-case", default=None, choices=sorted(PROFILE_CASES),
                     help="profiling: run one small case of one path twice (the second run is the one to capture) and exit")
     ap.add_argument("--duration", type=float, default=None,
@@ -590,14 +592,21 @@ def main():
     import torch
     torch.cuda.set_device(local)
     from itr_gpu import GpuSolver
+    def apply_options(g):
+        for kv in args.set:
+            key, val = kv.split("=", 1)
+            g.set_option(key, int(val))
+
     if args.profile_case:
         g = GpuSolver(local)
+        apply_options(g)
         PROFILE_CASES[args.profile_case](g)
         g.close()
         print(json.dumps({"profile_case": args.profile_case, "ok": True}))
         return 0
     if args.adjoint_only:
         g = GpuSolver(local)
+        apply_options(g)
         print(json.dumps({"adjoint": adjoint_summary(g, duration=args.duration, which=4 if args.workload == 2 else 5)}))
         g.close()
         return 0

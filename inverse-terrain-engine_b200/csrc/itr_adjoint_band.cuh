@@ -131,10 +131,13 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A,
   const int r1 = r0 + R < ny ? r0 + R : ny;
   const bool own = lane >= 1 && lane <= kAdjOwn && col < nx;   // an owned cell column
   if (n >= A.n_steps[d]) {   // the design stopped before this step: the adjoint passes through
-    if (own)
-      for (int r = r0; r < r1; ++r) {
-        const size_t gi = (size_t)r * nx + col;
-        LO[gi] = LI[gi]; LO[N + gi] = LI[N + gi]; LO[2 * N + gi] = LI[2 * N + gi];
+    const int c_lo = blockIdx.x * kAdjWarps * kAdjOwn;   // the block's cells, all threads at once
+    const int w = (c_lo + kAdjWarps * kAdjOwn < nx ? c_lo + kAdjWarps * kAdjOwn : nx) - c_lo;
+    if (w > 0)
+      for (int e = threadIdx.x; e < w * (r1 - r0); e += blockDim.x) {
+        const size_t gi = (size_t)(r0 + e / w) * nx + c_lo + e % w;
+        const float a = LI[gi], b = LI[N + gi], c = LI[2 * N + gi];
+        LO[gi] = a; LO[N + gi] = b; LO[2 * N + gi] = c;
       }
     return;
   }
@@ -160,15 +163,17 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A,
   const bool xcol = col >= 0 && col <= nx;    // x-face `col` exists
   const bool ycol = col >= 0 && col < nx;     // y-faces of column `col` exist
   // forward x-face between (r, col - 1) and (r, col); L: the west cell
+  // (computed on every lane, then zeroed where the face does not exist: one straight-line body
+  //  lets the compiler interleave a row's independent chains)
   auto xfwd = [&](const ACell& L, const ACell& C, int r, float dz, float dz2) -> FaceF {
-    FaceF o{};
-    if (xcol && r >= 0 && r < ny) o = face<true, CREST>(L.h, L.u, L.v, L.c, C.h, C.u, C.v, C.c, dz, dz2, k);
+    FaceF o = face<true, CREST>(L.h, L.u, L.v, L.c, C.h, C.u, C.v, C.c, dz, dz2, k);
+    if (!(xcol && r >= 0 && r < ny)) o = FaceF{};
     return o;
   };
   // forward y-face f between (f - 1, col) and (f, col)
   auto yfwd = [&](const ACell& T, const ACell& B, int f, float dz, float dz2) -> FaceF {
-    FaceF o{};
-    if (ycol && f >= 0 && f <= ny) o = face<false, CREST>(T.h, T.u, T.v, T.c, B.h, B.u, B.v, B.c, dz, dz2, k);
+    FaceF o = face<false, CREST>(T.h, T.u, T.v, T.c, B.h, B.u, B.v, B.c, dz, dz2, k);
+    if (!(ycol && f >= 0 && f <= ny)) o = FaceF{};
     return o;
   };
   auto jx = [&](const float* a, int r) -> float { return (xcol && r >= 0 && r < ny) ? a[(size_t)r * nxp1 + col] : 0.0f; };
@@ -204,16 +209,16 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A,
   auto l1_of = [&](const ACell& C, const FaceF& W, const FaceF& E, const FaceF& Nf, const FaceF& Sf, int r, float wet,
                    float gn2, float lh, float lqx, float lqy) -> L1 {
     L1 o{0.0f, 0.0f, 0.0f};
-    if (ycol && r >= 0 && r < ny) {
-      if (seeded) {
-        const size_t gi = (size_t)r * nx + col;
-        for (int q = 0; q < sn[d]; ++q) {
-          const size_t si = (size_t)d * A.max_seeds + q;
-          if (A.seed_cell[si] == gi && A.seed_state[si] == n + 1) lh += A.seed_w[si];
-        }
+    const bool in = ycol && r >= 0 && r < ny;
+    if (seeded && in) {
+      const size_t gi = (size_t)r * nx + col;
+      for (int q = 0; q < sn[d]; ++q) {
+        const size_t si = (size_t)d * A.max_seeds + q;
+        if (A.seed_cell[si] == gi && A.seed_state[si] == n + 1) lh += A.seed_w[si];
       }
-      sources_bwd(C.h, C.qx, C.qy, W, E, Nf, Sf, wet, gn2, k, lh, lqx, lqy, o.h, o.qx, o.qy);
     }
+    sources_bwd(C.h, C.qx, C.qy, W, E, Nf, Sf, wet, gn2, k, lh, lqx, lqy, o.h, o.qx, o.qy);
+    if (!in) o = L1{0.0f, 0.0f, 0.0f};
     return o;
   };
   // inputs of row r for this lane's column (zero outside)
@@ -255,14 +260,16 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A,
     lc = l1_of(Sc, xc, xce, yb, yc, r0, ic.wet, ic.gn2, ic.lh, ic.lqx, ic.lqy);
   }
   FaceBwd nb{};   // adjoint of the north y-face of the current row
-  if (own) {
+  {
     const float lm = -k.dtdy * lb.h + k.dtdy * lc.h;
     const float lt = -k.dtdy * lb.qx + k.dtdy * lc.qx;
     const float lnl = -k.dtdy * lb.qy, lnr = k.dtdy * lc.qy;
     nb = face_bwd<false, CREST>(Sb.h, Sb.u, Sb.v, Sb.c, Sc.h, Sc.u, Sc.v, Sc.c, jyb, jyb2, k, lm, lnl, lnr, lt);
-    double* gp = A.gdzy + d * SY + (size_t)r0 * nx + col;
-    *gp = *gp + (double)nb.dz;
-    if (CREST) { double* gp2 = A.gdzy2 + d * SY + (size_t)r0 * nx + col; *gp2 = *gp2 + (double)nb.dz2; }
+    if (own) {
+      double* gp = A.gdzy + d * SY + (size_t)r0 * nx + col;
+      *gp = *gp + (double)nb.dz;
+      if (CREST) { double* gp2 = A.gdzy2 + d * SY + (size_t)r0 * nx + col; *gp2 = *gp2 + (double)nb.dz2; }
+    }
   }
 
   // ---- row sweep ----
@@ -276,6 +283,16 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A,
       inn = load_in(r + 2);
       Se = raw(col, r + 3);
     }
+    // this row's gradient sums, read before the arithmetic so the loads are in flight
+    const bool yown_r = own && (r + 1 < r1 || r + 1 == ny);
+    double* gyp = A.gdzy + d * SY + (size_t)(r + 1) * nx + col;
+    double* gxp = A.gdzx + d * SX + (size_t)r * nxp1 + col;
+    const double gy_old = yown_r ? *gyp : 0.0, gx_old = xown ? *gxp : 0.0;
+    double gy2_old = 0.0, gx2_old = 0.0;
+    if (CREST) {
+      gy2_old = yown_r ? A.gdzy2[d * SY + (size_t)(r + 1) * nx + col] : 0.0;
+      gx2_old = xown ? A.gdzx2[d * SX + (size_t)r * nxp1 + col] : 0.0;
+    }
     // forward faces around row r + 1 and its source adjoint
     const float jyd = jy(dzy, r + 2), jyd2 = CREST ? jy(dzy2, r + 2) : 0.0f;
     const FaceF yd = yfwd(Sd, Snext, r + 2, jyd, jyd2);
@@ -285,33 +302,32 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A,
     const FaceF xde = facef_shfl_down(xd);
     const L1 ld = l1_of(Sd, xd, xde, yc, yd, r + 1, in1.wet, in1.gn2, in1.lh, in1.lqx, in1.lqy);
     // adjoint of the y-face (r | r + 1)
-    FaceBwd sb{};
-    if (own) {
+    FaceBwd sb;
+    {
       const float lm = -k.dtdy * lc.h + k.dtdy * ld.h;
       const float lt = -k.dtdy * lc.qx + k.dtdy * ld.qx;
       const float lnl = -k.dtdy * lc.qy, lnr = k.dtdy * ld.qy;
       sb = face_bwd<false, CREST>(Sc.h, Sc.u, Sc.v, Sc.c, Sd.h, Sd.u, Sd.v, Sd.c, jyc, jyc2, k, lm, lnl, lnr, lt);
-      if (r + 1 < r1 || r + 1 == ny) {
-        double* gp = A.gdzy + d * SY + (size_t)(r + 1) * nx + col;
-        *gp = *gp + (double)sb.dz;
-        if (CREST) { double* gp2 = A.gdzy2 + d * SY + (size_t)(r + 1) * nx + col; *gp2 = *gp2 + (double)sb.dz2; }
-      }
     }
     // adjoint of the west x-face of (r, col), lanes 1 .. 30 (lane 30's is the east face of 29)
     const ACell Wc = acell_shfl_up(Sc);
     const float lwh = __shfl_up_sync(0xffffffffu, lc.h, 1), lwqx = __shfl_up_sync(0xffffffffu, lc.qx, 1),
                 lwqy = __shfl_up_sync(0xffffffffu, lc.qy, 1);
-    FaceBwd xb{};
-    if (lane >= 1 && lane <= kAdjOwn + 1 && xcol) {
+    FaceBwd xb;
+    {
       const float lm = -k.dtdx * lwh + k.dtdx * lc.h;
       const float lnl = -k.dtdx * lwqx, lnr = k.dtdx * lc.qx;
       const float lt = -k.dtdx * lwqy + k.dtdx * lc.qy;
       xb = face_bwd<true, CREST>(Wc.h, Wc.u, Wc.v, Wc.c, Sc.h, Sc.u, Sc.v, Sc.c, jxc, jxc2, k, lm, lnl, lnr, lt);
-      if (xown) {
-        double* gp = A.gdzx + d * SX + (size_t)r * nxp1 + col;
-        *gp = *gp + (double)xb.dz;
-        if (CREST) { double* gp2 = A.gdzx2 + d * SX + (size_t)r * nxp1 + col; *gp2 = *gp2 + (double)xb.dz2; }
-      }
+    }
+    if (!(xcol && lane >= 1)) xb = FaceBwd{};   // (lane 0 and columns past the east face)
+    if (yown_r) {
+      *gyp = gy_old + (double)sb.dz;
+      if (CREST) A.gdzy2[d * SY + (size_t)(r + 1) * nx + col] = gy2_old + (double)sb.dz2;
+    }
+    if (xown) {
+      *gxp = gx_old + (double)xb.dz;
+      if (CREST) A.gdzx2[d * SX + (size_t)r * nxp1 + col] = gx2_old + (double)xb.dz2;
     }
     const FaceBwd xe = facebwd_shfl_down(xb);
     const ACell Ec = acell_shfl_down(Sc);
