@@ -28,11 +28,15 @@
 namespace itr {
 
 constexpr int kAdjOwn = 29;     // columns a warp owns (lanes 1 .. 29)
-constexpr int kAdjWarps = 4;    // warps (segments) per block
+constexpr int kAdjWarps = 4;    // most warps (segments) per block
 constexpr int kAdjRows = 32;    // most rows per band
+#ifndef ITR_ADJ_MIN_BLOCKS
+#define ITR_ADJ_MIN_BLOCKS 4    // resident blocks per SM the register budget is cut for
+#endif
 
 struct AdjGeom {
   int ns;      // segments of kAdjOwn columns
+  int wpb;     // warps per block: the divisor-friendliest of 4, 3, 2 (fewest idle segments)
   int rows;    // rows per band
   int gx, gy;  // blocks per design
 };
@@ -40,8 +44,14 @@ struct AdjGeom {
 __host__ __device__ inline AdjGeom adj_geom(int nx, int ny, int rows) {
   AdjGeom g;
   g.ns = (nx + kAdjOwn - 1) / kAdjOwn;
+  g.wpb = 1;
+  int waste = 1 << 30;
+  for (int w = kAdjWarps; w >= 1; --w) {
+    const int e = (g.ns + w - 1) / w * w - g.ns;
+    if (e < waste) { waste = e; g.wpb = w; }
+  }
   g.rows = rows;
-  g.gx = (g.ns + kAdjWarps - 1) / kAdjWarps;
+  g.gx = (g.ns + g.wpb - 1) / g.wpb;
   g.gy = (ny + rows - 1) / rows;
   return g;
 }
@@ -49,12 +59,12 @@ __host__ __device__ inline AdjGeom adj_geom(int nx, int ny, int rows) {
 // Rows per band: the busy fraction of the launch's rounds of resident warps (16 per SM at the
 // kernel's occupancy) times R / (R + 2), the share of rows a band does not recompute.
 inline int adj_rows_for(int nx, int ny, int n_designs, int sm_count) {
-  const double resident = 16.0 * (sm_count > 0 ? sm_count : 148);
+  const double resident = 4.0 * ITR_ADJ_MIN_BLOCKS * (sm_count > 0 ? sm_count : 148);
   int best = kAdjRows;
   double best_score = -1.0;
   for (int rows = kAdjRows; rows >= 6; --rows) {
     const AdjGeom g = adj_geom(nx, ny, rows);
-    const double warps = (double)n_designs * g.gx * kAdjWarps * g.gy;
+    const double warps = (double)n_designs * g.gx * g.wpb * g.gy;
     const double rounds = std::ceil(warps / resident);
     const double score = warps / (rounds * resident) * rows / (rows + 2.0);
     if (score > best_score + 1e-9) { best_score = score; best = rows; }
@@ -113,7 +123,7 @@ ITR_DEV FaceBwd facebwd_shfl_down(const FaceBwd& b) {
 }
 
 template <bool BND, bool CREST>
-__global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A, int j) {
+__global__ void __launch_bounds__(kAdjWarps * 32, ITR_ADJ_MIN_BLOCKS) k_adj_band(const AdjArgs A, int j) {
   __shared__ FaceF edge[kAdjWarps][2 * 32];   // lane 0's west x-face, rows r0 - 1 .. r1
   __shared__ float2 sinf[kMaxInflow];
   const int d = blockIdx.z;
@@ -123,7 +133,8 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A,
   const float* LI = A.lin + (size_t)d * 3 * N;
   float* LO = A.lout + (size_t)d * 3 * N;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int s = blockIdx.x * kAdjWarps + wid;      // this warp's segment
+  const int wpb = blockDim.x >> 5;
+  const int s = blockIdx.x * wpb + wid;            // this warp's segment
   const int cs = s * kAdjOwn;                      // its first owned column
   const int col = cs - 1 + lane;                   // this lane's column
   const int R = A.band_rows;
@@ -131,8 +142,8 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) k_adj_band(const AdjArgs A,
   const int r1 = r0 + R < ny ? r0 + R : ny;
   const bool own = lane >= 1 && lane <= kAdjOwn && col < nx;   // an owned cell column
   if (n >= A.n_steps[d]) {   // the design stopped before this step: the adjoint passes through
-    const int c_lo = blockIdx.x * kAdjWarps * kAdjOwn;   // the block's cells, all threads at once
-    const int w = (c_lo + kAdjWarps * kAdjOwn < nx ? c_lo + kAdjWarps * kAdjOwn : nx) - c_lo;
+    const int c_lo = blockIdx.x * wpb * kAdjOwn;   // the block's cells, all threads at once
+    const int w = (c_lo + wpb * kAdjOwn < nx ? c_lo + wpb * kAdjOwn : nx) - c_lo;
     if (w > 0)
       for (int e = threadIdx.x; e < w * (r1 - r0); e += blockDim.x) {
         const size_t gi = (size_t)(r0 + e / w) * nx + c_lo + e % w;

@@ -128,7 +128,7 @@ struct itr_ctx {
   int autotune = 1, autotune_top = 6, probe_steps = 200;
   int exact_special = 0;
   int band = 1;           // tiled path update kernel: 1 = row-band sweep (k_band), 0 = 16x16 tiles
-  int adj_band = 1;       // adjoint replay and backward step: 1 = row-band sweeps, 0 = 16x16 tiles
+  int adj_band = 1;       // adjoint kernels on row bands: bit 0 the replay, bit 1 the backward step (else 16x16 tiles)
   unsigned wait_limit = 1u << 22;   // bounded barrier wait of single-CTA designs (try_wait rounds)
   int stall_wait_test = 0;          // test of the timeout path: that wait never completes
   float tune_ms = 0.0f;
@@ -620,7 +620,7 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   else if (k == "exact_special") ctx->exact_special = value != 0;
   else if (k == "warm_start") ctx->warm_start = value != 0;
   else if (k == "band") ctx->band = value != 0;
-  else if (k == "adj_band") ctx->adj_band = value != 0;
+  else if (k == "adj_band") { if (value < 0 || value > 3) return fail(ctx, ITR_INVALID_ARG, "adj_band is 0 .. 3"); ctx->adj_band = (int)value; }
   else if (k == "wait_limit") { if (value < 1 || value > 0x7fffffff) return fail(ctx, ITR_INVALID_ARG, "wait_limit out of range"); ctx->wait_limit = (unsigned)value; }
   else if (k == "stall_wait_test") ctx->stall_wait_test = value != 0;
   else if (k == "probe_steps") { if (value < 1) return fail(ctx, ITR_INVALID_ARG, "probe_steps must be >= 1"); ctx->probe_steps = (int)value; }
@@ -941,7 +941,7 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   CU(cudaStreamWaitEvent(s2, ctx->ev_bwd, 0));
   // Row-band replay: k_band<..., TAPE> over the tape, slot j to slot j + 1, with the control
   // blocks k_adj_plan writes for the segment (one buffer per tape).
-  const bool adj_band = ctx->adj_band != 0;
+  const bool adj_band = (ctx->adj_band & 1) != 0, adj_step_band = (ctx->adj_band & 2) != 0;
   PlainArgs T;
   memset(&T, 0, sizeof(T));
   T.P = F.P; T.nx = nx; T.ny = ny; T.mode = F.mode; T.n_designs = n;
@@ -953,7 +953,7 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
   const dim3 tgrid((unsigned)tg.gx, (unsigned)tg.gy, (unsigned)n), tblock((unsigned)(32 * tg.wpb));
   A.band_rows = adj_rows_for(nx, ny, n, ctx->sm_count);
   const AdjGeom ag = adj_geom(nx, ny, A.band_rows);
-  const dim3 agrid((unsigned)ag.gx, (unsigned)ag.gy, (unsigned)n), ablock(32 * kAdjWarps);
+  const dim3 agrid((unsigned)ag.gx, (unsigned)ag.gy, (unsigned)n), ablock((unsigned)(32 * ag.wpb));
   if (adj_band)
     for (int i = 0; i < 2; ++i) CU(ctx->aPlan[i].ensure((size_t)K * n * sizeof(PlainCtl)));
   auto replay = [&](uint64_t b) -> int {
@@ -1004,7 +1004,7 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
     A.seg = ctx->aSeg.as<double>() + b * seg_elems;
     for (int j = K - 1; j >= 0; --j) {
       A.lin = lin; A.lout = lout;
-      if (adj_band) {
+      if (adj_step_band) {
         if (crest) {
           if (bnd) k_adj_band<true, true><<<agrid, ablock, 0, st>>>(A, j);
           else k_adj_band<false, true><<<agrid, ablock, 0, st>>>(A, j);

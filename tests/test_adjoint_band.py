@@ -1,8 +1,9 @@
 """The adjoint's row-band kernels against its 16x16-tile kernels, bit for bit.
 
-itr_gpu_vjp replays each checkpoint segment and steps the adjoint back through it. The default
-kernels are row-band sweeps (the forward's own k_band in TAPE mode for the replay, k_adj_band
-for the backward step); option adj_band = 0 selects the tile kernels (k_adj_replay, k_adj_step).
+itr_gpu_vjp replays each checkpoint segment and steps the adjoint back through it, each part on
+row-band sweeps or on 16x16 tiles (option adj_band: bit 0 the replay, the forward's own k_band
+in TAPE mode instead of k_adj_replay; bit 1 the backward step, k_adj_band instead of
+k_adj_step).
 Both replays are the forward step bit for bit, and k_adj_band evaluates k_adj_step's arithmetic
 in the same order, so every gradient must be identical: walls and transmissive edges, stage
 and inflow ghosts, crest faces, a dry start, and configuration 4's grid with several designs
@@ -90,13 +91,14 @@ def test_band_backward_equals_tile_backward(gpu, name):
     p, terrains, obj, K = CASES[name](gpu)
     runs = {}
     try:
-        for band in (1, 0):
+        for band in (3, 1, 0):
             gpu.set_option("adj_band", band)
             runs[band] = gpu.vjp(p, terrains, obj.monitors, obj, checkpoint_interval=K)
     finally:
         gpu.set_option("adj_band", 1)
     nonzero = 0
-    for i, (a, b) in enumerate(zip(runs[1], runs[0])):
+    pairs = [(i, a, b) for band in (3, 1) for i, (a, b) in enumerate(zip(runs[band], runs[0]))]
+    for i, a, b in pairs:
         assert a.steps == b.steps and a.j == b.j, (name, i)
         for f in ("dj_ddzx", "dj_ddzy", "dj_ddzx2", "dj_ddzy2"):
             ga, gb = getattr(a, f, None), getattr(b, f, None)
