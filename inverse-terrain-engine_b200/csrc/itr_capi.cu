@@ -1327,7 +1327,7 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     const size_t items = faces > NB ? faces : NB;
     k_materialize<<<dim3((unsigned)((N + 255) / 256), (unsigned)n), 256, 0, ctx->stream>>>(MA);
     k_mat_jumps<<<dim3((unsigned)((items + 255) / 256), (unsigned)n), 256, 0, ctx->stream>>>(MA);
-    k_mat_volumes<<<(n + 63) / 64, 64, 0, ctx->stream>>>(MA);
+    k_mat_volumes<<<(n + 3) / 4, 128, 0, ctx->stream>>>(MA);   // a warp per design
     launches += 3;
     double* hv = ctx->mVol.as<double>();
     CU(cudaMemcpyAsync(hv, dv + o_cut, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));

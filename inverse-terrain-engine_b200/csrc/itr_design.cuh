@@ -144,21 +144,30 @@ __global__ void k_mat_jumps(const MatArgs M) {
 }
 
 // Cut and fill volumes of each design's edit (design.rs:376-383), summed over its bounding
-// box in row-major order as the reference does (one thread per design).
+// box in row-major order as the reference does. One warp per design: the lanes load 32
+// consecutive cells of a row at once, and every lane runs the sum over them in column order
+// (values broadcast by shuffle), so the f64 sums are the sequential ones, bit for bit.
 __global__ void k_mat_volumes(const MatArgs M) {
-  const int d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d >= M.n) return;
+  const int lane = threadIdx.x & 31;
+  const int d = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (d >= M.n) return;   // (whole warps)
   const MatDesign D = M.des[d];
   const size_t N = (size_t)M.nx * M.ny;
   const double a = M.dx * M.dy;
   double cut = 0.0, fill = 0.0;
   for (int r = D.r0; r < D.r1; ++r)
-    for (int c = D.c0; c < D.c1; ++c) {
-      const double v = M.dz[(size_t)d * N + (size_t)r * M.nx + c];
-      if (v > 0.0) fill += v * a; else cut -= v * a;
+    for (int c0 = D.c0; c0 < D.c1; c0 += 32) {
+      const int c = c0 + lane, m = D.c1 - c0 < 32 ? D.c1 - c0 : 32;
+      const double mine = c < D.c1 ? M.dz[(size_t)d * N + (size_t)r * M.nx + c] : 0.0;
+      for (int k = 0; k < m; ++k) {
+        const double v = __shfl_sync(0xffffffffu, mine, k);
+        if (v > 0.0) fill += v * a; else cut -= v * a;
+      }
     }
-  M.cut[d] = cut;
-  M.fill[d] = fill;
+  if (lane == 0) {
+    M.cut[d] = cut;
+    M.fill[d] = fill;
+  }
 }
 
 // ---- the design chain of the adjoint: dJ/d(height, width, length) per primitive ----
