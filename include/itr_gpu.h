@@ -211,6 +211,9 @@ int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int3
  *   "adj_band" adjoint kernels on row-band sweeps instead of 16x16 tiles with a halo: bit 0
  *              the replay of each segment, bit 1 the backward step (default 1; identical
  *              gradients for every value 0 .. 3)
+ *   "adj_trim" 1 = the backward sweep of a design stops at the latest state that set one of its
+ *              assets' maxima (after it the adjoint is zero: identical gradients, fewer steps;
+ *              default 1), 0 = every step of the run
  *   "wait_limit"        try_wait rounds of the batched kernel's barrier wait in single-CTA
  *                       designs before the run gives up with ITR_DEVICE_TIMEOUT (default 2^22)
  *   "stall_wait_test"   1 = that barrier expects one arrival more than the CTA makes, so every

@@ -129,6 +129,7 @@ struct itr_ctx {
   int exact_special = 0;
   int band = 1;           // tiled path update kernel: 1 = row-band sweep (k_band), 0 = 16x16 tiles
   int adj_band = 1;       // adjoint kernels on row bands: bit 0 the replay, bit 1 the backward step (else 16x16 tiles)
+  int adj_trim = 1;       // adjoint: skip the steps after a design's latest asset maximum (zero adjoint there)
   unsigned wait_limit = 1u << 22;   // bounded barrier wait of single-CTA designs (try_wait rounds)
   int stall_wait_test = 0;          // test of the timeout path: that wait never completes
   float tune_ms = 0.0f;
@@ -620,6 +621,7 @@ int itr_gpu_set_option(itr_ctx* ctx, const char* key, int64_t value) {
   else if (k == "exact_special") ctx->exact_special = value != 0;
   else if (k == "warm_start") ctx->warm_start = value != 0;
   else if (k == "band") ctx->band = value != 0;
+  else if (k == "adj_trim") ctx->adj_trim = value != 0;
   else if (k == "adj_band") { if (value < 0 || value > 3) return fail(ctx, ITR_INVALID_ARG, "adj_band is 0 .. 3"); ctx->adj_band = (int)value; }
   else if (k == "wait_limit") { if (value < 1 || value > 0x7fffffff) return fail(ctx, ITR_INVALID_ARG, "wait_limit out of range"); ctx->wait_limit = (unsigned)value; }
   else if (k == "stall_wait_test") ctx->stall_wait_test = value != 0;
@@ -863,7 +865,19 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
     }
   std::vector<unsigned long long> nst(n);
   unsigned long long nmax = 0;
-  for (int d = 0; d < n; ++d) { nst[d] = hdo[d].steps; nmax = nst[d] > nmax ? nst[d] : nmax; }
+  for (int d = 0; d < n; ++d) {
+    nst[d] = hdo[d].steps;
+    // Past the latest state that set one of its assets' maxima, a design's adjoint is zero
+    // (no seed is left to add and the adjoint after the last step starts at zero), so those
+    // steps change no gradient: its backward covers steps 0 .. S - 1 (S = that state index,
+    // 0 without seeds) and the later steps pass the zero adjoint through.
+    if (ctx->adj_trim) {
+      unsigned long long S = 0;
+      for (int q = 0; q < sn[d]; ++q) S = ss[(size_t)d * ms + q] > S ? ss[(size_t)d * ms + q] : S;
+      nst[d] = S < nst[d] ? S : nst[d];
+    }
+    nmax = nst[d] > nmax ? nst[d] : nmax;
+  }
   const uint64_t nblocks = (nmax + K - 1) / K;
   if (nblocks > V->blocks) return fail(ctx, ITR_DEVICE_ERROR, "adjoint: %llu segments but %llu checkpoints",
                                        (unsigned long long)nblocks, (unsigned long long)V->blocks);
@@ -994,8 +1008,10 @@ static int vjp_backward(itr_ctx* ctx, const PlainArgs& F, const itr_objective* o
     CU(cudaEventRecord(ctx->ev_rep[slot], s2));
     return ITR_OK;
   };
-  rc_ = replay(nblocks - 1);
-  if (rc_ != ITR_OK) return rc_;
+  if (nblocks > 0) {   // (none: no design has a seed, every gradient is zero)
+    rc_ = replay(nblocks - 1);
+    if (rc_ != ITR_OK) return rc_;
+  }
   for (uint64_t b = nblocks; b-- > 0;) {   // no host round trip between segments
     const int slot = (int)(b & 1u);
     CU(cudaStreamWaitEvent(st, ctx->ev_rep[slot], 0));

@@ -109,3 +109,21 @@ def test_band_backward_equals_tile_backward(gpu, name):
                 (name, i, f, int(np.count_nonzero(ga != gb)), float(np.max(np.abs(ga - gb))))
             nonzero += int(np.count_nonzero(ga))
     assert nonzero > 0, name
+
+
+@pytest.mark.parametrize("name", ["smooth", "stage_inflow", "config4"])
+def test_trimmed_sweep_equals_full_sweep(gpu, name):
+    """The backward sweep stops at each design's latest asset maximum (option adj_trim): past it
+    the adjoint is zero, so the gradients equal the full sweep's bit for bit."""
+    p, terrains, obj, K = CASES[name](gpu)
+    runs = {}
+    try:
+        for trim in (1, 0):
+            gpu.set_option("adj_trim", trim)
+            runs[trim] = gpu.vjp(p, terrains, obj.monitors, obj, checkpoint_interval=K)
+    finally:
+        gpu.set_option("adj_trim", 1)
+    for i, (a, b) in enumerate(zip(runs[1], runs[0])):
+        for f in ("dj_ddzx", "dj_ddzy"):
+            ga, gb = np.asarray(getattr(a, f)), np.asarray(getattr(b, f))
+            assert np.array_equal(ga.view(np.uint64), gb.view(np.uint64)), (name, i, f, int(np.count_nonzero(ga != gb)))
