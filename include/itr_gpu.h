@@ -209,8 +209,9 @@ int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_grid* g, int3
  *   "band"     tiled path update kernel: 1 = row-band sweep (default), 0 = 16x16 tiles with a
  *              halo (identical results; for comparison)
  *   "adj_band" adjoint kernels on row-band sweeps instead of 16x16 tiles with a halo: bit 0
- *              the replay of each segment, bit 1 the backward step (default 1; identical
- *              gradients for every value 0 .. 3)
+ *              the replay of each segment, bit 1 the backward step; -1 (default) = the replay
+ *              on bands, the backward step on bands for grids of 2^18 cells or more
+ *              (identical gradients for every value)
  *   "adj_trim" 1 = the backward sweep of a design stops at the latest state that set one of its
  *              assets' maxima (after it the adjoint is zero: identical gradients, fewer steps;
  *              default 1), 0 = every step of the run

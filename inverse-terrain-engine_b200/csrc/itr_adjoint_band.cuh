@@ -31,7 +31,8 @@ constexpr int kAdjOwn = 29;     // columns a warp owns (lanes 1 .. 29)
 constexpr int kAdjWarps = 4;    // most warps (segments) per block
 constexpr int kAdjRows = 32;    // most rows per band
 #ifndef ITR_ADJ_MIN_BLOCKS
-#define ITR_ADJ_MIN_BLOCKS 4    // resident blocks per SM the register budget is cut for
+#define ITR_ADJ_MIN_BLOCKS 6    // resident blocks per SM the register budget is cut for (85
+                                // registers, a few spilled: measured faster than 4 and 8)
 #endif
 
 struct AdjGeom {
@@ -56,8 +57,9 @@ __host__ __device__ inline AdjGeom adj_geom(int nx, int ny, int rows) {
   return g;
 }
 
-// Rows per band: the busy fraction of the launch's rounds of resident warps (16 per SM at the
-// kernel's occupancy) times R / (R + 2), the share of rows a band does not recompute.
+// Rows per band: the busy fraction of the launch's rounds of resident warps (4 per block,
+// ITR_ADJ_MIN_BLOCKS blocks per SM) times R / (R + 2), the share of rows a band does not
+// recompute.
 inline int adj_rows_for(int nx, int ny, int n_designs, int sm_count) {
   const double resident = 4.0 * ITR_ADJ_MIN_BLOCKS * (sm_count > 0 ? sm_count : 148);
   int best = kAdjRows;

@@ -95,7 +95,7 @@ def test_band_backward_equals_tile_backward(gpu, name):
             gpu.set_option("adj_band", band)
             runs[band] = gpu.vjp(p, terrains, obj.monitors, obj, checkpoint_interval=K)
     finally:
-        gpu.set_option("adj_band", 1)
+        gpu.set_option("adj_band", -1)
     nonzero = 0
     pairs = [(i, a, b) for band in (3, 1) for i, (a, b) in enumerate(zip(runs[band], runs[0]))]
     for i, a, b in pairs:
