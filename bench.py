@@ -645,6 +645,7 @@ def main():
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall0
     barrier(world)
+    launch_shape = g.adapter_info().split("; last batch: ")[-1] if "; last batch: " in g.adapter_info() else None
     k_total_ms = max_over_ranks(sum(kern_ms), world)
     total_cs = sum_over_ranks(cell_steps * args.steps, world)
     value = total_cs / (k_total_ms / 1e3)
@@ -714,6 +715,7 @@ def main():
                        "path": args.impl_path,
                        "designs_per_gpu": len(terrs), "cells": N, "steps_per_design_mean": sum(steps_per_design) / len(steps_per_design),
                        "parallelism": f"designs sharded over {world} GPU(s), 1 design per thread-block cluster",
+                       "launch": launch_shape,
                        "l2": "flushed between timed iterations (256 MB write)"},
             "designs_per_s": designs_per_s,
             "precision": ("device path bit-identical to the f32 CPU port (tests/test_gpu_parity.py); that port's "

@@ -605,8 +605,13 @@ int itr_gpu_info(itr_ctx* ctx, char* buf, size_t len) {
   size_t fr = 0, tot = 0;
   cudaSetDevice(ctx->device);
   cudaMemGetInfo(&fr, &tot);
-  snprintf(buf, len, "%s (device %d, %d SMs, %.1f GB, %zu B smem/CTA opt-in; itr_gpu ABI %d, sm_100a)", ctx->name, ctx->device,
-           ctx->sm_count, tot / 1e9, ctx->smem_optin, ITR_GPU_ABI_VERSION);
+  int k = snprintf(buf, len, "%s (device %d, %d SMs, %.1f GB, %zu B smem/CTA opt-in; itr_gpu ABI %d, sm_100a)", ctx->name,
+                   ctx->device, ctx->sm_count, tot / 1e9, ctx->smem_optin, ITR_GPU_ABI_VERSION);
+  if (k > 0 && (size_t)k < len && ctx->have_last && !ctx->last_was_plain && !ctx->last_was_tiled)
+    snprintf(buf + k, len - (size_t)k, "; last batch: cluster kernel, %d CTAs x %d threads (%d strips of %d warps)",
+             ctx->last_cfg.C, ctx->last_cfg.T, ctx->last_cfg.S, ctx->last_cfg.W);
+  else if (k > 0 && (size_t)k < len && ctx->have_last && ctx->last_was_tiled)
+    snprintf(buf + k, len - (size_t)k, "; last batch: tiled path (%s)", ctx->band ? "row bands" : "16x16 tiles");
   return ITR_OK;
 }
 
