@@ -1498,7 +1498,8 @@ extern "C" int itr_gpu_run_batch(itr_ctx* ctx, const itr_params* p, const itr_gr
     A.warm = warm_dev;
     // launch configuration
     LaunchCfg cfg;
-    auto key = std::make_tuple(nx, ny, n, (int)g->mode + (bnd ? 2 : 0));
+    // (the dry-row instantiation is tuned apart: its bookkeeping changes the best shape)
+    auto key = std::make_tuple(nx, ny, n, (int)g->mode + (bnd ? 2 : 0) + (A.P.skip_dry ? 4 : 0));
     if (ctx->cluster > 0 || ctx->threads > 0) {
       cfg = make_cfg(ctx, nx, ny, ctx->cluster > 0 ? ctx->cluster : 1, ctx->threads > 0 ? ctx->threads : 512, crest, bnd);
       if (!cfg.ok) return fail(ctx, ITR_UNSUPPORTED, "cluster=%d threads=%d does not fit a %dx%d grid in shared memory", ctx->cluster, ctx->threads, nx, ny);
