@@ -53,11 +53,12 @@ __host__ __device__ inline BandGeom band_geom(int nx, int ny, int rows) {
 }
 
 // Rows per band. Every warp sweeps one band segment, all warps about equally long, so a launch
-// takes ceil(warps / resident) rounds of the SMs (16 warps resident per SM at the kernel's
-// occupancy): the chosen height maximises the busy fraction of those rounds times R / (R + 1),
-// the share of y-faces computed once (each band recomputes its top y-face row).
+// takes ceil(warps / resident) rounds of the SMs (12 warps resident per SM: 3 blocks of 4
+// warps, the register budget at which nothing spills, measured 7-8 % faster than 4 blocks
+// with spills). The chosen height maximises the busy fraction of those rounds times
+// R / (R + 1), the share of y-faces computed once (each band recomputes its top y-face row).
 inline int band_rows_for(int nx, int ny, int n_designs, int sm_count) {
-  const double resident = 16.0 * (sm_count > 0 ? sm_count : 148);
+  const double resident = 12.0 * (sm_count > 0 ? sm_count : 148);
   int best = kBandRows;
   double best_score = -1.0;
   for (int rows = kBandRows; rows >= 6; --rows) {
@@ -144,7 +145,7 @@ ITR_DEV Raw2 band_row(const PlainArgs& A, const PlainDesign& D, const float2* in
 struct RowIn { float2 dys, dys2, dxn, dxn2, wet, gn2, pk; };
 
 template <bool CREST, bool BND, bool TAPE = false>
-__global__ void __launch_bounds__(kBandWarps * 32, 4) k_band(const PlainArgs A) {
+__global__ void __launch_bounds__(kBandWarps * 32, 3) k_band(const PlainArgs A) {
   __shared__ float4 edge_w[kBandWarps][kBandRows], edge_e[kBandWarps][kBandRows];
   __shared__ float wmax[kBandWarps];
   __shared__ unsigned wbad[kBandWarps];
