@@ -614,6 +614,7 @@ def main():
     if args.duration is not None:
         sc.params.duration_s = float(args.duration)
     g = GpuSolver(local)
+    apply_options(g)
     if args.cluster or args.threads:
         g.set_option("cluster", args.cluster)
         g.set_option("threads", args.threads)
