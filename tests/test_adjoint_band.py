@@ -127,3 +127,29 @@ def test_trimmed_sweep_equals_full_sweep(gpu, name):
         for f in ("dj_ddzx", "dj_ddzy"):
             ga, gb = np.asarray(getattr(a, f)), np.asarray(getattr(b, f))
             assert np.array_equal(ga.view(np.uint64), gb.view(np.uint64)), (name, i, f, int(np.count_nonzero(ga != gb)))
+
+
+def test_default_kernels_on_a_large_grid_equal_the_tiles(gpu):
+    """From 2^18 cells on, the default (adj_band = -1) runs the backward step on row bands too:
+    on a 512 x 512 grid (configuration 5's fractal terrain at 4 m, two designs, the first 300 s)
+    its gradients equal the all-tile sweep's bit for bit."""
+    from itr_gpu.scenes import fractal_scene
+    sc = fractal_scene(512, 4.0)
+    sc.params.duration_s = 300.0
+    terrs = [t for _, _, t in sc.designs(2)]
+    runs = {}
+    try:
+        for band in (-1, 0):
+            gpu.set_option("adj_band", band)
+            runs[band] = gpu.vjp(sc.params, terrs, sc.monitors, sc.objective, checkpoint_interval=64)
+    finally:
+        gpu.set_option("adj_band", -1)
+    nonzero = 0
+    for i, (a, b) in enumerate(zip(runs[-1], runs[0])):
+        assert a.steps == b.steps and a.j == b.j, i
+        for f in ("dj_ddzx", "dj_ddzy"):
+            ga, gb = np.asarray(getattr(a, f)), np.asarray(getattr(b, f))
+            assert np.all(np.isfinite(ga)), (i, f)
+            assert np.array_equal(ga.view(np.uint64), gb.view(np.uint64)), (i, f, int(np.count_nonzero(ga != gb)))
+            nonzero += int(np.count_nonzero(ga))
+    assert nonzero > 0
